@@ -1,0 +1,688 @@
+// dev_cuda.cu — CUDA implementation of the device layer (ecg_dev.h) for
+// sm_100a: FP64 GEMM on the double-precision MMA pipe, tensor permutation,
+// amplitude updates and deterministic reductions.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdio>
+
+#include "ecg_dev.h"
+
+namespace ecg {
+namespace dev {
+
+static std::atomic<int64_t> g_launches{0};
+int64_t launches() { return g_launches.load(); }
+static inline int launched() {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return (int)cudaGetLastError();
+}
+
+int set_device(int device) { return (int)cudaSetDevice(device); }
+int stream_create(stream_t* s) {
+  cudaStream_t st;
+  int e = (int)cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  *s = (stream_t)st;
+  return e;
+}
+void stream_destroy(stream_t s) { cudaStreamDestroy((cudaStream_t)s); }
+int sync(stream_t s) { return (int)cudaStreamSynchronize((cudaStream_t)s); }
+const char* error_string(int code) { return cudaGetErrorString((cudaError_t)code); }
+int check_launch() { return (int)cudaGetLastError(); }
+
+void* dmalloc(size_t bytes) {
+  void* p = nullptr;
+  if (cudaMalloc(&p, bytes < 256 ? 256 : bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return p;
+}
+void dfree(void* p) {
+  if (p) cudaFree(p);
+}
+void* hmalloc_pinned(size_t bytes) {
+  void* p = nullptr;
+  if (cudaMallocHost(&p, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return p;
+}
+void hfree_pinned(void* p) {
+  if (p) cudaFreeHost(p);
+}
+int h2d(void* dst, const void* src, size_t bytes, stream_t s) {
+  if (!bytes) return 0;
+  return (int)cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, (cudaStream_t)s);
+}
+int d2h(void* dst, const void* src, size_t bytes, stream_t s) {
+  if (!bytes) return 0;
+  return (int)cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, (cudaStream_t)s);
+}
+int d2d(void* dst, const void* src, size_t bytes, stream_t s) {
+  if (!bytes) return 0;
+  return (int)cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, (cudaStream_t)s);
+}
+int memset0(void* dst, size_t bytes, stream_t s) {
+  if (!bytes) return 0;
+  return (int)cudaMemsetAsync(dst, 0, bytes, (cudaStream_t)s);
+}
+
+// ---------------------------------------------------------------- GEMM
+//
+// Column-major C(m,n) = alpha*opA(A)(m,k)*opB(B)(k,n) + beta*C.  Tiles of
+// BM x BN per CTA, BK deep, staged through shared memory with a
+// STAGES-deep cp.async ring; each warp owns a WM x WN sub-tile computed
+// with mma.sync m8n8k4 f64 (the FP64 MMA pipe).  Shared tiles are stored
+// k-major ([k][m] and [k][n]) with a row pitch of BM+4 / BN+4 doubles so that
+// the 8x4 fragment reads of a half-warp hit 32 distinct banks.
+
+struct GemmArgs {
+  const double* A;
+  const double* B;
+  double* C;
+  int64_t m, n, k;
+  int64_t sam, sak, sab, sbk, sbn, sbb, scm, scn, scb;
+  double alpha, beta;
+  int a_kfast, b_nfast;  // loader thread order follows the unit-stride index
+};
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool pred) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  int sz = pred ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(sz));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+__device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
+  asm volatile(
+      "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+      : "+d"(d[0]), "+d"(d[1])
+      : "d"(a), "d"(b));
+}
+
+template <int BM, int BN, int BK, int WM, int WN, int STAGES>
+struct GemmCfg {
+  static constexpr int WARPS_M = BM / WM;
+  static constexpr int WARPS_N = BN / WN;
+  static constexpr int THREADS = WARPS_M * WARPS_N * 32;
+  static constexpr int LDA_S = BM + 4;
+  static constexpr int LDB_S = BN + 4;
+  static constexpr int A_STAGE = BK * LDA_S;
+  static constexpr int B_STAGE = BK * LDB_S;
+  static constexpr size_t SMEM = (size_t)STAGES * (A_STAGE + B_STAGE) * sizeof(double);
+};
+
+template <int BM, int BN, int BK, int WM, int WN, int STAGES>
+__global__ void __launch_bounds__(GemmCfg<BM, BN, BK, WM, WN, STAGES>::THREADS)
+    dgemm_kernel(GemmArgs g) {
+  using Cfg = GemmCfg<BM, BN, BK, WM, WN, STAGES>;
+  constexpr int NT = Cfg::THREADS;
+  constexpr int MT = WM / 8, NTL = WN / 8;
+  extern __shared__ double smem[];
+  double* As = smem;
+  double* Bs = smem + STAGES * Cfg::A_STAGE;
+
+  const int64_t bz = blockIdx.z;
+  const double* A = g.A + bz * g.sab;
+  const double* B = g.B + bz * g.sbb;
+  double* C = g.C + bz * g.scb;
+  const int64_t m0 = (int64_t)blockIdx.x * BM;
+  const int64_t n0 = (int64_t)blockIdx.y * BN;
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  const int wm0 = (warp % Cfg::WARPS_M) * WM;
+  const int wn0 = (warp / Cfg::WARPS_M) * WN;
+  const int gq = lane >> 2, tq = lane & 3;
+  const int64_t KT = (g.k + BK - 1) / BK;
+
+  auto load_tile = [&](int stage, int64_t kt) {
+    const int64_t k0 = kt * BK;
+    double* as = As + stage * Cfg::A_STAGE;
+    double* bs = Bs + stage * Cfg::B_STAGE;
+#pragma unroll
+    for (int r = 0; r < (BM * BK + NT - 1) / NT; ++r) {
+      int e = tid + r * NT;
+      if (e < BM * BK) {
+        int mm, kk;
+        if (!g.a_kfast) { mm = e % BM; kk = e / BM; } else { kk = e % BK; mm = e / BK; }
+        int64_t gm = m0 + mm, gk = k0 + kk;
+        bool ok = gm < g.m && gk < g.k;
+        const double* src = ok ? A + gm * g.sam + gk * g.sak : A;
+        cp_async8(as + kk * Cfg::LDA_S + mm, src, ok);
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < (BN * BK + NT - 1) / NT; ++r) {
+      int e = tid + r * NT;
+      if (e < BN * BK) {
+        int nn, kk;
+        if (!g.b_nfast) { kk = e % BK; nn = e / BK; } else { nn = e % BN; kk = e / BN; }
+        int64_t gn = n0 + nn, gk = k0 + kk;
+        bool ok = gn < g.n && gk < g.k;
+        const double* src = ok ? B + gk * g.sbk + gn * g.sbn : B;
+        cp_async8(bs + kk * Cfg::LDB_S + nn, src, ok);
+      }
+    }
+  };
+
+  double acc[MT][NTL][2];
+#pragma unroll
+  for (int i = 0; i < MT; ++i)
+#pragma unroll
+    for (int j = 0; j < NTL; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < KT) load_tile(s, s);
+    cp_async_commit();
+  }
+  for (int64_t kt = 0; kt < KT; ++kt) {
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();
+    int64_t nxt = kt + STAGES - 1;
+    if (nxt < KT) load_tile((int)(nxt % STAGES), nxt);
+    cp_async_commit();
+    const double* as = As + (kt % STAGES) * Cfg::A_STAGE;
+    const double* bs = Bs + (kt % STAGES) * Cfg::B_STAGE;
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 4) {
+      double af[MT], bf[NTL];
+#pragma unroll
+      for (int i = 0; i < MT; ++i) af[i] = as[(kk + tq) * Cfg::LDA_S + wm0 + i * 8 + gq];
+#pragma unroll
+      for (int j = 0; j < NTL; ++j) bf[j] = bs[(kk + tq) * Cfg::LDB_S + wn0 + j * 8 + gq];
+#pragma unroll
+      for (int i = 0; i < MT; ++i)
+#pragma unroll
+        for (int j = 0; j < NTL; ++j) dmma884(acc[i][j], af[i], bf[j]);
+    }
+  }
+  cp_async_wait<0>();
+
+#pragma unroll
+  for (int i = 0; i < MT; ++i) {
+    int64_t row = m0 + wm0 + i * 8 + gq;
+    if (row >= g.m) continue;
+#pragma unroll
+    for (int j = 0; j < NTL; ++j) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        int64_t col = n0 + wn0 + j * 8 + 2 * tq + h;
+        if (col < g.n) {
+          double* cp = C + row * g.scm + col * g.scn;
+          double v = g.alpha * acc[i][j][h];
+          if (g.beta != 0.0) v += g.beta * *cp;
+          *cp = v;
+        }
+      }
+    }
+  }
+}
+
+template <int BM, int BN, int BK, int WM, int WN, int STAGES>
+static int launch_gemm(const GemmArgs& g, int64_t batch, cudaStream_t st) {
+  using Cfg = GemmCfg<BM, BN, BK, WM, WN, STAGES>;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(dgemm_kernel<BM, BN, BK, WM, WN, STAGES>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
+    attr = true;
+  }
+  int64_t gx = (g.m + BM - 1) / BM, gy = (g.n + BN - 1) / BN;
+  if (gy > 65535 || batch > 65535) return (int)cudaErrorInvalidConfiguration;
+  dim3 grid((unsigned)gx, (unsigned)gy, (unsigned)batch);
+  dgemm_kernel<BM, BN, BK, WM, WN, STAGES><<<grid, Cfg::THREADS, Cfg::SMEM, st>>>(g);
+  return launched();
+}
+
+int gemm_strided(stream_t s, const Gemm& q) {
+  if (q.m <= 0 || q.n <= 0 || q.batch <= 0) return 0;
+  cudaStream_t st = (cudaStream_t)s;
+  if (q.k <= 0 || q.alpha == 0.0) {
+    if (q.beta == 1.0) return 0;
+    for (int64_t b = 0; b < q.batch; ++b)
+      for (int64_t j = 0; j < q.n; ++j)
+        for (int64_t i = 0; i < q.m; ++i) {
+          // rare path (empty contraction): scale C element-wise
+          double* p = q.C + b * q.scb + j * q.scn + i * q.scm;
+          int e = axpby(s, 1, 0.0, p, q.beta, p);
+          if (e) return e;
+        }
+    return 0;
+  }
+  GemmArgs g{q.A, q.B, q.C, q.m, q.n, q.k, q.sam, q.sak, q.sab, q.sbk, q.sbn, q.sbb,
+             q.scm, q.scn, q.scb, q.alpha, q.beta, (q.sam != 1 && q.sak == 1) ? 1 : 0,
+             (q.sbk != 1 && q.sbn == 1) ? 1 : 0};
+  int64_t big_tiles = ((q.m + 127) / 128) * ((q.n + 127) / 128) * q.batch;
+  if (big_tiles >= 2 * 148) return launch_gemm<128, 128, 16, 64, 32, 3>(g, q.batch, st);
+  return launch_gemm<64, 64, 16, 32, 32, 3>(g, q.batch, st);
+}
+
+int gemm(stream_t s, char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha,
+         const double* A, int64_t lda, const double* B, int64_t ldb, double beta, double* C,
+         int64_t ldc, int64_t batch, int64_t sa, int64_t sb, int64_t sc) {
+  Gemm q;
+  q.m = m; q.n = n; q.k = k; q.batch = batch; q.alpha = alpha; q.beta = beta;
+  q.A = A; q.B = B; q.C = C;
+  bool at = (ta == 'T' || ta == 't'), bt = (tb == 'T' || tb == 't');
+  q.sam = at ? lda : 1; q.sak = at ? 1 : lda; q.sab = sa;
+  q.sbk = bt ? ldb : 1; q.sbn = bt ? 1 : ldb; q.sbb = sb;
+  q.scm = 1; q.scn = ldc; q.scb = sc;
+  return gemm_strided(s, q);
+}
+
+// ---------------------------------------------------------------- permute
+
+struct PermArgs {
+  int nd;
+  int64_t odim[8];   // out dims
+  int64_t istr[8];   // in stride of out dim d
+  int64_t ostr[8];   // out stride of out dim d
+  int q;             // out dim that is the in-fastest dim (perm[q] == 0)
+  int64_t total;
+  double alpha, beta;
+  const double* in;
+  double* out;
+};
+
+// Plain elementwise permutation (out-fastest index also drives the input
+// fastest or the tensor is small): one thread per output element.
+__global__ void permute_plain_kernel(PermArgs p) {
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < p.total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = idx, off = 0;
+#pragma unroll 8
+    for (int d = 0; d < p.nd; ++d) {
+      int64_t x = r % p.odim[d];
+      r /= p.odim[d];
+      off += x * p.istr[d];
+    }
+    double v = p.alpha * p.in[off];
+    if (p.beta != 0.0) v += p.beta * p.out[idx];
+    p.out[idx] = v;
+  }
+}
+
+// Tiled permutation: 32x32 tiles spanning out dim 0 (written contiguously)
+// and out dim q (read contiguously); all other dims enumerate tiles.
+__global__ void permute_tiled_kernel(PermArgs p, int64_t tiles0, int64_t tilesq, int64_t rest) {
+  __shared__ double tile[32][33];
+  const int64_t ntile = tiles0 * tilesq * rest;
+  const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+  for (int64_t t = blockIdx.x; t < ntile; t += gridDim.x) {
+    int64_t t0 = t % tiles0;
+    int64_t tq = (t / tiles0) % tilesq;
+    int64_t r = t / (tiles0 * tilesq);
+    int64_t ibase = 0, obase = 0;
+    for (int d = 1; d < p.nd; ++d) {
+      if (d == p.q) continue;
+      int64_t x = r % p.odim[d];
+      r /= p.odim[d];
+      ibase += x * p.istr[d];
+      obase += x * p.ostr[d];
+    }
+    const int64_t x0b = t0 * 32, xqb = tq * 32;
+    // read: contiguous along q (input fastest)
+    for (int j = ty; j < 32; j += 8) {
+      int64_t x0 = x0b + j, xq = xqb + tx;
+      if (x0 < p.odim[0] && xq < p.odim[p.q])
+        tile[j][tx] = p.in[ibase + x0 * p.istr[0] + xq * p.istr[p.q]];
+    }
+    __syncthreads();
+    for (int j = ty; j < 32; j += 8) {
+      int64_t x0 = x0b + tx, xq = xqb + j;
+      if (x0 < p.odim[0] && xq < p.odim[p.q]) {
+        int64_t o = obase + x0 + xq * p.ostr[p.q];
+        double v = p.alpha * tile[tx][j];
+        if (p.beta != 0.0) v += p.beta * p.out[o];
+        p.out[o] = v;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+int permute(stream_t s, int nd, const int64_t* in_dims, const int* perm, double alpha,
+            const double* in, double beta, double* out) {
+  if (nd < 1 || nd > 8) return (int)cudaErrorInvalidValue;
+  PermArgs p{};
+  p.nd = nd;
+  int64_t istride[8];
+  istride[0] = 1;
+  for (int d = 1; d < nd; ++d) istride[d] = istride[d - 1] * in_dims[d - 1];
+  p.total = 1;
+  for (int d = 0; d < nd; ++d) {
+    p.odim[d] = in_dims[perm[d]];
+    p.istr[d] = istride[perm[d]];
+    p.ostr[d] = p.total;
+    p.total *= p.odim[d];
+    if (perm[d] == 0) p.q = d;
+  }
+  if (p.total == 0) return 0;
+  p.alpha = alpha;
+  p.beta = beta;
+  p.in = in;
+  p.out = out;
+  cudaStream_t st = (cudaStream_t)s;
+  if (p.q == 0 || p.odim[0] < 8 || p.odim[p.q] < 8) {
+    int64_t blocks = (p.total + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    permute_plain_kernel<<<(unsigned)blocks, 256, 0, st>>>(p);
+  } else {
+    int64_t t0 = (p.odim[0] + 31) / 32, tq = (p.odim[p.q] + 31) / 32;
+    int64_t rest = p.total / (p.odim[0] * p.odim[p.q]);
+    int64_t blocks = t0 * tq * rest;
+    if (blocks > 148 * 32) blocks = 148 * 32;
+    permute_tiled_kernel<<<(unsigned)blocks, dim3(32, 8), 0, st>>>(p, t0, tq, rest);
+  }
+  return launched();
+}
+
+// ---------------------------------------------------------------- elementwise
+
+__global__ void axpby_kernel(int64_t n, double alpha, const double* x, double beta, double* y) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double v = alpha * x[i];
+    if (beta != 0.0) v += beta * y[i];
+    y[i] = v;
+  }
+}
+
+static unsigned grid_for(int64_t n, int threads = 256, int64_t cap = 148 * 16) {
+  int64_t b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > cap) b = cap;
+  return (unsigned)b;
+}
+
+int axpby(stream_t s, int64_t n, double alpha, const double* x, double beta, double* y) {
+  if (n <= 0) return 0;
+  axpby_kernel<<<grid_for(n), 256, 0, (cudaStream_t)s>>>(n, alpha, x, beta, y);
+  return launched();
+}
+
+__global__ void strided_sum_kernel(int64_t nb, int64_t sb, int64_t nk, int64_t sk, double alpha,
+                                   const double* in, double beta, double* out) {
+  for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < nb;
+       b += (int64_t)gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (int64_t k = 0; k < nk; ++k) acc += in[b * sb + k * sk];
+    double v = alpha * acc;
+    if (beta != 0.0) v += beta * out[b];
+    out[b] = v;
+  }
+}
+
+int strided_sum(stream_t s, int64_t nb, int64_t sb, int64_t nk, int64_t sk, double alpha,
+                const double* in, double beta, double* out) {
+  if (nb <= 0) return 0;
+  strided_sum_kernel<<<grid_for(nb), 256, 0, (cudaStream_t)s>>>(nb, sb, nk, sk, alpha, in, beta,
+                                                                 out);
+  return launched();
+}
+
+__global__ void update_doubles_kernel(int nv, int no, const double* eo, const double* ev,
+                                      double shift, const double* R, double* T) {
+  const int64_t n = (int64_t)nv * nv * no * no;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < n;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    int a = (int)(idx % nv);
+    int b = (int)((idx / nv) % nv);
+    int i = (int)((idx / ((int64_t)nv * nv)) % no);
+    int j = (int)(idx / ((int64_t)nv * nv * no));
+    T[idx] -= R[idx] / (ev[a] + ev[b] - eo[i] - eo[j] + shift);
+  }
+}
+
+__global__ void update_singles_kernel(int nv, int no, const double* eo, const double* ev,
+                                      double shift, const double* R, double* T) {
+  const int64_t n = (int64_t)nv * no;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < n;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    int a = (int)(idx % nv);
+    int i = (int)(idx / nv);
+    T[idx] -= R[idx] / (ev[a] - eo[i] + shift);
+  }
+}
+
+int update_doubles(stream_t s, int nv, int no, const double* eo, const double* ev, double shift,
+                   const double* R, double* T) {
+  int64_t n = (int64_t)nv * nv * no * no;
+  if (n <= 0) return 0;
+  update_doubles_kernel<<<grid_for(n), 256, 0, (cudaStream_t)s>>>(nv, no, eo, ev, shift, R, T);
+  return launched();
+}
+int update_singles(stream_t s, int nv, int no, const double* eo, const double* ev, double shift,
+                   const double* R, double* T) {
+  int64_t n = (int64_t)nv * no;
+  if (n <= 0) return 0;
+  update_singles_kernel<<<grid_for(n), 256, 0, (cudaStream_t)s>>>(nv, no, eo, ev, shift, R, T);
+  return launched();
+}
+
+// ---------------------------------------------------------------- reductions
+//
+// Fixed grid (RED_BLOCKS x 256) + a single-block final pass in a fixed order:
+// results are bitwise reproducible run to run.
+
+static constexpr int RED_BLOCKS = 592;
+int64_t reduce_scratch_len() { return 2 * RED_BLOCKS; }
+
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (w == 0) {
+    r = (l < (int)(blockDim.x >> 5)) ? sh[l] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+  }
+  __syncthreads();
+  return r;
+}
+
+__global__ void dot_partial_kernel(int64_t n, const double* x, const double* y, double* part) {
+  __shared__ double sh[32];
+  double acc = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    acc += x[i] * y[i];
+  double r = block_sum(acc, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = r;
+}
+
+__global__ void cs_dot_partial_kernel(int nv, int no, const double* X, const double* Y,
+                                      double* part) {
+  __shared__ double sh[32];
+  const int64_t vv = (int64_t)nv * nv, n = vv * no * no;
+  double d = 0.0, ex = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t a = i % nv, b = (i / nv) % nv, ij = i / vv;
+    double y = Y[i];
+    d += X[i] * y;
+    ex += X[b + a * nv + ij * vv] * y;
+  }
+  double r0 = block_sum(d, sh);
+  double r1 = block_sum(ex, sh);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = r0;
+    part[RED_BLOCKS + blockIdx.x] = r1;
+  }
+}
+
+__global__ void final_sum_kernel(int nparts, int nout, const double* part, double* out) {
+  __shared__ double sh[32];
+  for (int o = 0; o < nout; ++o) {
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < nparts; i += blockDim.x) acc += part[o * RED_BLOCKS + i];
+    double r = block_sum(acc, sh);
+    if (threadIdx.x == 0) out[o] = r;
+  }
+}
+
+int dot(stream_t s, int64_t n, const double* x, const double* y, double* scratch, double* out) {
+  cudaStream_t st = (cudaStream_t)s;
+  dot_partial_kernel<<<RED_BLOCKS, 256, 0, st>>>(n, x, y, scratch);
+  int e = launched();
+  if (e) return e;
+  final_sum_kernel<<<1, 256, 0, st>>>(RED_BLOCKS, 1, scratch, out);
+  return launched();
+}
+
+int cs_dot(stream_t s, int nv, int no, const double* X, const double* Y, double* scratch,
+           double* out) {
+  cudaStream_t st = (cudaStream_t)s;
+  cs_dot_partial_kernel<<<RED_BLOCKS, 256, 0, st>>>(nv, no, X, Y, scratch);
+  int e = launched();
+  if (e) return e;
+  final_sum_kernel<<<1, 256, 0, st>>>(RED_BLOCKS, 2, scratch, out);
+  return launched();
+}
+
+__global__ void geam_kernel(int64_t m, int64_t n, double alpha, const double* A, int64_t lda,
+                            double beta, double* C, int64_t ldc) {
+  const int64_t total = m * n;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    int64_t i = idx % m, j = idx / m;
+    double v = alpha * A[i + j * lda];
+    if (beta != 0.0) v += beta * C[i + j * ldc];
+    C[i + j * ldc] = v;
+  }
+}
+
+int geam(stream_t s, int64_t m, int64_t n, double alpha, const double* A, int64_t lda,
+         double beta, double* C, int64_t ldc) {
+  if (m <= 0 || n <= 0) return 0;
+  geam_kernel<<<grid_for(m * n), 256, 0, (cudaStream_t)s>>>(m, n, alpha, A, lda, beta, C, ldc);
+  return launched();
+}
+
+__global__ void outer_kernel(int64_t na, int64_t ni, int64_t nb, int64_t nj, double alpha,
+                             const double* X, const double* Y, double beta, double* out) {
+  const int64_t total = na * nb * ni * nj;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    int64_t a = idx % na, b = (idx / na) % nb, i = (idx / (na * nb)) % ni, j = idx / (na * nb * ni);
+    double v = alpha * X[a + i * na] * Y[b + j * nb];
+    if (beta != 0.0) v += beta * out[idx];
+    out[idx] = v;
+  }
+}
+
+int outer(stream_t s, int64_t na, int64_t ni, int64_t nb, int64_t nj, double alpha,
+          const double* X, const double* Y, double beta, double* out) {
+  int64_t total = na * nb * ni * nj;
+  if (total <= 0) return 0;
+  outer_kernel<<<grid_for(total), 256, 0, (cudaStream_t)s>>>(na, ni, nb, nj, alpha, X, Y, beta,
+                                                              out);
+  return launched();
+}
+
+struct CombineArgs {
+  const double* X[8];
+};
+
+__global__ void combine_kernel(int64_t n, int m, CombineArgs a, const double* coef, double* out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double v = coef[0] * a.X[0][i];
+    for (int k = 1; k < m; ++k) v += coef[k] * a.X[k][i];
+    out[i] = v;
+  }
+}
+
+int combine(stream_t s, int64_t n, int m, const double* const* X, const double* coef,
+            double* out) {
+  if (m < 1 || m > 8) return (int)cudaErrorInvalidValue;
+  if (n <= 0) return 0;
+  CombineArgs a{};
+  for (int k = 0; k < m; ++k) a.X[k] = X[k];
+  combine_kernel<<<grid_for(n), 256, 0, (cudaStream_t)s>>>(n, m, a, coef, out);
+  return launched();
+}
+
+// ---------------------------------------------------------------- (T)
+
+__global__ void triples_x_kernel(int nv, const double* __restrict__ K, double eijk,
+                                 const double* __restrict__ ev, double* __restrict__ X,
+                                 double* part, int want_e) {
+  __shared__ double sh[32];
+  const int64_t v = nv, n = v * v * v;
+  double acc = 0.0;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < n;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    int64_t a = idx % v, b = (idx / v) % v, c = idx / (v * v);
+    double kabc = K[idx];
+    double x = 4.0 * kabc - 2.0 * K[a + v * c + v * v * b] - 2.0 * K[c + v * b + v * v * a] -
+               2.0 * K[b + v * a + v * v * c] + K[c + v * a + v * v * b] + K[b + v * c + v * v * a];
+    x /= (eijk - ev[a] - ev[b] - ev[c]);
+    X[idx] = x;
+    acc += kabc * x;
+  }
+  if (want_e) {
+    double r = block_sum(acc, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = r;
+  }
+}
+
+int triples_x(stream_t s, int nv, const double* K, double eijk, const double* ev, double* X,
+              double* scratch, double* eout) {
+  cudaStream_t st = (cudaStream_t)s;
+  triples_x_kernel<<<RED_BLOCKS, 256, 0, st>>>(nv, K, eijk, ev, X, scratch, eout ? 1 : 0);
+  int e = launched();
+  if (e || !eout) return e;
+  final_sum_kernel<<<1, 256, 0, st>>>(RED_BLOCKS, 1, scratch, eout);
+  return launched();
+}
+
+__global__ void triples_int_kernel(int nv, const double* __restrict__ X, const double* Mjk,
+                                   const double* Mik, const double* Mij, const double* Njk,
+                                   const double* Nik, const double* Nij, double fac, double* IntX,
+                                   double* IntY, int i, int j, int k) {
+  __shared__ double sh[32];
+  const int64_t v = nv, x = blockIdx.x;
+  double s[6] = {0, 0, 0, 0, 0, 0};
+  for (int64_t e = threadIdx.x; e < v * v; e += blockDim.x) {
+    int64_t p = e % v, q = e / v;
+    double x0 = X[x + v * p + v * v * q];  // X[x,b,c], (b,c) = (p,q)
+    double x1 = X[p + v * x + v * v * q];  // X[a,x,c], (a,c) = (p,q)
+    double x2 = X[p + v * q + v * v * x];  // X[a,b,x], (a,b) = (p,q)
+    s[0] += x0 * Mjk[e];
+    s[1] += x1 * Mik[e];
+    s[2] += x2 * Mij[e];
+    s[3] += x0 * Njk[e];
+    s[4] += x1 * Nik[e];
+    s[5] += x2 * Nij[e];
+  }
+  double r[6];
+  for (int t = 0; t < 6; ++t) r[t] = block_sum(s[t], sh);
+  if (threadIdx.x == 0) {
+    IntX[x + v * i] += fac * r[0];
+    IntX[x + v * j] += fac * r[1];
+    IntX[x + v * k] += fac * r[2];
+    IntY[x + v * i] += fac * r[3];
+    IntY[x + v * j] += fac * r[4];
+    IntY[x + v * k] += fac * r[5];
+  }
+}
+
+int triples_int(stream_t s, int nv, const double* X, const double* Mjk, const double* Mik,
+                const double* Mij, const double* Njk, const double* Nik, const double* Nij,
+                double fac, double* IntX, double* IntY, int i, int j, int k) {
+  triples_int_kernel<<<nv, 256, 0, (cudaStream_t)s>>>(nv, X, Mjk, Mik, Mij, Njk, Nik, Nij, fac,
+                                                      IntX, IntY, i, j, k);
+  return launched();
+}
+
+}  // namespace dev
+}  // namespace ecg

@@ -1,0 +1,400 @@
+// ecg_api.cpp — extern "C" entry points of libecgpu (declared in
+// include/ecgpu.h).  Each call catches the library's exceptions and turns
+// them into a status code plus a per-context message.
+#include <cmath>
+#include <cstring>
+#include <exception>
+#include <new>
+
+#include "ecg_core.h"
+#include "ecg_lambda.h"
+#include "ecg_triples.h"
+
+using namespace ecg;
+
+struct ecg_ctx : Ctx {};
+
+struct ecg_diis {
+  ecg_ctx* ctx;
+  DiisState st;
+  double* v;
+  double* r;
+};
+
+static thread_local std::string g_noctx_err;
+
+template <class F>
+static int guarded(Ctx* c, F&& f) {
+  try {
+    f();
+    if (c) c->err.clear();
+    return ECG_OK;
+  } catch (const Error& e) {
+    if (c) c->err = e.what();
+    else g_noctx_err = e.what();
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    if (c) c->err = "host out of memory";
+    return ECG_ERR_OOM;
+  } catch (const std::exception& e) {
+    if (c) c->err = e.what();
+    return ECG_ERR_ARG;
+  }
+}
+
+static void need_system(Ctx& c) {
+  if (!c.have_system) throw Error(ECG_ERR_STATE, "no system set (call ecg_set_system first)");
+}
+
+static void need_ptr(const void* p, const char* what) {
+  if (!p) throw Error(ECG_ERR_ARG, std::string("NULL pointer: ") + what);
+}
+
+static void check_finite(const double* x, int64_t n, const char* what) {
+  for (int64_t i = 0; i < n; ++i)
+    if (!std::isfinite(x[i])) throw Error(ECG_ERR_NONFINITE, std::string("non-finite value in ") + what);
+}
+
+static void opts_or_default(const ecg_cc_opts* in, ecg_cc_opts& o) {
+  if (in) o = *in;
+  else ecg_default_opts(&o);
+  if (o.maxdiis < 1 || o.maxdiis > 8) throw Error(ECG_ERR_ARG, "maxdiis must be in 1..8");
+  if (o.maxit < 0) throw Error(ECG_ERR_ARG, "maxit must be >= 0");
+}
+
+static void load_T(Ctx& c, const double* T1, const double* T2) {
+  need_ptr(T1, "T1");
+  need_ptr(T2, "T2");
+  check_finite(T1, c.n1(), "T1");
+  check_finite(T2, c.n2(), "T2");
+  check(dev::h2d(c.T1(), T1, c.n1() * 8, c.st), "h2d T1");
+  check(dev::h2d(c.T2(), T2, c.n2() * 8, c.st), "h2d T2");
+}
+
+extern "C" {
+
+void ecg_default_opts(ecg_cc_opts* o) {
+  if (!o) return;
+  o->thr = 1.0e-10;
+  o->conven = 0.1;
+  o->maxit = 50;
+  o->shifts = 0.15;
+  o->shiftp = 0.2;
+  o->maxdiis = 6;
+  o->resthr = 10.0;
+}
+
+int ecg_create(int device, ecg_ctx** out) {
+  if (!out) return ECG_ERR_ARG;
+  *out = nullptr;
+  ecg_ctx* c = new (std::nothrow) ecg_ctx();
+  if (!c) return ECG_ERR_OOM;
+  int st = guarded(c, [&] {
+    c->device = device;
+    check(dev::set_device(device), "cudaSetDevice");
+    check(dev::stream_create(&c->st), "cudaStreamCreate");
+    ecg_default_opts(&c->opts);
+  });
+  if (st != ECG_OK) {
+    g_noctx_err = c->err;
+    delete c;
+    return st;
+  }
+  *out = c;
+  return ECG_OK;
+}
+
+int ecg_destroy(ecg_ctx* c) {
+  if (!c) return ECG_OK;
+  dev::set_device(c->device);
+  c->free_all();
+  if (c->st) dev::stream_destroy(c->st);
+  delete c;
+  return ECG_OK;
+}
+
+const char* ecg_last_error(const ecg_ctx* c) {
+  if (!c) return g_noctx_err.c_str();
+  return c->err.c_str();
+}
+
+int ecg_set_mem_cap(ecg_ctx* c, uint64_t bytes) {
+  if (!c) return ECG_ERR_ARG;
+  c->memcap = bytes;
+  return ECG_OK;
+}
+
+int ecg_set_precision(ecg_ctx* c, int prec) {
+  if (!c) return ECG_ERR_ARG;
+  return guarded(c, [&] {
+    if (prec != ECG_PREC_FP64 && prec != ECG_PREC_MIXED)
+      throw Error(ECG_ERR_ARG, "precision must be ECG_PREC_FP64 or ECG_PREC_MIXED");
+    c->prec = prec;
+  });
+}
+
+int ecg_set_system(ecg_ctx* c, int32_t no, int32_t nv, int32_t nq, const double* B,
+                   const double* h1, double e0) {
+  if (!c) return ECG_ERR_ARG;
+  return guarded(c, [&] {
+    need_ptr(B, "B");
+    need_ptr(h1, "h1");
+    if (!std::isfinite(e0)) throw Error(ECG_ERR_NONFINITE, "non-finite e0");
+    check(dev::set_device(c->device), "cudaSetDevice");
+    setup_system(*c, no, nv, nq, B, h1, e0);
+  });
+}
+
+int ecg_fock(ecg_ctx* c, double* fock, double* eps, double* e_hf) {
+  if (!c) return ECG_ERR_ARG;
+  return guarded(c, [&] {
+    need_system(*c);
+    const int64_t n = c->n;
+    if (fock) std::memcpy(fock, c->fock_host.data(), n * n * 8);
+    if (eps)
+      for (int64_t p = 0; p < n; ++p) eps[p] = c->fock_host[p + p * n];
+    if (e_hf) {
+      // calc_HF_energy closed shell (cctools.jl:65-72)
+      double e = c->e0;
+      for (int64_t i = 0; i < c->no; ++i) e += c->fock_host[i + i * n] + c->h_host[i + i * n];
+      *e_hf = e;
+    }
+  });
+}
+
+int ecg_mp2(ecg_ctx* c, double* T1, double* T2, double* e_mp2) {
+  if (!c) return ECG_ERR_ARG;
+  return guarded(c, [&] {
+    need_system(*c);
+    dev::stream_t s = c->st;
+    const double* eo = c->eps;
+    const double* ev = c->eps + c->no;
+    // T2 = -<ab|ij>/D, T1 = -f[v,o]/D without level shift (cc.jl:1012-1017)
+    check(dev::memset0(c->T, (c->n1() + c->n2()) * 8, s), "memset");
+    check(dev::update_doubles(s, c->nv, c->no, eo, ev, 0.0, c->Kvvoo, c->T2()), "mp2 T2");
+    check(dev::geam(s, c->nv, c->no, 1.0, c->fock + c->no, c->n, 0.0, c->R1(), c->nv), "fvo");
+    check(dev::update_singles(s, c->nv, c->no, eo, ev, 0.0, c->R1(), c->T1()), "mp2 T1");
+    check(dev::cs_dot(s, c->nv, c->no, c->T2(), c->Kvvoo, c->red, c->dscal), "mp2 e");
+    check(dev::dot(s, c->n1(), c->fvo_t, c->T1(), c->red, c->dscal + 2), "mp2 e1");
+    if (T1) check(dev::d2h(T1, c->T1(), c->n1() * 8, s), "d2h");
+    if (T2) check(dev::d2h(T2, c->T2(), c->n2() * 8, s), "d2h");
+    sync_scalars(*c, 3);
+    if (e_mp2) *e_mp2 = 2.0 * c->hscal[0] - c->hscal[1] + 2.0 * c->hscal[2];
+  });
+}
+
+int ecg_cc_residual(ecg_ctx* c, int dc, const double* T1, const double* T2, double* R1,
+                    double* R2) {
+  if (!c) return ECG_ERR_ARG;
+  return guarded(c, [&] {
+    need_system(*c);
+    load_T(*c, T1, T2);
+    cc_residual(*c, dc != 0);
+    if (R1) check(dev::d2h(R1, c->R1(), c->n1() * 8, c->st), "d2h R1");
+    if (R2) check(dev::d2h(R2, c->R2(), c->n2() * 8, c->st), "d2h R2");
+    check(dev::sync(c->st), "sync");
+  });
+}
+
+int ecg_cc_load(ecg_ctx* c, const double* T1, const double* T2, const ecg_cc_opts* opts) {
+  if (!c) return ECG_ERR_ARG;
+  return guarded(c, [&] {
+    need_system(*c);
+    ecg_cc_opts o;
+    opts_or_default(opts, o);
+    if (T1 || T2) load_T(*c, T1, T2);
+    cc_init_iterations(*c, o);
+    check(dev::sync(c->st), "sync");
+  });
+}
+
+int ecg_cc_step(ecg_ctx* c, int dc, int32_t nsteps, double* out) {
+  if (!c) return ECG_ERR_ARG;
+  return guarded(c, [&] {
+    need_system(*c);
+    if (c->diis.len == 0) throw Error(ECG_ERR_STATE, "call ecg_cc_load first");
+    IterResult r{};
+    for (int32_t k = 0; k < nsteps; ++k) r = cc_iteration(*c, dc != 0);
+    if (out) {
+      out[0] = r.E;
+      out[1] = r.ESS;
+      out[2] = r.EOS;
+      out[3] = r.normR;
+      out[4] = r.dE;
+    }
+  });
+}
+
+int ecg_cc_store(ecg_ctx* c, double* T1, double* T2) {
+  if (!c) return ECG_ERR_ARG;
+  return guarded(c, [&] {
+    need_system(*c);
+    if (T1) check(dev::d2h(T1, c->T1(), c->n1() * 8, c->st), "d2h T1");
+    if (T2) check(dev::d2h(T2, c->T2(), c->n2() * 8, c->st), "d2h T2");
+    check(dev::sync(c->st), "sync");
+  });
+}
+
+int ecg_cc_solve(ecg_ctx* c, int dc, const ecg_cc_opts* opts, double* T1, double* T2,
+                 double* out, int32_t* iterations, int32_t* converged) {
+  if (!c) return ECG_ERR_ARG;
+  return guarded(c, [&] {
+    need_system(*c);
+    ecg_cc_opts o;
+    opts_or_default(opts, o);
+    load_T(*c, T1, T2);
+    cc_init_iterations(*c, o);
+    const double thren = std::sqrt(o.thr) * o.conven;
+    IterResult r{};
+    int it = 0;
+    bool conv = false;
+    for (it = 1; it <= o.maxit; ++it) {
+      r = cc_iteration(*c, dc != 0);
+      if (r.normR < o.thr && std::fabs(r.dE) < thren) {
+        conv = true;
+        break;
+      }
+    }
+    if (it > o.maxit) it = o.maxit;
+    check(dev::d2h(T1, c->T1(), c->n1() * 8, c->st), "d2h T1");
+    check(dev::d2h(T2, c->T2(), c->n2() * 8, c->st), "d2h T2");
+    check(dev::sync(c->st), "sync");
+    if (out) {
+      out[0] = r.E;
+      out[1] = r.ESS;
+      out[2] = r.EOS;
+      out[3] = r.normR;
+      out[4] = r.dE;
+    }
+    if (iterations) *iterations = it;
+    if (converged) *converged = conv ? 1 : 0;
+  });
+}
+
+int ecg_pert_t(ecg_ctx* c, const double* T1, const double* T2, double* e_t, double* e_tb) {
+  if (!c) return ECG_ERR_ARG;
+  return guarded(c, [&] {
+    need_system(*c);
+    load_T(*c, T1, T2);
+    double et = 0, etb = 0;
+    pert_triples(*c, nullptr, nullptr, &et, &etb);
+    if (e_t) *e_t = et;
+    if (e_tb) *e_tb = etb;
+  });
+}
+
+int ecg_lambda_pert_t(ecg_ctx* c, const double* T1, const double* T2, const double* U1,
+                      const double* U2, double* e_t, double* e_tb) {
+  if (!c) return ECG_ERR_ARG;
+  return guarded(c, [&] {
+    need_system(*c);
+    load_T(*c, T1, T2);
+    need_ptr(U1, "U1");
+    need_ptr(U2, "U2");
+    check_finite(U1, c->n1(), "U1");
+    check_finite(U2, c->n2(), "U2");
+    double et = 0, etb = 0;
+    pert_triples(*c, U1, U2, &et, &etb);
+    if (e_t) *e_t = et;
+    if (e_tb) *e_tb = etb;
+  });
+}
+
+int ecg_lambda_residual(ecg_ctx* c, int dc, const double* T1, const double* T2, const double* U1,
+                        const double* U2, double* R1, double* R2) {
+  if (!c) return ECG_ERR_ARG;
+  return guarded(c, [&] {
+    need_system(*c);
+    load_T(*c, T1, T2);
+    need_ptr(U1, "U1");
+    need_ptr(U2, "U2");
+    check_finite(U1, c->n1(), "U1");
+    check_finite(U2, c->n2(), "U2");
+    lambda_prepare(*c, dc != 0);
+    lambda_load_U(*c, U1, U2);
+    lambda_residual(*c, dc != 0);
+    lambda_store_R(*c, R1, R2);
+  });
+}
+
+int ecg_lambda_solve(ecg_ctx* c, int dc, const ecg_cc_opts* opts, const double* T1,
+                     const double* T2, double* U1, double* U2, double* out, int32_t* iterations,
+                     int32_t* converged) {
+  if (!c) return ECG_ERR_ARG;
+  return guarded(c, [&] {
+    need_system(*c);
+    ecg_cc_opts o;
+    opts_or_default(opts, o);
+    load_T(*c, T1, T2);
+    need_ptr(U1, "U1");
+    need_ptr(U2, "U2");
+    LambdaResult r = lambda_solve(*c, dc != 0, o);
+    lambda_store_U(*c, U1, U2);
+    if (out) {
+      out[0] = r.norm;
+      out[1] = r.normR;
+      out[2] = r.dnorm;
+    }
+    if (iterations) *iterations = r.iterations;
+    if (converged) *converged = r.converged ? 1 : 0;
+  });
+}
+
+int ecg_one_rdm(ecg_ctx* c, const double* T1, const double* T2, const double* U1,
+                const double* U2, double* D1, double* dD1) {
+  if (!c) return ECG_ERR_ARG;
+  return guarded(c, [&] {
+    need_system(*c);
+    load_T(*c, T1, T2);
+    need_ptr(U1, "U1");
+    need_ptr(U2, "U2");
+    lambda_load_U(*c, U1, U2);
+    one_rdm(*c, D1, dD1);
+  });
+}
+
+int ecg_diis_create(ecg_ctx* c, int32_t maxdiis, double resthr, int64_t len, ecg_diis** out) {
+  if (!c || !out) return ECG_ERR_ARG;
+  *out = nullptr;
+  ecg_diis* d = new (std::nothrow) ecg_diis();
+  if (!d) return ECG_ERR_OOM;
+  d->ctx = c;
+  int st = guarded(c, [&] {
+    need_system(*c);
+    if (len <= 0) throw Error(ECG_ERR_ARG, "len must be positive");
+    diis_reset(*c, d->st, maxdiis, resthr, len, false);
+    d->v = c->alloc(len, "diis vec");
+    d->r = c->alloc(len, "diis res");
+  });
+  if (st != ECG_OK) {
+    delete d;
+    return st;
+  }
+  *out = d;
+  return ECG_OK;
+}
+
+int ecg_diis_perform(ecg_diis* d, double* vec, const double* res) {
+  if (!d) return ECG_ERR_ARG;
+  Ctx* c = d->ctx;
+  return guarded(c, [&] {
+    need_ptr(vec, "vec");
+    need_ptr(res, "res");
+    check_finite(vec, d->st.len, "vec");
+    check_finite(res, d->st.len, "res");
+    check(dev::h2d(d->v, vec, d->st.len * 8, c->st), "h2d");
+    check(dev::h2d(d->r, res, d->st.len * 8, c->st), "h2d");
+    diis_perform(*c, d->st, d->v, d->r);
+    check(dev::d2h(vec, d->v, d->st.len * 8, c->st), "d2h");
+    check(dev::sync(c->st), "sync");
+  });
+}
+
+int ecg_diis_destroy(ecg_diis* d) {
+  delete d;  // device slots belong to the context and are freed with it
+  return ECG_OK;
+}
+
+int64_t ecg_kernel_launches(const ecg_ctx*) { return dev::launches(); }
+
+}  // extern "C"

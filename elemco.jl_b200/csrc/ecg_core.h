@@ -1,0 +1,105 @@
+// ecg_core.h — the context behind the C ABI: device-resident system,
+// amplitudes, DIIS history and workspace for one closed-shell CC problem.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/ecgpu.h"
+#include "ecg_dev.h"
+#include "ecg_tensor.h"
+
+namespace ecg {
+
+// Device DIIS history (src/solvers/diis.jl:34-72), vectors in HBM.
+struct DiisState {
+  int maxdiis = 6;
+  double resthr = 10.0;
+  int next = 0, ndim = 0;
+  int64_t len = 0;           // vector length
+  std::vector<double*> amp;  // device slots
+  std::vector<double*> res;
+  std::vector<double> bmat;  // (maxdiis+1)^2, row-major on host
+  bool cs = true;            // closed-shell custom dots vs plain dot
+};
+
+struct Ctx {
+  int device = 0;
+  dev::stream_t st = nullptr;
+  std::string err;
+  uint64_t memcap = 0, memused = 0;
+  std::vector<std::pair<void*, size_t>> allocs;
+  int prec = ECG_PREC_FP64;
+
+  // system
+  bool have_system = false;
+  int no = 0, nv = 0, nq = 0, n = 0;
+  double e0 = 0.0;
+  Extents ext;
+  // undressed DF factors, column-major blocks [p,q,Q]
+  double *Bvv = nullptr, *Bov = nullptr, *Bvo = nullptr, *Boo = nullptr;
+  double* h = nullptr;     // n x n
+  double* fock = nullptr;  // n x n
+  double* eps = nullptr;   // n
+  double* klcd = nullptr;  // [k,l,c,d] = <kl|cd>
+  double* Kvvoo = nullptr; // [a,b,i,j] = <ij|ab>
+  double* fvo_t = nullptr; // [a,i] = f[i,a]
+  std::vector<double> h_host, fock_host;
+
+  // dressed quantities
+  double *dBvv = nullptr, *dBvo = nullptr, *dBoo = nullptr, *dBvvT = nullptr;
+  double *dh = nullptr, *dfock = nullptr, *J = nullptr;
+
+  // amplitudes: T = [T1 (nv*no) | T2 (nv^2 no^2)], same for R
+  double *T = nullptr, *R = nullptr;
+  double* TT = nullptr;  // outer-product scratch nv^2 no^2
+
+  // device scalars + reduction scratch, pinned host mirror
+  double* dscal = nullptr;
+  double* red = nullptr;
+  double* hscal = nullptr;
+  double* dcoef = nullptr;
+
+  Arena ws;
+  double* ws_base = nullptr;
+
+  DiisState diis;
+  ecg_cc_opts opts;
+
+  // Lambda equations: U = [U1 | U2], RU its residual, vT = v_{mb}^{cd} T^{ij}_{cd}
+  double *U = nullptr, *RU = nullptr, *vT = nullptr;
+  double *D1 = nullptr, *dD1 = nullptr;  // n x n
+  bool lambda_ready = false;
+  DiisState ldiis;
+  int64_t n1() const { return (int64_t)nv * no; }
+  int64_t n2() const { return (int64_t)nv * nv * no * no; }
+  double* T1() { return T; }
+  double* T2() { return T + n1(); }
+  double* R1() { return R; }
+  double* R2() { return R + n1(); }
+
+  double* alloc(int64_t ndoubles, const char* what);
+  void release_to(size_t nallocs);  // free allocations made after the first nallocs
+  void ensure_ws(int64_t ndoubles);  // grow the workspace arena (outside any capture)
+  void free_all();
+  Contractor con() { return Contractor(st, &ws, &ext); }
+};
+
+// ecg_cc.cpp
+void setup_system(Ctx& c, int no, int nv, int nq, const double* B, const double* h1, double e0);
+void dress(Ctx& c, const double* T1);                // dressed B, h, Fock (cc.jl:453-815)
+void cc_residual(Ctx& c, bool dc);                   // R = residual(T)   (cc.jl:1343-1489)
+// R2 += sum_cd (sum_Q Bf[a,c,Q] Bf[b,d,Q]) T2[c,d,i,j];  BfT[d,b,Q] = Bf[b,d,Q]
+void ladder(Ctx& c, const double* Bf, const double* BfT, const double* T2, double* R2);
+struct IterResult {
+  double E, ESS, EOS, normR, dE, En;
+};
+void cc_init_iterations(Ctx& c, const ecg_cc_opts& o);
+IterResult cc_iteration(Ctx& c, bool dc);
+void diis_reset(Ctx& c, DiisState& d, int maxdiis, double resthr, int64_t len, bool cs);
+// DIIS perform on device vectors (src/solvers/diis.jl:246-305)
+void diis_perform(Ctx& c, DiisState& d, double* amps, const double* res);
+double scal(Ctx& c, int i);
+void sync_scalars(Ctx& c, int count);
+
+}  // namespace ecg

@@ -1,0 +1,183 @@
+"""Context object over the libecgpu C ABI (one GPU, one CUDA stream).
+
+Arrays are numpy float64 in the reference's index order and Fortran (column-
+major) layout, exactly what the Julia ``ccall`` glue passes.
+"""
+import ctypes as C
+
+import numpy as np
+
+from ._lib import (CcOpts, ECGError, ECG_PREC_FP64, as_f, dptr, fvec, lib)
+
+
+class Context:
+    """Device-resident closed-shell CC problem (``ecg_ctx``)."""
+
+    def __init__(self, device=0):
+        self._L = lib()
+        h = C.c_void_p()
+        st = self._L.ecg_create(int(device), C.byref(h))
+        if st:
+            raise ECGError(st, self._L.ecg_last_error(None).decode())
+        self._h = h
+        self.no = self.nv = self.nq = 0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.ecg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _chk(self, st):
+        if st:
+            raise ECGError(st, self._L.ecg_last_error(self._h).decode())
+
+    # ------------------------------------------------------------ setup
+    def set_mem_cap(self, nbytes):
+        self._chk(self._L.ecg_set_mem_cap(self._h, int(nbytes)))
+
+    def set_precision(self, prec=ECG_PREC_FP64):
+        self._chk(self._L.ecg_set_precision(self._h, int(prec)))
+
+    def set_system(self, B, h1, e0, nocc):
+        """B[p,q,Q] (n x n x nQ) DF factors, h1 (n x n), core energy e0."""
+        B = as_f(B)
+        h1 = as_f(h1)
+        n, n2, nq = B.shape
+        if n != n2 or h1.shape != (n, n):
+            raise ValueError("shape mismatch between B and h1")
+        self.no, self.nv, self.nq, self.n = int(nocc), n - int(nocc), nq, n
+        self._chk(self._L.ecg_set_system(self._h, self.no, self.nv, self.nq, dptr(B), dptr(h1),
+                                         float(e0)))
+
+    @staticmethod
+    def opts(**kw):
+        o = CcOpts()
+        lib().ecg_default_opts(C.byref(o))
+        for k, v in kw.items():
+            setattr(o, k, v)
+        return o
+
+    def _t(self):
+        return fvec((self.nv, self.no)), fvec((self.nv, self.nv, self.no, self.no))
+
+    # ------------------------------------------------------------ calls
+    def fock(self):
+        f = fvec((self.n, self.n))
+        eps = fvec(self.n)
+        e = C.c_double()
+        self._chk(self._L.ecg_fock(self._h, dptr(f), dptr(eps), C.byref(e)))
+        return f, eps, e.value
+
+    def mp2(self):
+        T1, T2 = self._t()
+        e = C.c_double()
+        self._chk(self._L.ecg_mp2(self._h, dptr(T1), dptr(T2), C.byref(e)))
+        return e.value, T1, T2
+
+    def cc_residual(self, T1, T2, dc=False):
+        T1, T2 = as_f(T1), as_f(T2)
+        R1, R2 = self._t()
+        self._chk(self._L.ecg_cc_residual(self._h, int(dc), dptr(T1), dptr(T2), dptr(R1),
+                                          dptr(R2)))
+        return R1, R2
+
+    def cc_solve(self, T1, T2, dc=False, opts=None):
+        T1, T2 = as_f(T1).copy(order="F"), as_f(T2).copy(order="F")
+        out = fvec(5)
+        it, conv = C.c_int32(), C.c_int32()
+        o = opts or self.opts()
+        self._chk(self._L.ecg_cc_solve(self._h, int(dc), C.byref(o), dptr(T1), dptr(T2),
+                                       dptr(out), C.byref(it), C.byref(conv)))
+        return {"E": out[0], "ESS": out[1], "EOS": out[2], "NormR": out[3], "dE": out[4],
+                "iterations": it.value, "converged": bool(conv.value), "T1": T1, "T2": T2}
+
+    def cc_load(self, T1=None, T2=None, opts=None):
+        o = opts or self.opts()
+        T1 = None if T1 is None else as_f(T1)
+        T2 = None if T2 is None else as_f(T2)
+        self._chk(self._L.ecg_cc_load(self._h, dptr(T1), dptr(T2), C.byref(o)))
+
+    def cc_step(self, dc=False, nsteps=1):
+        out = fvec(5)
+        self._chk(self._L.ecg_cc_step(self._h, int(dc), int(nsteps), dptr(out)))
+        return out
+
+    def cc_store(self, T1=None, T2=None):
+        if T1 is None:
+            T1, T2 = self._t()
+        self._chk(self._L.ecg_cc_store(self._h, dptr(T1), dptr(T2)))
+        return T1, T2
+
+    def pert_t(self, T1, T2):
+        T1, T2 = as_f(T1), as_f(T2)
+        e, eb = C.c_double(), C.c_double()
+        self._chk(self._L.ecg_pert_t(self._h, dptr(T1), dptr(T2), C.byref(e), C.byref(eb)))
+        return e.value, eb.value
+
+    def lambda_residual(self, T1, T2, U1, U2, dc=False):
+        R1, R2 = self._t()
+        self._chk(self._L.ecg_lambda_residual(self._h, int(dc), dptr(as_f(T1)), dptr(as_f(T2)),
+                                              dptr(as_f(U1)), dptr(as_f(U2)), dptr(R1),
+                                              dptr(R2)))
+        return R1, R2
+
+    def lambda_solve(self, T1, T2, dc=False, opts=None):
+        U1, U2 = self._t()
+        out = fvec(3)
+        it, conv = C.c_int32(), C.c_int32()
+        o = opts or self.opts()
+        self._chk(self._L.ecg_lambda_solve(self._h, int(dc), C.byref(o), dptr(as_f(T1)),
+                                           dptr(as_f(T2)), dptr(U1), dptr(U2), dptr(out),
+                                           C.byref(it), C.byref(conv)))
+        return {"U1": U1, "U2": U2, "norm": out[0], "NormR": out[1], "dnorm": out[2],
+                "iterations": it.value, "converged": bool(conv.value)}
+
+    def lambda_pert_t(self, T1, T2, U1, U2):
+        e, eb = C.c_double(), C.c_double()
+        self._chk(self._L.ecg_lambda_pert_t(self._h, dptr(as_f(T1)), dptr(as_f(T2)),
+                                            dptr(as_f(U1)), dptr(as_f(U2)), C.byref(e),
+                                            C.byref(eb)))
+        return e.value, eb.value
+
+    def one_rdm(self, T1, T2, U1, U2):
+        D1 = fvec((self.n, self.n))
+        dD1 = fvec((self.n, self.n))
+        self._chk(self._L.ecg_one_rdm(self._h, dptr(as_f(T1)), dptr(as_f(T2)), dptr(as_f(U1)),
+                                      dptr(as_f(U2)), dptr(D1), dptr(dD1)))
+        return D1, dD1
+
+    def kernel_launches(self):
+        return int(self._L.ecg_kernel_launches(self._h))
+
+
+class Diis:
+    """Stand-alone device DIIS (``ecg_diis_*``, plain dot products)."""
+
+    def __init__(self, ctx, length, maxdiis=6, resthr=10.0):
+        h = C.c_void_p()
+        ctx._chk(ctx._L.ecg_diis_create(ctx._h, int(maxdiis), float(resthr), int(length),
+                                        C.byref(h)))
+        self._ctx, self._h, self.length = ctx, h, int(length)
+
+    def perform(self, vec, res):
+        vec = np.ascontiguousarray(vec, dtype=np.float64).copy()
+        res = np.ascontiguousarray(res, dtype=np.float64)
+        self._ctx._chk(self._ctx._L.ecg_diis_perform(self._h, dptr(vec), dptr(res)))
+        return vec
+
+    def close(self):
+        if self._h:
+            self._ctx._L.ecg_diis_destroy(self._h)
+            self._h = None

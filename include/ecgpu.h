@@ -1,0 +1,145 @@
+/*
+ * ecgpu.h — C ABI of libecgpu.so, the B200 (sm_100a) closed-shell
+ * coupled-cluster library that stands in for ElemCo.jl's CCSD/DCSD, (T),
+ * Lambda and DIIS path.
+ *
+ * All arrays are column-major (Julia order, first index fastest), float64,
+ * host memory owned by the caller.  Orbitals are ordered occupied first
+ * (no of them), then virtual (nv); n = no + nv.  Every call returns an int
+ * status (ECG_OK = 0); on failure ecg_last_error() holds a message.  Calls on
+ * one context must not overlap (one host thread per context); each context
+ * owns one CUDA stream and its device memory.
+ *
+ * Reference interfaces each entry point replaces are cited as
+ * file:line inside the ElemCo.jl project.
+ */
+#ifndef ECGPU_H
+#define ECGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ECG_OK 0
+#define ECG_ERR_ARG 1        /* bad argument / shape mismatch                */
+#define ECG_ERR_CUDA 2       /* CUDA runtime error                           */
+#define ECG_ERR_OOM 3        /* device memory (or the context's cap) exhausted */
+#define ECG_ERR_NONFINITE 4  /* NaN/Inf detected in inputs or results        */
+#define ECG_ERR_TIMEOUT 5    /* a bounded device-side wait gave up           */
+#define ECG_ERR_STATE 6      /* call order violated (e.g. no system set)     */
+
+#define ECG_PREC_FP64 0      /* all-FP64 path                                 */
+#define ECG_PREC_MIXED 1     /* reduced-precision tensor-core products + FP64 refinement */
+
+typedef struct ecg_ctx ecg_ctx;
+
+/* Options of the iterative solvers; mirrors CcOptions/DiisOptions
+ * (src/infos/options.jl:128-282). */
+typedef struct ecg_cc_opts {
+  double thr;      /* squared residual norm threshold, default 1e-10 (options.jl:130) */
+  double conven;   /* energy threshold factor, default 0.1 (options.jl:132)           */
+  int32_t maxit;   /* default 50 (options.jl:134)                                     */
+  double shifts;   /* singles level shift, default 0.15 (options.jl:136)              */
+  double shiftp;   /* doubles level shift, default 0.2 (options.jl:138)               */
+  int32_t maxdiis; /* default 6 (options.jl:274)                                      */
+  double resthr;   /* default 10.0 (options.jl:276)                                   */
+} ecg_cc_opts;
+
+/* Fill *o with the reference defaults. */
+void ecg_default_opts(ecg_cc_opts* o);
+
+/* Context lifetime.  Replaces nothing in the reference (which has no device
+ * state); the Julia glue wraps it in a finalizer. */
+int ecg_create(int device, ecg_ctx** out);
+int ecg_destroy(ecg_ctx* ctx);
+const char* ecg_last_error(const ecg_ctx* ctx);
+/* Cap the context's device memory (bytes, 0 = no cap); exceeding it returns
+ * ECG_ERR_OOM.  Used to test the out-of-memory path without exhausting HBM. */
+int ecg_set_mem_cap(ecg_ctx* ctx, uint64_t bytes);
+int ecg_set_precision(ecg_ctx* ctx, int prec);
+
+/* Upload the system.  B[p,q,Q] (n x n x nq) are the density-fitting factors
+ * with (pq|rs) = sum_Q B[p,q,Q] B[r,s,Q] — the `mmL` file of
+ * src/integrals/dftools.jl:92-134 / decomptools.jl:22-52; h1 (n x n) the
+ * one-electron integrals and e0 the core energy (FDump int1/int0,
+ * src/integrals/dump.jl:107-128).  Replaces the int2 build of
+ * src/integrals/dfdump.jl:29-119 (the 4-index int2 is never formed). */
+int ecg_set_system(ecg_ctx* ctx, int32_t no, int32_t nv, int32_t nq,
+                   const double* B, const double* h1, double e0);
+
+/* Fock matrix (n x n), orbital energies (n) and HF energy:
+ * calc_fock_matrix / calc_HF_energy (src/cc/cctools.jl:35-78),
+ * gen_fock (src/scf/fockfactory.jl:27-30). */
+int ecg_fock(ecg_ctx* ctx, double* fock, double* eps, double* e_hf);
+
+/* MP2 start amplitudes T1 (nv x no), T2 (nv x nv x no x no) and energy:
+ * calc_MP2 (src/cc/cc.jl:1011-1024). */
+int ecg_mp2(ecg_ctx* ctx, double* T1, double* T2, double* e_mp2);
+
+/* One closed-shell CCSD (dc=0) or DCSD (dc=1) residual:
+ * calc_cc_resid (src/cc/cc.jl:1343-1489). */
+int ecg_cc_residual(ecg_ctx* ctx, int dc, const double* T1, const double* T2,
+                    double* R1, double* R2);
+
+/* Whole CC iteration loop on the device: cc_iterations! closed shell
+ * (src/cc/cc.jl:2518-2656) with update_singles!/update_doubles!
+ * (cctools.jl:265-300), DIIS perform! (src/solvers/diis.jl:246-305) and the
+ * energies (cc.jl:97-249).  T1/T2 hold the start guess on entry and the
+ * converged amplitudes on exit.  out[0] = Hylleraas correlation energy
+ * ("E"), out[1] = same-spin, out[2] = opposite-spin part, out[3] = last
+ * squared residual norm, out[4] = last energy change.  *iterations receives
+ * the iteration count; *converged 1/0. */
+int ecg_cc_solve(ecg_ctx* ctx, int dc, const ecg_cc_opts* opts, double* T1,
+                 double* T2, double* out, int32_t* iterations, int32_t* converged);
+
+/* Iteration-level interface used for benchmarking and for callers that keep
+ * the loop on the host: load amplitudes into the context's device state,
+ * run `nsteps` iterations of the cc_iterations! body (residual, Hylleraas
+ * energy, update, DIIS, energy), read the amplitudes back.  Host pointers may
+ * be NULL to skip the copy (device-resident amplitudes). */
+int ecg_cc_load(ecg_ctx* ctx, const double* T1, const double* T2, const ecg_cc_opts* opts);
+int ecg_cc_step(ecg_ctx* ctx, int dc, int32_t nsteps, double* out);
+int ecg_cc_store(ecg_ctx* ctx, double* T1, double* T2);
+
+/* Closed-shell (T) and [T]: calc_pertT_closed_shell
+ * (src/cc/cc_triples.jl:39-157). */
+int ecg_pert_t(ecg_ctx* ctx, const double* T1, const double* T2, double* e_t,
+               double* e_t_bracket);
+
+/* Lambda equations.  ecg_lambda_residual: calc_ccsd_vector_times_Jacobian
+ * closed shell (src/cc/cc_lagrange.jl:9-220) for multipliers U1/U2
+ * (contravariant, as in the reference) at amplitudes T1/T2.
+ * ecg_lambda_solve: lm_cc_iterations! (cc_lagrange.jl:1155-1223); U1/U2 are
+ * outputs.  ecg_lambda_pert_t: calc_ΛpertT_closed_shell
+ * (cc_triples.jl:159-295). */
+int ecg_lambda_residual(ecg_ctx* ctx, int dc, const double* T1, const double* T2,
+                        const double* U1, const double* U2, double* R1, double* R2);
+int ecg_lambda_solve(ecg_ctx* ctx, int dc, const ecg_cc_opts* opts, const double* T1,
+                     const double* T2, double* U1, double* U2, double* out,
+                     int32_t* iterations, int32_t* converged);
+int ecg_lambda_pert_t(ecg_ctx* ctx, const double* T1, const double* T2,
+                      const double* U1, const double* U2, double* e_t,
+                      double* e_t_bracket);
+
+/* One-particle density matrices D1 and T1-dressed dD1 (n x n):
+ * calc_1RDM closed shell (src/cc/cc_lagrange.jl:793-848). */
+int ecg_one_rdm(ecg_ctx* ctx, const double* T1, const double* T2,
+                const double* U1, const double* U2, double* D1, double* dD1);
+
+/* Stand-alone DIIS on device vectors of length len (src/solvers/diis.jl:34-305,
+ * plain dot).  Vectors are host arrays; the history stays on the device. */
+typedef struct ecg_diis ecg_diis;
+int ecg_diis_create(ecg_ctx* ctx, int32_t maxdiis, double resthr, int64_t len,
+                    ecg_diis** out);
+int ecg_diis_perform(ecg_diis* d, double* vec, const double* res);
+int ecg_diis_destroy(ecg_diis* d);
+
+/* Number of kernels this context has launched so far (diagnostics). */
+int64_t ecg_kernel_launches(const ecg_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ECGPU_H */
