@@ -5,6 +5,8 @@
 
 #include <atomic>
 #include <cstdio>
+#include <utility>
+#include <vector>
 
 #include "ecg_dev.h"
 
@@ -241,7 +243,52 @@ static int launch_gemm(const GemmArgs& g, int64_t batch, cudaStream_t st) {
   return launched();
 }
 
+// Event-pair pool for GEMM timing.
+static bool g_timing = false;
+static std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_ev;
+static size_t g_ev_used = 0;
+static double g_flops = 0.0;
+
+void gemm_timing(bool enable) {
+  g_timing = enable;
+  g_ev_used = 0;
+  g_flops = 0.0;
+}
+
+void gemm_time(double* ms, int64_t* n, double* flops) {
+  double tot = 0.0;
+  for (size_t i = 0; i < g_ev_used; ++i) {
+    cudaEventSynchronize(g_ev[i].second);
+    float t = 0.f;
+    cudaEventElapsedTime(&t, g_ev[i].first, g_ev[i].second);
+    tot += t;
+  }
+  if (ms) *ms = tot;
+  if (n) *n = (int64_t)g_ev_used;
+  if (flops) *flops = g_flops;
+  g_ev_used = 0;
+  g_flops = 0.0;
+}
+
+static int gemm_launch(stream_t s, const Gemm& q);
+
 int gemm_strided(stream_t s, const Gemm& q) {
+  if (!g_timing || q.m <= 0 || q.n <= 0 || q.batch <= 0 || q.k <= 0) return gemm_launch(s, q);
+  if (g_ev_used == g_ev.size()) {
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    g_ev.push_back({a, b});
+  }
+  auto& e = g_ev[g_ev_used++];
+  cudaEventRecord(e.first, (cudaStream_t)s);
+  int r = gemm_launch(s, q);
+  cudaEventRecord(e.second, (cudaStream_t)s);
+  g_flops += 2.0 * (double)q.m * (double)q.n * (double)q.k * (double)q.batch;
+  return r;
+}
+
+static int gemm_launch(stream_t s, const Gemm& q) {
   if (q.m <= 0 || q.n <= 0 || q.batch <= 0) return 0;
   cudaStream_t st = (cudaStream_t)s;
   if (q.k <= 0 || q.alpha == 0.0) {

@@ -1,6 +1,7 @@
 // ecg_api.cpp — extern "C" entry points of libecgpu (declared in
 // include/ecgpu.h).  Each call catches the library's exceptions and turns
 // them into a status code plus a per-context message.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <exception>
@@ -396,5 +397,109 @@ int ecg_diis_destroy(ecg_diis* d) {
 }
 
 int64_t ecg_kernel_launches(const ecg_ctx*) { return dev::launches(); }
+
+int ecg_cc_step_host(ecg_ctx* c, int dc, double* T1, double* T2, double* out) {
+  if (!c) return ECG_ERR_ARG;
+  return guarded(c, [&] {
+    need_system(*c);
+    if (c->diis.len == 0) throw Error(ECG_ERR_STATE, "call ecg_cc_load first");
+    if (T1 && T2) load_T(*c, T1, T2);
+    IterResult r = cc_iteration(*c, dc != 0);
+    if (T1) check(dev::d2h(T1, c->T1(), c->n1() * 8, c->st), "d2h T1");
+    if (T2) check(dev::d2h(T2, c->T2(), c->n2() * 8, c->st), "d2h T2");
+    check(dev::sync(c->st), "sync");
+    if (out) {
+      out[0] = r.E;
+      out[1] = r.ESS;
+      out[2] = r.EOS;
+      out[3] = r.normR;
+      out[4] = r.dE;
+    }
+  });
+}
+
+int ecg_get_stream(ecg_ctx* c, void** stream) {
+  if (!c || !stream) return ECG_ERR_ARG;
+  *stream = c->st;
+  return ECG_OK;
+}
+
+int ecg_set_gemm_timing(ecg_ctx* c, int enable) {
+  if (!c) return ECG_ERR_ARG;
+  dev::gemm_timing(enable != 0);
+  return ECG_OK;
+}
+
+int ecg_gemm_time(ecg_ctx* c, double* ms, int64_t* launches, double* flops) {
+  if (!c) return ECG_ERR_ARG;
+  return guarded(c, [&] {
+    check(dev::sync(c->st), "sync");
+    dev::gemm_time(ms, launches, flops);
+  });
+}
+
+int ecg_diag_gemm(ecg_ctx* c, char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha,
+                  const double* A, int64_t lda, const double* B, int64_t ldb, double beta,
+                  double* C, int64_t ldc) {
+  if (!c) return ECG_ERR_ARG;
+  return guarded(c, [&] {
+    need_ptr(A, "A");
+    need_ptr(B, "B");
+    need_ptr(C, "C");
+    if (m < 0 || n < 0 || k < 0) throw Error(ECG_ERR_ARG, "negative dimension");
+    const bool at = (ta == 'T' || ta == 't'), bt = (tb == 'T' || tb == 't');
+    const int64_t ar = at ? k : m, ac = at ? m : k, br = bt ? n : k, bc = bt ? k : n;
+    if (lda < std::max<int64_t>(1, ar) || ldb < std::max<int64_t>(1, br) ||
+        ldc < std::max<int64_t>(1, m))
+      throw Error(ECG_ERR_ARG, "leading dimension too small");
+    const size_t sA = lda * ac, sB = ldb * bc, sC = ldc * n;
+    size_t n0 = c->allocs.size();
+    struct Scope {
+      Ctx& c;
+      size_t n0;
+      ~Scope() { c.release_to(n0); }
+    } scope{*c, n0};
+    double* dA = c->alloc(sA, "diag A");
+    double* dB = c->alloc(sB, "diag B");
+    double* dC = c->alloc(sC, "diag C");
+    check(dev::h2d(dA, A, sA * 8, c->st), "h2d");
+    check(dev::h2d(dB, B, sB * 8, c->st), "h2d");
+    check(dev::h2d(dC, C, sC * 8, c->st), "h2d");
+    check(dev::gemm(c->st, ta, tb, m, n, k, alpha, dA, lda, dB, ldb, beta, dC, ldc), "gemm");
+    check(dev::d2h(C, dC, sC * 8, c->st), "d2h");
+    check(dev::sync(c->st), "sync");
+  });
+}
+
+int ecg_diag_permute(ecg_ctx* c, int nd, const int64_t* in_dims, const int* perm, double alpha,
+                     const double* in, double beta, double* out) {
+  if (!c) return ECG_ERR_ARG;
+  return guarded(c, [&] {
+    if (nd < 1 || nd > 8) throw Error(ECG_ERR_ARG, "rank must be 1..8");
+    need_ptr(in_dims, "in_dims");
+    need_ptr(perm, "perm");
+    int64_t total = 1;
+    bool seen[8] = {false};
+    for (int d = 0; d < nd; ++d) {
+      if (in_dims[d] < 0 || perm[d] < 0 || perm[d] >= nd || seen[perm[d]])
+        throw Error(ECG_ERR_ARG, "bad dims or permutation");
+      seen[perm[d]] = true;
+      total *= in_dims[d];
+    }
+    size_t n0 = c->allocs.size();
+    struct Scope {
+      Ctx& c;
+      size_t n0;
+      ~Scope() { c.release_to(n0); }
+    } scope{*c, n0};
+    double* di = c->alloc(total, "diag in");
+    double* dout = c->alloc(total, "diag out");
+    check(dev::h2d(di, in, total * 8, c->st), "h2d");
+    check(dev::h2d(dout, out, total * 8, c->st), "h2d");
+    check(dev::permute(c->st, nd, in_dims, perm, alpha, di, beta, dout), "permute");
+    check(dev::d2h(out, dout, total * 8, c->st), "d2h");
+    check(dev::sync(c->st), "sync");
+  });
+}
 
 }  // extern "C"

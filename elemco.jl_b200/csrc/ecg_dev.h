@@ -106,6 +106,10 @@ int triples_int(stream_t s, int nv, const double* X, const double* Mjk, const do
                 const double* Mij, const double* Njk, const double* Nik, const double* Nij,
                 double fac, double* IntX, double* IntY, int i, int j, int k);
 
+// GEMM event timing (process-wide): enable, then read and reset the totals.
+void gemm_timing(bool enable);
+void gemm_time(double* ms, int64_t* launches, double* flops);
+
 // Count of kernels launched through this layer in this process.
 int64_t launches();
 

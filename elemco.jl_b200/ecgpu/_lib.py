@@ -70,6 +70,15 @@ SIGNATURES = {
     "ecg_diis_perform": (C.c_int, [_P, _D, _D]),
     "ecg_diis_destroy": (C.c_int, [_P]),
     "ecg_kernel_launches": (C.c_int64, [_P]),
+    "ecg_cc_step_host": (C.c_int, [_P, C.c_int, _D, _D, _D]),
+    "ecg_get_stream": (C.c_int, [_P, C.POINTER(_P)]),
+    "ecg_set_gemm_timing": (C.c_int, [_P, C.c_int]),
+    "ecg_gemm_time": (C.c_int, [_P, _D, C.POINTER(C.c_int64), _D]),
+    "ecg_diag_gemm": (C.c_int, [_P, C.c_char, C.c_char, C.c_int64, C.c_int64, C.c_int64,
+                                C.c_double, _D, C.c_int64, _D, C.c_int64, C.c_double, _D,
+                                C.c_int64]),
+    "ecg_diag_permute": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int),
+                                   C.c_double, _D, C.c_double, _D]),
 }
 
 

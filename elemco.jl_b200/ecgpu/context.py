@@ -158,8 +158,48 @@ class Context:
                                       dptr(as_f(U2)), dptr(D1), dptr(dD1)))
         return D1, dD1
 
+    def cc_step_host(self, T1, T2, dc=False):
+        """One iteration with host amplitudes (updated in place)."""
+        out = fvec(5)
+        self._chk(self._L.ecg_cc_step_host(self._h, int(dc), dptr(T1), dptr(T2), dptr(out)))
+        return out
+
+    def stream(self):
+        p = C.c_void_p()
+        self._chk(self._L.ecg_get_stream(self._h, C.byref(p)))
+        return p.value
+
     def kernel_launches(self):
         return int(self._L.ecg_kernel_launches(self._h))
+
+    def set_gemm_timing(self, enable=True):
+        self._chk(self._L.ecg_set_gemm_timing(self._h, int(enable)))
+
+    def gemm_time(self):
+        ms, fl = C.c_double(), C.c_double()
+        n = C.c_int64()
+        self._chk(self._L.ecg_gemm_time(self._h, C.byref(ms), C.byref(n), C.byref(fl)))
+        return ms.value, n.value, fl.value
+
+    def diag_gemm(self, ta, tb, alpha, A, B, beta, Cm):
+        A, B = as_f(A), as_f(B)
+        Cm = as_f(Cm).copy(order="F")
+        m, n = Cm.shape
+        k = A.shape[0] if ta == "T" else A.shape[1]
+        self._chk(self._L.ecg_diag_gemm(self._h, ta.encode(), tb.encode(), m, n, k, float(alpha),
+                                        dptr(A), A.shape[0], dptr(B), B.shape[0], float(beta),
+                                        dptr(Cm), m))
+        return Cm
+
+    def diag_permute(self, x, perm, alpha=1.0, beta=0.0, out=None):
+        x = as_f(x)
+        dims = (C.c_int64 * x.ndim)(*x.shape)
+        pm = (C.c_int * x.ndim)(*perm)
+        oshape = tuple(x.shape[p] for p in perm)
+        out = fvec(oshape) if out is None else as_f(out).copy(order="F")
+        self._chk(self._L.ecg_diag_permute(self._h, x.ndim, dims, pm, float(alpha), dptr(x),
+                                           float(beta), dptr(out)))
+        return out
 
 
 class Diis:

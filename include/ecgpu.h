@@ -136,8 +136,40 @@ int ecg_diis_create(ecg_ctx* ctx, int32_t maxdiis, double resthr, int64_t len,
 int ecg_diis_perform(ecg_diis* d, double* vec, const double* res);
 int ecg_diis_destroy(ecg_diis* d);
 
-/* Number of kernels this context has launched so far (diagnostics). */
+/* One cc_iterations! body with host amplitudes: T1/T2 are uploaded (if
+ * non-NULL), one iteration runs with the DIIS history kept in the context
+ * (ecg_cc_load must have been called once), and the new amplitudes are
+ * written back.  out as in ecg_cc_step. */
+int ecg_cc_step_host(ecg_ctx* ctx, int dc, double* T1, double* T2, double* out);
+
+/* ------------------------------------------------------------------------
+ * Diagnostics and instrumentation (no counterpart in the reference).
+ * ---------------------------------------------------------------------- */
+
+/* The context's CUDA stream (a cudaStream_t), for callers that record their
+ * own events around library calls. */
+int ecg_get_stream(ecg_ctx* ctx, void** stream);
+
+/* Number of kernels launched through the library in this process so far. */
 int64_t ecg_kernel_launches(const ecg_ctx* ctx);
+
+/* GEMM timing: when enabled, every FP64 GEMM launch of this process is
+ * bracketed by CUDA events on its stream; ecg_gemm_time returns the summed
+ * device milliseconds, the launch count and the summed 2*m*n*k*batch flops
+ * since the last reset, and resets them. */
+int ecg_set_gemm_timing(ecg_ctx* ctx, int enable);
+int ecg_gemm_time(ecg_ctx* ctx, double* ms, int64_t* launches, double* flops);
+
+/* The library's FP64 GEMM / permutation on host buffers (column-major),
+ * for self-tests of the device kernels:
+ * C = alpha op(A) op(B) + beta C  with op 'N' or 'T'. */
+int ecg_diag_gemm(ecg_ctx* ctx, char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha,
+                  const double* A, int64_t lda, const double* B, int64_t ldb, double beta,
+                  double* C, int64_t ldc);
+/* out = alpha permute(in) + beta out, in of rank nd with dims in_dims; out
+ * dimension d is input dimension perm[d]. */
+int ecg_diag_permute(ecg_ctx* ctx, int nd, const int64_t* in_dims, const int* perm, double alpha,
+                     const double* in, double beta, double* out);
 
 #ifdef __cplusplus
 }

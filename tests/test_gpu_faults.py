@@ -1,0 +1,68 @@
+"""Failure paths of the C ABI, injected on the host: every error is a status
+code plus message and leaves the context usable.  Nothing here faults,
+traps or hangs the GPU."""
+import numpy as np
+import pytest
+
+import ecgpu
+from ecgpu._lib import (ECG_ERR_ARG, ECG_ERR_NONFINITE, ECG_ERR_OOM, ECG_ERR_STATE)
+
+pytestmark = pytest.mark.gpu
+
+
+def test_call_before_system_is_state_error():
+    with ecgpu.Context(0) as c:
+        c.no, c.nv, c.n = 2, 3, 5
+        with pytest.raises(ecgpu.ECGError) as e:
+            c.mp2()
+        assert e.value.code == ECG_ERR_STATE
+
+
+def test_nonfinite_inputs(h2o_df):
+    B, S = h2o_df
+    with ecgpu.Context(0) as c:
+        Bbad = B.copy(order="F")
+        Bbad[1, 2, 3] = np.nan
+        with pytest.raises(ecgpu.ECGError) as e:
+            c.set_system(Bbad, S.h, S.e0, S.no)
+        assert e.value.code == ECG_ERR_NONFINITE
+        c.set_system(B, S.h, S.e0, S.no)
+        _, T1, T2 = c.mp2()
+        T2[0, 0, 0, 0] = np.inf
+        with pytest.raises(ecgpu.ECGError) as e:
+            c.cc_residual(T1, T2)
+        assert e.value.code == ECG_ERR_NONFINITE
+        T2[0, 0, 0, 0] = 0.0
+        R1, R2 = c.cc_residual(T1, T2)  # still usable
+        assert np.isfinite(R2).all()
+
+
+def test_memory_cap_is_oom(h2o_df):
+    B, S = h2o_df
+    with ecgpu.Context(0) as c:
+        c.set_mem_cap(1 << 16)
+        with pytest.raises(ecgpu.ECGError) as e:
+            c.set_system(B, S.h, S.e0, S.no)
+        assert e.value.code == ECG_ERR_OOM
+        c.set_mem_cap(0)
+        c.set_system(B, S.h, S.e0, S.no)
+        assert np.isfinite(c.mp2()[0])
+
+
+def test_bad_arguments(h2o_df):
+    B, S = h2o_df
+    with ecgpu.Context(0) as c:
+        with pytest.raises(ecgpu.ECGError) as e:
+            c.set_system(B, S.h, S.e0, 0)
+        assert e.value.code == ECG_ERR_ARG
+        c.set_system(B, S.h, S.e0, S.no)
+        _, T1, T2 = c.mp2()
+        with pytest.raises(ecgpu.ECGError) as e:
+            c.cc_solve(T1, T2, opts=c.opts(maxdiis=0))
+        assert e.value.code == ECG_ERR_ARG
+        with pytest.raises(ecgpu.ECGError) as e:
+            c.set_precision(7)
+        assert e.value.code == ECG_ERR_ARG
+        with pytest.raises(ecgpu.ECGError) as e:
+            c.diag_permute(np.zeros((2, 2)), (0, 0))
+        assert e.value.code == ECG_ERR_ARG

@@ -1,0 +1,203 @@
+"""Parity of the CUDA path (libecgpu through its C ABI) with the oracle.
+
+FP64 throughout; tolerances: residuals and densities 1e-11 absolute
+(summation-order differences only), energies 1e-10 Eh against the oracle on
+the same trajectory, and the reference's pinned energies as in
+tests/test_oracle_golden.py.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _perturbed(S, f, seed=0, amp=0.01):
+    rng = np.random.default_rng(seed)
+    _, T1, T2 = O.mp2(S, f)
+    T1 = T1 + amp * rng.standard_normal(T1.shape)
+    X = amp * rng.standard_normal(T2.shape)
+    return T1, T2 + X + X.transpose(1, 0, 3, 2)
+
+
+@pytest.mark.parametrize("ta", ["N", "T"])
+@pytest.mark.parametrize("tb", ["N", "T"])
+@pytest.mark.parametrize("m,n,k", [(1, 1, 1), (7, 5, 3), (64, 64, 16), (129, 65, 33),
+                                   (300, 200, 150), (520, 384, 96)])
+def test_gemm_kernel(ctx, ta, tb, m, n, k):
+    rng = np.random.default_rng(m * 1000 + n * 10 + k)
+    A = rng.standard_normal((k, m) if ta == "T" else (m, k))
+    B = rng.standard_normal((n, k) if tb == "T" else (k, n))
+    C = rng.standard_normal((m, n))
+    ref = 0.7 * ((A.T if ta == "T" else A) @ (B.T if tb == "T" else B)) - 0.3 * C
+    out = ctx.diag_gemm(ta, tb, 0.7, A, B, -0.3, C)
+    assert np.abs(out - ref).max() < 1e-12 * max(1, k)
+
+
+@pytest.mark.parametrize("shape,perm", [((5, 7, 3, 4), (1, 0, 3, 2)), ((40, 33, 9), (2, 0, 1)),
+                                        ((64, 64, 8, 8), (0, 3, 1, 2)), ((3, 70, 50), (0, 2, 1)),
+                                        ((100,), (0,))])
+def test_permute_kernel(ctx, shape, perm):
+    rng = np.random.default_rng(1)
+    x = np.asfortranarray(rng.standard_normal(shape))
+    y = np.asfortranarray(rng.standard_normal(tuple(shape[p] for p in perm)))
+    out = ctx.diag_permute(x, perm, 2.0, -1.0, y)
+    assert np.abs(out - (2.0 * np.transpose(x, perm) - y)).max() < 1e-14
+
+
+@pytest.fixture(scope="module")
+def sys_h2o(ctx, h2o_df):
+    B, S = h2o_df
+    ctx.set_system(B, S.h, S.e0, S.no)
+    return S, O.gen_fock(S)
+
+
+def test_fock_hf_mp2(ctx, sys_h2o):
+    S, f = sys_h2o
+    fg, eps, ehf = ctx.fock()
+    assert np.abs(fg - f).max() < 1e-13
+    assert abs(ehf - O.hf_energy(S, f)) < 1e-12
+    e, T1, T2 = ctx.mp2()
+    eo, T1o, T2o = O.mp2(S, f)
+    assert abs(e - eo) < 1e-13
+    assert np.abs(T1 - T1o).max() < 1e-14 and np.abs(T2 - T2o).max() < 1e-14
+
+
+@pytest.mark.parametrize("dc", [False, True])
+def test_cc_residual(ctx, sys_h2o, dc):
+    S, f = sys_h2o
+    T1, T2 = _perturbed(S, f)
+    R1, R2 = ctx.cc_residual(T1, T2, dc=dc)
+    R1o, R2o = O.cc_resid(S, T1, T2, dc=dc)
+    assert np.abs(R1 - R1o).max() < 1e-12
+    assert np.abs(R2 - R2o).max() < 1e-12
+
+
+@pytest.mark.parametrize("dc", [False, True])
+def test_cc_solve_matches_oracle(ctx, sys_h2o, dc):
+    S, f = sys_h2o
+    e, T1, T2 = ctx.mp2()
+    r = ctx.cc_solve(T1, T2, dc=dc)
+    Eo, T1o, T2o, it, conv = O.cc_iterations(S, *O.mp2(S, f)[1:], f, dc=dc)
+    assert r["converged"] and conv and r["iterations"] == it
+    assert abs(r["E"] - Eo) < 1e-10
+    assert np.abs(r["T2"] - T2o).max() < 1e-9
+
+
+def test_pert_t(ctx, sys_h2o):
+    S, f = sys_h2o
+    e, T1, T2 = ctx.mp2()
+    r = ctx.cc_solve(T1, T2)
+    et, etb = ctx.pert_t(r["T1"], r["T2"])
+    eto, etbo = O.pert_t(S, r["T1"], r["T2"], f)
+    assert abs(et - eto) < 1e-12 and abs(etb - etbo) < 1e-12
+
+
+@pytest.mark.parametrize("dc", [False, True])
+def test_lambda_residual_and_rdm(ctx, sys_h2o, dc):
+    S, f = sys_h2o
+    T1, T2 = _perturbed(S, f, seed=5)
+    rng = np.random.default_rng(7)
+    U1 = rng.standard_normal(T1.shape)
+    Y = rng.standard_normal(T2.shape)
+    U2 = Y + Y.transpose(1, 0, 3, 2)
+    R1, R2 = ctx.lambda_residual(T1, T2, U1, U2, dc=dc)
+    dr = O.dressed_ints(S, T1)
+    o, v = S.sl["o"], S.sl["v"]
+    vT = np.einsum("bmdc,dcji->mbij", dr[0][v, o, v, v], T2)
+    R1o, R2o = O.vector_times_jacobian(S, U1, U2, T1, T2, f, dr, vT, dc=dc)
+    assert np.abs(R1 - R1o).max() < 1e-11 * max(1, np.abs(R1o).max())
+    assert np.abs(R2 - R2o).max() < 1e-11 * max(1, np.abs(R2o).max())
+    D1, dD1 = ctx.one_rdm(T1, T2, U1, U2)
+    D1o, dD1o = O.one_rdm(S, U1, U2, T1, T2)
+    assert np.abs(D1 - D1o).max() < 1e-12 and np.abs(dD1 - dD1o).max() < 1e-12
+
+
+def test_lambda_solve_and_lambda_t(ctx, sys_h2o):
+    S, f = sys_h2o
+    e, T1, T2 = ctx.mp2()
+    r = ctx.cc_solve(T1, T2)
+    lr = ctx.lambda_solve(r["T1"], r["T2"])
+    U1o, U2o, lit, lconv = O.lambda_iterations(S, r["T1"], r["T2"], f)
+    assert lr["converged"] and lr["iterations"] == lit
+    assert np.abs(lr["U2"] - U2o).max() < 1e-9 and np.abs(lr["U1"] - U1o).max() < 1e-9
+    e1, e1b = ctx.lambda_pert_t(r["T1"], r["T2"], lr["U1"], lr["U2"])
+    e1o, e1bo = O.lambda_pert_t(S, r["T1"], r["T2"], U1o, U2o, f)
+    assert abs(e1 - e1o) < 1e-11 and abs(e1b - e1bo) < 1e-11
+
+
+def test_driver_reproduces_reference_pins(h2o, gold, tmp_path):
+    """ccdriver on the reference's H2O.FCIDUMP integrals (through Cholesky
+    factors) against test/h2o.jl's pinned energies."""
+    from ecgpu.driver import ECInfo, FDump, ccdriver
+    g = gold["h2o"]
+    EC = ECInfo(scr=str(tmp_path))
+    EC.fd = FDump(h2o.h, h2o.e0, 2 * h2o.no, V=h2o.V)
+    e = ccdriver(EC, "ccsd(t)")
+    assert abs(e["HF"] - g["HF"]) < 1e-9
+    assert abs(e["MP2c"] - g["MP2c"]) < 1e-9
+    assert abs(e["CCSD(T)c"] - g["CCSD(T)c"]) < 1e-6
+    ref = O.ccdriver(h2o, "ccsd(t)")
+    assert abs(e["CCSD(T)c"] - ref["CCSD(T)c"]) < 1e-9
+    e = ccdriver(EC, "λccsd(t)")
+    assert abs(e["ΛCCSD(T)c"] - g["LCCSD(T)c"]) < 1e-6
+    EC.set("cc", thr=1e-20, conven=1e-4, maxit=60)
+    e = ccdriver(EC, "dcsd")
+    assert abs(e["DCSDc"] - g["DCSDc"]) < 1e-9
+    assert (tmp_path / "cc_amplitudes_2.bin").exists()
+
+
+def test_synthetic_water_dimer_ccsd_t(ctx):
+    """(H2O)_2/cc-pVDZ-sized synthetic system: full CCSD(T) vs the oracle."""
+    from ecgpu.synthetic import make_workload
+    B, h1, e0, no = make_workload("h2o2_vdz")
+    S = O.System.from_df(np.transpose(B, (2, 0, 1)), h1, e0, no)
+    f = O.gen_fock(S)
+    ctx.set_system(B, h1, e0, no)
+    T1, T2 = _perturbed(S, f, seed=11)
+    for dc in (False, True):
+        R1, R2 = ctx.cc_residual(T1, T2, dc=dc)
+        R1o, R2o = O.cc_resid(S, T1, T2, dc=dc)
+        assert np.abs(R1 - R1o).max() < 1e-11 and np.abs(R2 - R2o).max() < 1e-11
+    e, T1, T2 = ctx.mp2()
+    r = ctx.cc_solve(T1, T2)
+    Eo, T1o, T2o, it, conv = O.cc_iterations(S, *O.mp2(S, f)[1:], f)
+    assert r["iterations"] == it and abs(r["E"] - Eo) < 1e-10
+    et, _ = ctx.pert_t(r["T1"], r["T2"])
+    eto, _ = O.pert_t(S, r["T1"], r["T2"], f)
+    assert abs(et - eto) < 1e-11
+
+
+def test_deterministic(ctx, h2o_df):
+    B, S = h2o_df
+    ctx.set_system(B, S.h, S.e0, S.no)
+    out = []
+    for _ in range(2):
+        e, T1, T2 = ctx.mp2()
+        r = ctx.cc_solve(T1, T2)
+        out.append((r["E"], ctx.pert_t(r["T1"], r["T2"])))
+    assert out[0] == out[1]
+
+
+def test_diis_standalone(ctx, h2o_df):
+    """ecg_diis_* against the oracle's DIIS on a linear fixed-point problem."""
+    import ecgpu
+    B, S = h2o_df
+    ctx.set_system(B, S.h, S.e0, S.no)
+    rng = np.random.default_rng(2)
+    n = 50
+    A = np.eye(n) + 0.1 * rng.standard_normal((n, n))
+    b = rng.standard_normal(n)
+    d = ecgpu.Diis(ctx, n, maxdiis=4)
+    od = O.Diis(4, 10.0, dots=None)
+    x = np.zeros(n)
+    xo = np.zeros(n)
+    for _ in range(8):
+        r = A @ x - b
+        x = d.perform(x - 0.5 * r, r)
+        ro = A @ xo - b
+        vec = [xo - 0.5 * ro]
+        od.perform(vec, [ro])
+        xo = vec[0]
+        assert np.abs(x - xo).max() < 1e-10
