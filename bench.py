@@ -321,7 +321,7 @@ def main():
                      "step_frac": F / (total / a.steps / 1000.0) / 1e12 / fp64_peak},
         "clocks": clk,
     }
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and a.cpu_sample > 0:
         rate, dt = cpu_ccsd_rate(no, nv, nq, dc, a.cpu_sample)
         line["cpu_baseline"] = {"value": rate, "unit": "iter/s", "cores": host_cores(),
                                 "kind": "port",

@@ -3,6 +3,7 @@
 // amplitude updates and deterministic reductions.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstdio>
 #include <utility>
@@ -88,6 +89,7 @@ struct GemmArgs {
   int64_t sam, sak, sab, sbk, sbn, sbb, scm, scn, scb;
   double alpha, beta;
   int a_kfast, b_nfast;  // loader thread order follows the unit-stride index
+  int64_t klast;         // split-K: depth of the last z-slice (0 = all slices use k)
 };
 
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool pred) {
@@ -108,7 +110,7 @@ __device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
       : "d"(a), "d"(b));
 }
 
-template <int BM, int BN, int BK, int WM, int WN, int STAGES>
+template <int BM, int BN, int BK, int WM, int WN, int STAGES, int MINB = 1>
 struct GemmCfg {
   static constexpr int WARPS_M = BM / WM;
   static constexpr int WARPS_N = BN / WN;
@@ -120,8 +122,8 @@ struct GemmCfg {
   static constexpr size_t SMEM = (size_t)STAGES * (A_STAGE + B_STAGE) * sizeof(double);
 };
 
-template <int BM, int BN, int BK, int WM, int WN, int STAGES>
-__global__ void __launch_bounds__(GemmCfg<BM, BN, BK, WM, WN, STAGES>::THREADS)
+template <int BM, int BN, int BK, int WM, int WN, int STAGES, int MINB>
+__global__ void __launch_bounds__(GemmCfg<BM, BN, BK, WM, WN, STAGES>::THREADS, MINB)
     dgemm_kernel(GemmArgs g) {
   using Cfg = GemmCfg<BM, BN, BK, WM, WN, STAGES>;
   constexpr int NT = Cfg::THREADS;
@@ -141,7 +143,8 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, BK, WM, WN, STAGES>::THREADS)
   const int wm0 = (warp % Cfg::WARPS_M) * WM;
   const int wn0 = (warp / Cfg::WARPS_M) * WN;
   const int gq = lane >> 2, tq = lane & 3;
-  const int64_t KT = (g.k + BK - 1) / BK;
+  const int64_t kdep = (g.klast > 0 && bz == (int64_t)gridDim.z - 1) ? g.klast : g.k;
+  const int64_t KT = (kdep + BK - 1) / BK;
 
   auto load_tile = [&](int stage, int64_t kt) {
     const int64_t k0 = kt * BK;
@@ -154,7 +157,7 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, BK, WM, WN, STAGES>::THREADS)
         int mm, kk;
         if (!g.a_kfast) { mm = e % BM; kk = e / BM; } else { kk = e % BK; mm = e / BK; }
         int64_t gm = m0 + mm, gk = k0 + kk;
-        bool ok = gm < g.m && gk < g.k;
+        bool ok = gm < g.m && gk < kdep;
         const double* src = ok ? A + gm * g.sam + gk * g.sak : A;
         cp_async8(as + kk * Cfg::LDA_S + mm, src, ok);
       }
@@ -166,7 +169,7 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, BK, WM, WN, STAGES>::THREADS)
         int nn, kk;
         if (!g.b_nfast) { kk = e % BK; nn = e / BK; } else { nn = e % BN; kk = e / BN; }
         int64_t gn = n0 + nn, gk = k0 + kk;
-        bool ok = gn < g.n && gk < g.k;
+        bool ok = gn < g.n && gk < kdep;
         const double* src = ok ? B + gk * g.sbk + gn * g.sbn : B;
         cp_async8(bs + kk * Cfg::LDB_S + nn, src, ok);
       }
@@ -227,20 +230,56 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, BK, WM, WN, STAGES>::THREADS)
   }
 }
 
-template <int BM, int BN, int BK, int WM, int WN, int STAGES>
+template <int BM, int BN, int BK, int WM, int WN, int STAGES, int MINB = 1>
 static int launch_gemm(const GemmArgs& g, int64_t batch, cudaStream_t st) {
   using Cfg = GemmCfg<BM, BN, BK, WM, WN, STAGES>;
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(dgemm_kernel<BM, BN, BK, WM, WN, STAGES>,
+    cudaFuncSetAttribute(dgemm_kernel<BM, BN, BK, WM, WN, STAGES, MINB>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
     attr = true;
   }
   int64_t gx = (g.m + BM - 1) / BM, gy = (g.n + BN - 1) / BN;
   if (gy > 65535 || batch > 65535) return (int)cudaErrorInvalidConfiguration;
   dim3 grid((unsigned)gx, (unsigned)gy, (unsigned)batch);
-  dgemm_kernel<BM, BN, BK, WM, WN, STAGES><<<grid, Cfg::THREADS, Cfg::SMEM, st>>>(g);
+  dgemm_kernel<BM, BN, BK, WM, WN, STAGES, MINB><<<grid, Cfg::THREADS, Cfg::SMEM, st>>>(g);
   return launched();
+}
+
+static unsigned grid_for(int64_t n, int threads = 256, int64_t cap = 148 * 16);
+
+// Device scratch for split-K partial products (grown on demand; cudaFree of
+// the old buffer synchronises the device, so no kernel still uses it).
+static double* g_splitk = nullptr;
+static size_t g_splitk_len = 0;
+static double* splitk_buffer(size_t n) {
+  if (n > g_splitk_len) {
+    if (g_splitk) cudaFree(g_splitk);
+    g_splitk = nullptr;
+    g_splitk_len = 0;
+    size_t want = std::max(n, (size_t)1 << 22);
+    if (cudaMalloc(&g_splitk, want * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    g_splitk_len = want;
+  }
+  return g_splitk;
+}
+
+__global__ void splitk_reduce_kernel(int64_t m, int64_t n, int S, const double* __restrict__ P,
+                                     double alpha, double beta, double* C, int64_t scm,
+                                     int64_t scn) {
+  const int64_t total = m * n;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (int z = 0; z < S; ++z) acc += P[z * total + idx];
+    double* c = C + (idx % m) * scm + (idx / m) * scn;
+    double v = alpha * acc;
+    if (beta != 0.0) v += beta * *c;
+    *c = v;
+  }
 }
 
 // Event-pair pool for GEMM timing.
@@ -305,10 +344,40 @@ static int gemm_launch(stream_t s, const Gemm& q) {
   }
   GemmArgs g{q.A, q.B, q.C, q.m, q.n, q.k, q.sam, q.sak, q.sab, q.sbk, q.sbn, q.sbb,
              q.scm, q.scn, q.scb, q.alpha, q.beta, (q.sam != 1 && q.sak == 1) ? 1 : 0,
-             (q.sbk != 1 && q.sbn == 1) ? 1 : 0};
-  int64_t big_tiles = ((q.m + 127) / 128) * ((q.n + 127) / 128) * q.batch;
-  if (big_tiles >= 2 * 148) return launch_gemm<128, 128, 16, 64, 32, 3>(g, q.batch, st);
-  return launch_gemm<64, 64, 16, 32, 32, 3>(g, q.batch, st);
+             (q.sbk != 1 && q.sbn == 1) ? 1 : 0, 0};
+  // Split-K for GEMMs whose output covers too few tiles to fill the SMs:
+  // each z-slice writes a partial product, a fixed-order reduction sums them.
+  const int64_t tiles64 = ((q.m + 63) / 64) * ((q.n + 63) / 64);
+  if (q.batch == 1 && tiles64 < 148 && q.k >= 512) {
+    int64_t S = std::min<int64_t>((2 * 148 + tiles64 - 1) / tiles64, q.k / 256);
+    S = std::max<int64_t>(2, std::min<int64_t>(S, 64));
+    int64_t kc = (q.k + S - 1) / S;
+    kc = (kc + 15) / 16 * 16;
+    S = (q.k + kc - 1) / kc;
+    double* P = splitk_buffer((size_t)S * q.m * q.n);
+    if (!P) return (int)cudaErrorMemoryAllocation;
+    GemmArgs h = g;
+    h.k = kc;
+    h.klast = q.k - (S - 1) * kc;
+    h.sab = kc * q.sak;
+    h.sbb = kc * q.sbk;
+    h.C = P;
+    h.scm = 1;
+    h.scn = q.m;
+    h.scb = q.m * q.n;
+    h.alpha = 1.0;
+    h.beta = 0.0;
+    int e = launch_gemm<64, 64, 16, 32, 32, 3, 3>(h, S, st);
+    if (e) return e;
+    int64_t total = q.m * q.n;
+    splitk_reduce_kernel<<<grid_for(total), 256, 0, st>>>(q.m, q.n, (int)S, P, q.alpha, q.beta,
+                                                          q.C, q.scm, q.scn);
+    return launched();
+  }
+  // 64x64 tiles, 4 warps of 32x32, 3 CTAs per SM: the best of the measured
+  // configurations on both the small (o^3 v^3 at o=16, v=76) and the large
+  // (8192^3, 7632^3) shapes on B200.
+  return launch_gemm<64, 64, 16, 32, 32, 3, 3>(g, q.batch, st);
 }
 
 int gemm(stream_t s, char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha,
@@ -442,7 +511,7 @@ __global__ void axpby_kernel(int64_t n, double alpha, const double* x, double be
   }
 }
 
-static unsigned grid_for(int64_t n, int threads = 256, int64_t cap = 148 * 16) {
+static unsigned grid_for(int64_t n, int threads, int64_t cap) {
   int64_t b = (n + threads - 1) / threads;
   if (b < 1) b = 1;
   if (b > cap) b = cap;
@@ -655,6 +724,93 @@ int combine(stream_t s, int64_t n, int m, const double* const* X, const double* 
   CombineArgs a{};
   for (int k = 0; k < m; ++k) a.X[k] = X[k];
   combine_kernel<<<grid_for(n), 256, 0, (cudaStream_t)s>>>(n, m, a, coef, out);
+  return launched();
+}
+
+// ---------------------------------------------------------------- ladder
+
+__global__ void ladder_pack_t_kernel(int nv, int no, const double* __restrict__ T,
+                                     const int2* __restrict__ cdp, const int2* __restrict__ ijp,
+                                     double* __restrict__ Ts, double* __restrict__ Ta) {
+  const int64_t v = nv, o = no, ncdp = v * (v + 1) / 2, ncdm = v * (v - 1) / 2;
+  const int64_t nijp = o * (o + 1) / 2, total = ncdp * nijp;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = idx % ncdp, q = idx / ncdp;
+    const int2 cd = cdp[k], ij = ijp[q];
+    const int64_t ij0 = v * v * (ij.x + o * ij.y);
+    const double x = T[cd.x + v * cd.y + ij0], y = T[cd.y + v * cd.x + ij0];
+    Ts[idx] = 0.5 * (x + y);
+    if (cd.x < cd.y && ij.x < ij.y) Ta[(k - cd.y) + ncdm * (q - ij.y)] = 0.5 * (x - y);
+  }
+}
+
+int ladder_pack_t(stream_t s, int nv, int no, const double* T2, const int* cdp, const int* ijp,
+                  double* Ts, double* Ta) {
+  int64_t total = (int64_t)nv * (nv + 1) / 2 * ((int64_t)no * (no + 1) / 2);
+  ladder_pack_t_kernel<<<grid_for(total), 256, 0, (cudaStream_t)s>>>(
+      nv, no, T2, (const int2*)cdp, (const int2*)ijp, Ts, Ta);
+  return launched();
+}
+
+__global__ void ladder_pack_v_kernel(int nv, int a0, int na, int npairs,
+                                     const int2* __restrict__ pairs, const int2* __restrict__ cdp,
+                                     const double* __restrict__ V, double* __restrict__ Vp,
+                                     double* __restrict__ Vm) {
+  const int64_t v = nv, ncdp = v * (v + 1) / 2, ncdm = v * (v - 1) / 2, total = ncdp * npairs;
+  const int64_t lda = v * na;  // Vblk[c + v a' + v na (d + v b'')]
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = idx % ncdp, pr = idx / ncdp;
+    const int2 cd = cdp[k], ab = pairs[pr];
+    const int64_t ap = ab.x - a0, bp = ab.y - a0;
+    const double x = V[cd.x + v * ap + lda * (cd.y + v * bp)];
+    const double y = V[cd.y + v * ap + lda * (cd.x + v * bp)];
+    Vp[idx] = (cd.x == cd.y) ? x : x + y;
+    if (cd.x < cd.y && ab.x < ab.y) Vm[(k - cd.y) + ncdm * (pr - ap - 1)] = x - y;
+  }
+}
+
+int ladder_pack_v(stream_t s, int nv, int a0, int na, int npairs, const int* pairs,
+                  const int* cdp, const double* Vblk, double* Vp, double* Vm) {
+  int64_t total = (int64_t)nv * (nv + 1) / 2 * npairs;
+  ladder_pack_v_kernel<<<grid_for(total), 256, 0, (cudaStream_t)s>>>(
+      nv, a0, na, npairs, (const int2*)pairs, (const int2*)cdp, Vblk, Vp, Vm);
+  return launched();
+}
+
+__global__ void ladder_unpack_kernel(int nv, int no, int a0, int npairs,
+                                     const int2* __restrict__ pairs, const int2* __restrict__ ijp,
+                                     const double* __restrict__ Lp, const double* __restrict__ Lm,
+                                     double* __restrict__ R2) {
+  const int64_t v = nv, o = no, nijp = o * (o + 1) / 2, total = (int64_t)npairs * nijp;
+  int64_t npm = 0;  // minus pairs of this block = npairs - na' where na' = #a in block
+  {
+    // count of a values in the block = number of pairs with a == b
+    // (pairs with b == a are the first of each a); derived from the last pair
+    const int2 last = pairs[npairs - 1];
+    npm = npairs - (last.x - a0 + 1);
+  }
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t pr = idx % npairs, q = idx / npairs;
+    const int2 ab = pairs[pr], ij = ijp[q];
+    const double p = Lp[idx];
+    double m = 0.0;
+    if (ab.x < ab.y && ij.x < ij.y) m = Lm[(pr - (ab.x - a0) - 1) + npm * (q - ij.y)];
+    const int64_t a = ab.x, b = ab.y, i = ij.x, j = ij.y;
+    R2[a + v * b + v * v * (i + o * j)] += p + m;
+    if (a != b) R2[b + v * a + v * v * (i + o * j)] += p - m;
+    if (i != j) R2[a + v * b + v * v * (j + o * i)] += p - m;
+    if (a != b && i != j) R2[b + v * a + v * v * (j + o * i)] += p + m;
+  }
+}
+
+int ladder_unpack(stream_t s, int nv, int no, int a0, int npairs, const int* pairs,
+                  const int* ijp, const double* Lp, const double* Lm, double* R2) {
+  int64_t total = (int64_t)npairs * ((int64_t)no * (no + 1) / 2);
+  ladder_unpack_kernel<<<grid_for(total), 256, 0, (cudaStream_t)s>>>(
+      nv, no, a0, npairs, (const int2*)pairs, (const int2*)ijp, Lp, Lm, R2);
   return launched();
 }
 

@@ -74,12 +74,50 @@ void sync_scalars(Ctx& c, int count) {
 
 // --------------------------------------------------------------- setup
 
-// Ladder block size over the second virtual index: two v^3 x nb buffers.
-static int64_t ladder_nb(int64_t nv) {
-  const int64_t budget = (int64_t)1 << 29;  // doubles (4 GiB) for the two buffers
-  int64_t v3 = nv * nv * nv;
-  int64_t nb = std::max<int64_t>(1, budget / std::max<int64_t>(2 * v3, 1));
-  return std::min(nb, nv);
+// a-block size of the symmetric ladder: Vblk holds v^2 na (v - a0) doubles.
+static int64_t ladder_na(int64_t nv) {
+  const int64_t budget = (int64_t)1 << 28;  // doubles (2 GiB) for one V block
+  int64_t na = (nv + 7) / 8;
+  na = std::min<int64_t>(na, std::max<int64_t>(1, budget / std::max<int64_t>(nv * nv * nv, 1)));
+  return std::max<int64_t>(1, std::min(na, nv));
+}
+
+// Pair tables for the symmetric ladder (host build, one upload).
+static void ladder_setup(Ctx& c) {
+  const int v = c.nv, o = c.no;
+  std::vector<int> cd, ij, pr;
+  for (int d = 0; d < v; ++d)
+    for (int x = 0; x <= d; ++x) {
+      cd.push_back(x);
+      cd.push_back(d);
+    }
+  for (int j = 0; j < o; ++j)
+    for (int i = 0; i <= j; ++i) {
+      ij.push_back(i);
+      ij.push_back(j);
+    }
+  const int na = (int)ladder_na(v);
+  c.lblocks.clear();
+  for (int a0 = 0; a0 < v; a0 += na) {
+    Ctx::LadderBlock b{a0, std::min(na, v - a0), 0, 0, (int64_t)pr.size() / 2};
+    for (int a = a0; a < a0 + b.na; ++a)
+      for (int bb = a; bb < v; ++bb) {
+        pr.push_back(a);
+        pr.push_back(bb);
+      }
+    b.npp = (int)((int64_t)pr.size() / 2 - b.poff);
+    b.npm = b.npp - b.na;
+    c.lblocks.push_back(b);
+  }
+  auto up = [&](std::vector<int>& x, const char* what) {
+    int* d = (int*)c.alloc(((int64_t)x.size() + 1) / 2, what);
+    check(dev::h2d(d, x.data(), x.size() * sizeof(int), c.st), "h2d tables");
+    return d;
+  };
+  c.cdp = up(cd, "ladder cd pairs");
+  c.ijp = up(ij, "ladder ij pairs");
+  c.pairs = up(pr, "ladder ab pairs");
+  check(dev::sync(c.st), "sync tables");
 }
 
 void setup_system(Ctx& c, int no, int nv, int nq, const double* B, const double* h1, double e0) {
@@ -129,9 +167,9 @@ void setup_system(Ctx& c, int no, int nv, int nq, const double* B, const double*
   c.hscal = (double*)dev::hmalloc_pinned(256 * sizeof(double));
   if (!c.hscal) throw Error(ECG_ERR_OOM, "pinned host scalars");
 
-  const int64_t n2 = c.n2(), nb = ladder_nb(v);
-  int64_t wsn = 14 * n2 + 6 * v * o * Q + 3 * v * v * Q + 2 * n * n * Q + 4 * o * o * o * o +
-                2 * nb * v * v * v + 8 * n * n + (1 << 16);
+  const int64_t n2 = c.n2(), na = ladder_na(v);
+  int64_t wsn = 16 * n2 + 6 * v * o * Q + 3 * v * v * Q + 2 * n * n * Q + 4 * o * o * o * o +
+                3 * na * v * v * v + 8 * n * n + (1 << 16);
   c.ws_base = c.alloc(wsn, "workspace");
   c.ws.init(c.ws_base, wsn);
 
@@ -154,6 +192,7 @@ void setup_system(Ctx& c, int no, int nv, int nq, const double* B, const double*
   check(dev::h2d(c.Boo, boo.data(), boo.size() * 8, c.st), "h2d");
   check(dev::h2d(c.h, h1, n * n * 8, c.st), "h2d");
   c.h_host.assign(h1, h1 + n * n);
+  ladder_setup(c);
 
   // undressed Fock = dressing with T1 = 0 (gen_fock, src/scf/fockfactory.jl:27-30)
   dress(c, nullptr);
@@ -245,28 +284,50 @@ void dress(Ctx& c, const double* T1) {
 
 // --------------------------------------------------------------- residual
 
-// Particle-particle ladder  R2[a,b,i,j] += sum_cd (ac|bd)^ T2[c,d,i,j], with
-// (ac|bd)^ = sum_Q Bf[a,c,Q] Bf[b,d,Q] built per block of b and never stored
-// whole (replaces the kext GEMM, cc.jl:1400-1410).  BfT[d,b,Q] = Bf[b,d,Q].
+// Particle-particle ladder  R2[a,b,i,j] += sum_cd (ac|bd)^ T2[c,d,i,j] with
+// (ac|bd)^ = sum_Q Bf[a,c,Q] Bf[b,d,Q] (replaces the kext GEMM,
+// cc.jl:1400-1410).  T2 is split into its parts symmetric / antisymmetric
+// under c<->d (and then also i<->j); with V+-[ab,cd] = V[acbd] +- V[adbc]
+//   L+[ab,ij] = sum_{c<=d} V+ T+,   L-[ab,ij] = sum_{c<d} V- T-
+// are symmetric / antisymmetric in (a,b) and (i,j), so only a<=b, i<=j, c<=d
+// are formed: a quarter of the contraction flops and, by building V for
+// a<=b only (blocks of a against all b >= a0), about half of the DF rebuild.
+// V is never stored beyond one a-block.  BfT[c,a,Q] = Bf[a,c,Q].
 void ladder(Ctx& c, const double* Bf, const double* BfT, const double* T2, double* R2) {
+  (void)Bf;
   const int64_t o = c.no, v = c.nv, Q = c.nq;
-  const int64_t nb = ladder_nb(v);
+  const int64_t ncdp = v * (v + 1) / 2, ncdm = v * (v - 1) / 2;
+  const int64_t nijp = o * (o + 1) / 2, nijm = o * (o - 1) / 2;
   dev::stream_t s = c.st;
   const int64_t mark = c.ws.mark();
-  double* V = c.ws.get(nb * v * v * v);
-  double* Vp = c.ws.get(nb * v * v * v);
-  for (int64_t b0 = 0; b0 < v; b0 += nb) {
-    const int64_t bn = std::min(nb, v - b0);
-    // V[a,c,d,b'] = sum_Q dB[a,c,Q] dBT[d,b0+b',Q]
-    check(dev::gemm(s, 'N', 'T', v * v, v * bn, Q, 1.0, Bf, v * v, BfT + v * b0, v * v, 0.0, V,
-                    v * v),
+  double* Ts = c.ws.get(ncdp * nijp);
+  double* Ta = c.ws.get(std::max<int64_t>(ncdm * nijm, 1));
+  check(dev::ladder_pack_t(s, (int)v, (int)o, T2, c.cdp, c.ijp, Ts, Ta), "ladder pack T");
+  int64_t maxpp = 0, maxv = 0;
+  for (auto& b : c.lblocks) {
+    maxpp = std::max<int64_t>(maxpp, b.npp);
+    maxv = std::max<int64_t>(maxv, v * b.na * v * (v - b.a0));
+  }
+  double* V = c.ws.get(maxv);
+  double* Vp = c.ws.get(ncdp * maxpp);
+  double* Vm = c.ws.get(std::max<int64_t>(ncdm * maxpp, 1));
+  double* Lp = c.ws.get(maxpp * nijp);
+  double* Lm = c.ws.get(std::max<int64_t>(maxpp * nijm, 1));
+  for (auto& b : c.lblocks) {
+    const int64_t nb = v - b.a0;
+    // V[c,a',d,b''] = sum_Q BfT[c,a0+a',Q] BfT[d,a0+b'',Q]
+    check(dev::gemm(s, 'N', 'T', v * b.na, v * nb, Q, 1.0, BfT + v * b.a0, v * v, BfT + v * b.a0,
+                    v * v, 0.0, V, v * b.na),
           "gemm ladder V");
-    int64_t dims[4] = {v, v, v, bn};
-    int perm[4] = {0, 3, 1, 2};  // -> [a,b',c,d]
-    check(dev::permute(s, 4, dims, perm, 1.0, V, 0.0, Vp), "permute ladder");
-    check(dev::gemm(s, 'N', 'N', v * bn, o * o, v * v, 1.0, Vp, v * bn, T2, v * v, 1.0,
-                    R2 + v * b0, v * v),
-          "gemm ladder");
+    const int* pairs = c.pairs + 2 * b.poff;
+    check(dev::ladder_pack_v(s, (int)v, b.a0, b.na, b.npp, pairs, c.cdp, V, Vp, Vm), "pack V");
+    check(dev::gemm(s, 'T', 'N', b.npp, nijp, ncdp, 1.0, Vp, ncdp, Ts, ncdp, 0.0, Lp, b.npp),
+          "gemm ladder +");
+    if (b.npm > 0 && nijm > 0)
+      check(dev::gemm(s, 'T', 'N', b.npm, nijm, ncdm, 1.0, Vm, ncdm, Ta, ncdm, 0.0, Lm, b.npm),
+            "gemm ladder -");
+    check(dev::ladder_unpack(s, (int)v, (int)o, b.a0, b.npp, pairs, c.ijp, Lp, Lm, R2),
+          "ladder unpack");
   }
   c.ws.release(mark);
 }

@@ -63,6 +63,14 @@ struct Ctx {
   Arena ws;
   double* ws_base = nullptr;
 
+  // ladder pair tables (device int pairs) and a-blocks
+  int *cdp = nullptr, *ijp = nullptr, *pairs = nullptr;
+  struct LadderBlock {
+    int a0, na, npp, npm;
+    int64_t poff;  // offset (in pairs) into `pairs`
+  };
+  std::vector<LadderBlock> lblocks;
+
   DiisState diis;
   ecg_cc_opts opts;
 

@@ -110,6 +110,21 @@ int triples_int(stream_t s, int nv, const double* X, const double* Mjk, const do
 void gemm_timing(bool enable);
 void gemm_time(double* ms, int64_t* launches, double* flops);
 
+// Symmetric/antisymmetric particle-particle ladder helpers.  Pair tables hold
+// (x,y) as int pairs: cdp enumerates c<=d (d outer), ijp i<=j, pairs the
+// (a,b), a<=b of one a-block.  Packed "minus" indices follow arithmetically:
+// idx-(c,d) = idx+(c,d) - d (c<d); pair-(a,b) = pair+(a,b) - (a-a0) - 1 (a<b).
+//   ladder_pack_t: Ts[cd+,ij+] = (T[c,d,i,j]+T[d,c,i,j])/2, Ta[cd-,ij-] = (T[c,d,i,j]-T[d,c,i,j])/2
+//   ladder_pack_v: Vblk[c,a',d,b''] (a' = a-a0, b'' = b-a0) ->
+//                  Vp[cd+,pair+] = V[acbd]+V[adbc] (c<d), V[acbc] (c=d);  Vm[cd-,pair-] = V[acbd]-V[adbc]
+//   ladder_unpack: R2[a,b,i,j] += Lp+Lm, R2[b,a,i,j] += Lp-Lm, R2[a,b,j,i] += Lp-Lm, R2[b,a,j,i] += Lp+Lm
+int ladder_pack_t(stream_t s, int nv, int no, const double* T2, const int* cdp, const int* ijp,
+                  double* Ts, double* Ta);
+int ladder_pack_v(stream_t s, int nv, int a0, int na, int npairs, const int* pairs,
+                  const int* cdp, const double* Vblk, double* Vp, double* Vm);
+int ladder_unpack(stream_t s, int nv, int no, int a0, int npairs, const int* pairs,
+                  const int* ijp, const double* Lp, const double* Lm, double* R2);
+
 // Count of kernels launched through this layer in this process.
 int64_t launches();
 

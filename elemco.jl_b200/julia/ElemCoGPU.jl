@@ -1,0 +1,212 @@
+"""
+    ElemCoGPU
+
+Julia side of libecgpu: `ccall` bindings of include/ecgpu.h and drop-in
+replacements for ElemCo.jl's closed-shell `calc_cc`, `calc_pertT` and
+`calc_lm_cc` (src/cc/cc.jl:2451, src/cc/cc_triples.jl:11,
+src/cc/cc_lagrange.jl:1120).  They read the same inputs (the `mmL` DF factors
+or EC.fd, the Fock matrix) and write the same scratch files (`T_vo`,
+`T_vvoo`, `U_vo`, `U_vvoo`, `cc_amplitudes_*`, `cc_multipliers_*`), so the
+rest of `ccdriver` is unchanged.  Wiring into `eval_cc_groundstate` is shown
+in INTEGRATION.md.
+
+Host arrays are passed as `Ptr{Cdouble}` inside `GC.@preserve`; Julia's
+column-major layout is the library's layout.  Status codes other than 0 raise
+`ErrorException(ecg_last_error)`.
+"""
+module ElemCoGPU
+
+export GPUContext, gpu_calc_cc, gpu_calc_pertT, gpu_calc_lm_cc
+
+const libecgpu = get(ENV, "ECGPU_LIB", joinpath(@__DIR__, "..", "ecgpu", "libecgpu.so"))
+
+struct CcOpts
+  thr::Cdouble
+  conven::Cdouble
+  maxit::Int32
+  shifts::Cdouble
+  shiftp::Cdouble
+  maxdiis::Int32
+  resthr::Cdouble
+end
+
+"""
+    GPUContext(device=0)
+
+One device-resident closed-shell CC problem (`ecg_ctx`); freed by a finalizer.
+"""
+mutable struct GPUContext
+  ptr::Ptr{Cvoid}
+  no::Int
+  nv::Int
+  nq::Int
+  function GPUContext(device::Integer=0)
+    r = Ref{Ptr{Cvoid}}(C_NULL)
+    st = ccall((:ecg_create, libecgpu), Cint, (Cint, Ptr{Ptr{Cvoid}}), device, r)
+    st == 0 || error(unsafe_string(ccall((:ecg_last_error, libecgpu), Cstring, (Ptr{Cvoid},), C_NULL)))
+    ctx = new(r[], 0, 0, 0)
+    finalizer(c -> (c.ptr != C_NULL && ccall((:ecg_destroy, libecgpu), Cint, (Ptr{Cvoid},), c.ptr); c.ptr = C_NULL), ctx)
+    return ctx
+  end
+end
+
+function check(ctx::GPUContext, st::Cint)
+  st == 0 && return nothing
+  error("libecgpu status $st: " * unsafe_string(ccall((:ecg_last_error, libecgpu), Cstring, (Ptr{Cvoid},), ctx.ptr)))
+end
+
+function options(EC)
+  cc = EC.options.cc
+  d = EC.options.diis
+  return CcOpts(cc.thr, cc.conven, Int32(cc.maxit), cc.shifts, cc.shiftp, Int32(d.maxdiis), d.resthr)
+end
+
+"""
+    set_system!(ctx, B, h1, e0, nocc)
+
+Upload `B[p,q,L]` (the `mmL` file, src/integrals/dftools.jl:92-134), the
+one-electron integrals and the core energy (`ecg_set_system`).
+"""
+function set_system!(ctx::GPUContext, B::Array{Float64,3}, h1::Matrix{Float64}, e0::Float64, nocc::Integer)
+  n = size(B, 1)
+  @assert size(B, 2) == n && size(h1) == (n, n)
+  ctx.no, ctx.nv, ctx.nq = nocc, n - nocc, size(B, 3)
+  GC.@preserve B h1 check(ctx, ccall((:ecg_set_system, libecgpu), Cint,
+      (Ptr{Cvoid}, Int32, Int32, Int32, Ptr{Cdouble}, Ptr{Cdouble}, Cdouble),
+      ctx.ptr, ctx.no, ctx.nv, ctx.nq, B, h1, e0))
+  return ctx
+end
+
+function mp2!(ctx::GPUContext)
+  T1 = zeros(ctx.nv, ctx.no)
+  T2 = zeros(ctx.nv, ctx.nv, ctx.no, ctx.no)
+  e = Ref{Cdouble}(0.0)
+  GC.@preserve T1 T2 check(ctx, ccall((:ecg_mp2, libecgpu), Cint,
+      (Ptr{Cvoid}, Ptr{Cdouble}, Ptr{Cdouble}, Ref{Cdouble}), ctx.ptr, T1, T2, e))
+  return e[], T1, T2
+end
+
+function cc_solve!(ctx::GPUContext, T1, T2, dc::Bool, o::CcOpts)
+  out = zeros(5)
+  it = Ref{Int32}(0)
+  conv = Ref{Int32}(0)
+  GC.@preserve T1 T2 out check(ctx, ccall((:ecg_cc_solve, libecgpu), Cint,
+      (Ptr{Cvoid}, Cint, Ref{CcOpts}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ref{Int32}, Ref{Int32}),
+      ctx.ptr, dc, o, T1, T2, out, it, conv))
+  return out, Int(it[]), conv[] != 0
+end
+
+function pert_t(ctx::GPUContext, T1, T2)
+  e = Ref{Cdouble}(0.0); eb = Ref{Cdouble}(0.0)
+  GC.@preserve T1 T2 check(ctx, ccall((:ecg_pert_t, libecgpu), Cint,
+      (Ptr{Cvoid}, Ptr{Cdouble}, Ptr{Cdouble}, Ref{Cdouble}, Ref{Cdouble}), ctx.ptr, T1, T2, e, eb))
+  return e[], eb[]
+end
+
+function lambda_pert_t(ctx::GPUContext, T1, T2, U1, U2)
+  e = Ref{Cdouble}(0.0); eb = Ref{Cdouble}(0.0)
+  GC.@preserve T1 T2 U1 U2 check(ctx, ccall((:ecg_lambda_pert_t, libecgpu), Cint,
+      (Ptr{Cvoid}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ref{Cdouble}, Ref{Cdouble}),
+      ctx.ptr, T1, T2, U1, U2, e, eb))
+  return e[], eb[]
+end
+
+function lambda_solve!(ctx::GPUContext, T1, T2, dc::Bool, o::CcOpts)
+  U1 = zeros(ctx.nv, ctx.no)
+  U2 = zeros(ctx.nv, ctx.nv, ctx.no, ctx.no)
+  out = zeros(3)
+  it = Ref{Int32}(0); conv = Ref{Int32}(0)
+  GC.@preserve T1 T2 U1 U2 out check(ctx, ccall((:ecg_lambda_solve, libecgpu), Cint,
+      (Ptr{Cvoid}, Cint, Ref{CcOpts}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble},
+       Ptr{Cdouble}, Ref{Int32}, Ref{Int32}),
+      ctx.ptr, dc, o, T1, T2, U1, U2, out, it, conv))
+  return U1, U2, Int(it[]), conv[] != 0
+end
+
+# ---------------------------------------------------------------- drop-ins
+# These use ElemCo's own helpers (passed in as the module `EM`, i.e.
+# `ElemCo`), so this file loads without ElemCo installed.
+
+"""
+    df_factors(EM, EC)
+
+`mmL` DF factors for EC.fd: the file written by @dfints/dfdump, or — for an
+FCIDUMP — the Cholesky decomposition of src/integrals/decomptools.jl:22-52.
+"""
+function df_factors(EM, EC)
+  if !EM.ECInfos.file_exists(EC, "mmL")
+    EM.DecompTools.calc_integrals_decomposition(EC)
+  end
+  return EM.TensorTools.load3idx(EC, "mmL")
+end
+
+function context(EM, EC)
+  ctx = get!(EC.options.gpu, :ctx) do
+    GPUContext(get(EC.options.gpu, :device, 0))
+  end
+  SP = EC.space
+  set_system!(ctx, df_factors(EM, EC), EM.FciDumps.integ1(EC.fd), EC.fd.int0, length(SP['o']))
+  return ctx
+end
+
+"""
+    gpu_calc_cc(EM, EC, method) -> OutDict
+
+Closed-shell `calc_cc` (src/cc/cc.jl:2451-2516) on the GPU: starts from the
+`T_vo`/`T_vvoo` MP2 guess, writes the converged amplitudes back to the same
+files and returns the Hylleraas energies.
+"""
+function gpu_calc_cc(EM, EC, method)
+  ctx = context(EM, EC)
+  dc = method.theory[1:2] == "DC"
+  T1 = EM.TensorTools.load2idx(EC, "T_vo")
+  T2 = EM.TensorTools.load4idx(EC, "T_vvoo")
+  out, it, conv = cc_solve!(ctx, T1, T2, dc, options(EC))
+  conv || println("WARNING: CC iterations did not converge!")
+  EM.TensorTools.save!(EC, "T_vo", T1)
+  EM.TensorTools.save!(EC, "T_vvoo", T2)
+  EM.CCTools.try2save_singles!(EC, T1)
+  EM.CCTools.try2save_doubles!(EC, T2)
+  return EM.OutDict("E"=>out[1], "ESS"=>out[2], "EOS"=>out[3], "EO"=>0.0)
+end
+
+"""
+    gpu_calc_lm_cc(EM, EC, method)
+
+Closed-shell `calc_lm_cc` (src/cc/cc_lagrange.jl:1120-1153): writes `U_vo`,
+`U_vvoo` and the `cc_multipliers_*` files.
+"""
+function gpu_calc_lm_cc(EM, EC, method)
+  ctx = context(EM, EC)
+  dc = (method.theory == "DC" || last(method.theory, 2) == "DC")
+  T1 = EM.TensorTools.load2idx(EC, "T_vo")
+  T2 = EM.TensorTools.load4idx(EC, "T_vvoo")
+  U1, U2, it, conv = lambda_solve!(ctx, T1, T2, dc, options(EC))
+  conv || println("WARNING: CC-LM iterations did not converge!")
+  EM.TensorTools.save!(EC, "U_vo", U1)
+  EM.TensorTools.save!(EC, "U_vvoo", U2)
+  EM.CCTools.try2save_singles!(EC, U1; type="LM")
+  EM.CCTools.try2save_doubles!(EC, U2; type="LM")
+  return nothing
+end
+
+"""
+    gpu_calc_pertT(EM, EC, method) -> OutDict("ET3"=>..., "ET3b"=>...)
+
+Closed-shell (T) / Λ(T) (src/cc/cc_triples.jl:11-30, :39-295).
+"""
+function gpu_calc_pertT(EM, EC, method)
+  ctx = context(EM, EC)
+  T1 = EM.TensorTools.load2idx(EC, "T_vo")
+  T2 = EM.TensorTools.load4idx(EC, "T_vvoo")
+  if EM.ECMethods.has_prefix(method, "Λ")
+    U1 = EM.TensorTools.load2idx(EC, "U_vo")
+    U2 = EM.TensorTools.load4idx(EC, "U_vvoo")
+    e, eb = lambda_pert_t(ctx, T1, T2, U1, U2)
+  else
+    e, eb = pert_t(ctx, T1, T2)
+  end
+  return EM.OutDict("ET3"=>e, "ET3b"=>eb)
+end
+
+end # module
