@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <mutex>
 #include <cstdio>
 #include <utility>
 #include <vector>
@@ -280,6 +281,68 @@ __global__ void splitk_reduce_kernel(int64_t m, int64_t n, int S, const double* 
     if (beta != 0.0) v += beta * *c;
     *c = v;
   }
+}
+
+// ---- split-K GEMM without any allocation --------------------------------
+//
+// For callers that cannot allocate device memory (code running under a
+// framework's memory manager, inside stream capture, or in a process whose
+// device memory is fully handed out): the partial products live in this
+// fixed file-scope array, 2^22 doubles (32 MiB), which every GPU that loads
+// the library keeps until process exit.  Host code cannot use the symbol as
+// a device address; its address is looked up once per device with
+// cudaGetSymbolAddress (on the first call on that device, with that device
+// current) and cached.
+static constexpr size_t kNoAllocScratchDoubles = (size_t)1 << 22;
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
+static double* g_noalloc_ptr[128] = {nullptr};
+static std::mutex g_noalloc_mu;
+
+size_t noalloc_scratch_doubles() { return kNoAllocScratchDoubles; }
+
+static int noalloc_scratch_ptr(double** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return (int)e;
+  if (dev < 0 || dev >= 128) return (int)cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return (int)e;
+    g_noalloc_ptr[dev] = (double*)p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return 0;
+}
+
+int gemm_splitk_noalloc(stream_t s, char ta, char tb, int64_t m, int64_t n, int64_t k,
+                        double alpha, const double* A, int64_t lda, const double* B, int64_t ldb,
+                        double beta, double* C, int64_t ldc, int* nsplit) {
+  if (m <= 0 || n <= 0 || k <= 0) return (int)cudaErrorInvalidValue;
+  if ((size_t)m * (size_t)n > kNoAllocScratchDoubles) return (int)cudaErrorInvalidValue;
+  double* P = nullptr;
+  int e = noalloc_scratch_ptr(&P);
+  if (e) return e;
+  const bool at = (ta == 'T' || ta == 't'), bt = (tb == 'T' || tb == 't');
+  const int64_t tiles64 = ((m + 63) / 64) * ((n + 63) / 64);
+  int64_t S = std::min<int64_t>((2 * 148 + tiles64 - 1) / tiles64, (k + 255) / 256);
+  S = std::max<int64_t>(1, std::min<int64_t>(S, 64));
+  while (S > 1 && (size_t)S * m * n > kNoAllocScratchDoubles) --S;
+  int64_t kc = (k + S - 1) / S;
+  kc = (kc + 15) / 16 * 16;
+  S = (k + kc - 1) / kc;
+  GemmArgs h{A, B, P, m, n, kc, at ? lda : 1, at ? 1 : lda, 0, bt ? ldb : 1, bt ? 1 : ldb, 0,
+             1, m, m * n, 1.0, 0.0, (at && lda != 1) ? 1 : 0, (bt && ldb != 1) ? 1 : 0,
+             k - (S - 1) * kc};
+  h.sab = kc * h.sak;
+  h.sbb = kc * h.sbk;
+  cudaStream_t st = (cudaStream_t)s;
+  e = launch_gemm<64, 64, 16, 32, 32, 3, 3>(h, S, st);
+  if (e) return e;
+  splitk_reduce_kernel<<<grid_for(m * n), 256, 0, st>>>(m, n, (int)S, P, alpha, beta, C, 1, ldc);
+  if (nsplit) *nsplit = (int)S;
+  return launched();
 }
 
 // Event-pair pool for GEMM timing.

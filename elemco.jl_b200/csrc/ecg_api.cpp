@@ -398,6 +398,35 @@ int ecg_diis_destroy(ecg_diis* d) {
 
 int64_t ecg_kernel_launches(const ecg_ctx*) { return dev::launches(); }
 
+// Allocation-free FP64 GEMM on device pointers (see include/ecgpu.h): argument
+// checks on the host, then dev::gemm_splitk_noalloc, which uses only the
+// library's static scratch array.
+int ecg_gemm_noalloc(char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha,
+                     const double* A, int64_t lda, const double* B, int64_t ldb, double beta,
+                     double* C, int64_t ldc, void* stream, int32_t* nsplit) {
+  return guarded(nullptr, [&] {
+    const bool at = (ta == 'T' || ta == 't'), bt = (tb == 'T' || tb == 't');
+    if (!(at || ta == 'N' || ta == 'n') || !(bt || tb == 'N' || tb == 'n'))
+      throw Error(ECG_ERR_ARG, "ta/tb must be 'N' or 'T'");
+    if (m <= 0 || n <= 0 || k <= 0) throw Error(ECG_ERR_ARG, "m, n, k must be positive");
+    need_ptr(A, "A");
+    need_ptr(B, "B");
+    need_ptr(C, "C");
+    if (lda < (at ? k : m) || ldb < (bt ? n : k) || ldc < m)
+      throw Error(ECG_ERR_ARG, "leading dimension too small");
+    const uint64_t cap = dev::noalloc_scratch_doubles();
+    if ((uint64_t)m * (uint64_t)n > cap)
+      throw Error(ECG_ERR_ARG, "m*n = " + std::to_string((uint64_t)m * (uint64_t)n) +
+                                   " exceeds the allocation-free scratch (" +
+                                   std::to_string(cap) + " output elements)");
+    int S = 0;
+    int e = dev::gemm_splitk_noalloc(stream, at ? 'T' : 'N', bt ? 'T' : 'N', m, n, k, alpha, A,
+                                     lda, B, ldb, beta, C, ldc, &S);
+    check(e, "ecg_gemm_noalloc");
+    if (nsplit) *nsplit = S;
+  });
+}
+
 int ecg_cc_step_host(ecg_ctx* c, int dc, double* T1, double* T2, double* out) {
   if (!c) return ECG_ERR_ARG;
   return guarded(c, [&] {

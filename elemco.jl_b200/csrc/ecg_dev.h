@@ -106,6 +106,14 @@ int triples_int(stream_t s, int nv, const double* X, const double* Mjk, const do
                 const double* Mij, const double* Njk, const double* Nik, const double* Nij,
                 double fac, double* IntX, double* IntY, int i, int j, int k);
 
+// Split-K GEMM (column-major, device pointers) whose partial products use a
+// fixed file-scope device array instead of allocated memory; m*n must not
+// exceed noalloc_scratch_doubles().  *nsplit receives the K split used.
+size_t noalloc_scratch_doubles();
+int gemm_splitk_noalloc(stream_t s, char ta, char tb, int64_t m, int64_t n, int64_t k,
+                        double alpha, const double* A, int64_t lda, const double* B, int64_t ldb,
+                        double beta, double* C, int64_t ldc, int* nsplit);
+
 // GEMM event timing (process-wide): enable, then read and reset the totals.
 void gemm_timing(bool enable);
 void gemm_time(double* ms, int64_t* launches, double* flops);

@@ -79,6 +79,9 @@ SIGNATURES = {
                                 C.c_int64]),
     "ecg_diag_permute": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int),
                                    C.c_double, _D, C.c_double, _D]),
+    "ecg_gemm_noalloc": (C.c_int, [C.c_char, C.c_char, C.c_int64, C.c_int64, C.c_int64,
+                                   C.c_double, _P, C.c_int64, _P, C.c_int64, C.c_double, _P,
+                                   C.c_int64, _P, C.POINTER(C.c_int32)]),
 }
 
 

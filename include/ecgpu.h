@@ -171,6 +171,30 @@ int ecg_diag_gemm(ecg_ctx* ctx, char ta, char tb, int64_t m, int64_t n, int64_t 
 int ecg_diag_permute(ecg_ctx* ctx, int nd, const int64_t* in_dims, const int* perm, double alpha,
                      const double* in, double beta, double* out);
 
+/* ------------------------------------------------------------------------
+ * Allocation-free entry point (no counterpart in the reference).
+ *
+ * For callers that must not allocate device memory in their call path — code
+ * that runs under another framework's memory manager, inside CUDA stream
+ * capture, or in a process whose device memory is already handed out.  It
+ * computes C = alpha op(A) op(B) + beta C (column-major, op 'N' or 'T') on
+ * DEVICE pointers with the library's FP64 split-K GEMM; the split-K partial
+ * products go to a fixed 32 MiB device array inside the library (2^22
+ * doubles; every GPU that loads the library holds it until process exit), so
+ * m*n may be at most 4194304 (larger sizes return ECG_ERR_ARG).  The call
+ * makes no cudaMalloc/cudaFree.  The first call on a device looks up that
+ * array's device address (with the device current) and must come before any
+ * stream capture on that device.  All calls share the one array, so calls
+ * whose kernels overlap on the GPU (different streams, other threads) race
+ * and give wrong results; every call overwrites the partial products it
+ * reads, nothing needs to start at zero.  `stream` is a cudaStream_t (NULL =
+ * legacy default stream); the call is asynchronous on it.  *nsplit (may be
+ * NULL) receives the number of K slices used.
+ * ---------------------------------------------------------------------- */
+int ecg_gemm_noalloc(char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha,
+                     const double* A, int64_t lda, const double* B, int64_t ldb, double beta,
+                     double* C, int64_t ldc, void* stream, int32_t* nsplit);
+
 #ifdef __cplusplus
 }
 #endif
