@@ -494,9 +494,17 @@ int ecg_diag_gemm(ecg_ctx* c, char ta, char tb, int64_t m, int64_t n, int64_t k,
     check(dev::h2d(dA, A, sA * 8, c->st), "h2d");
     check(dev::h2d(dB, B, sB * 8, c->st), "h2d");
     check(dev::h2d(dC, C, sC * 8, c->st), "h2d");
-    check(dev::gemm(c->st, ta, tb, m, n, k, alpha, dA, lda, dB, ldb, beta, dC, ldc), "gemm");
+    if (c->prec == ECG_PREC_MIXED)
+      check(dev::gemm_mixed(c->st, ta, tb, m, n, k, alpha, dA, lda, dB, ldb, beta, dC, ldc),
+            "gemm_mixed");
+    else
+      check(dev::gemm(c->st, ta, tb, m, n, k, alpha, dA, lda, dB, ldb, beta, dC, ldc), "gemm");
     check(dev::d2h(C, dC, sC * 8, c->st), "d2h");
     check(dev::sync(c->st), "sync");
+    int tc = 0;
+    check(dev::tc_error(&tc), "tc_error");
+    if (tc) throw Error(ECG_ERR_TIMEOUT, "tensor-core GEMM wait timed out (code " +
+                                             std::to_string(tc) + ")");
   });
 }
 

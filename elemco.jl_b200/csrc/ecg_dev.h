@@ -114,6 +114,14 @@ int gemm_splitk_noalloc(stream_t s, char ta, char tb, int64_t m, int64_t n, int6
                         double alpha, const double* A, int64_t lda, const double* B, int64_t ldb,
                         double beta, double* C, int64_t ldc, int* nsplit);
 
+// Split-BF16 tensor-core GEMM (tcgen05, FP32 accumulate, ~FP32 accuracy),
+// same interface as gemm().  tc_error() returns and clears the time-out code
+// of the tensor-core kernels (0 = none).
+int gemm_mixed(stream_t s, char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha,
+               const double* A, int64_t lda, const double* B, int64_t ldb, double beta,
+               double* C, int64_t ldc);
+int tc_error(int* code);
+
 // GEMM event timing (process-wide): enable, then read and reset the totals.
 void gemm_timing(bool enable);
 void gemm_time(double* ms, int64_t* launches, double* flops);

@@ -160,9 +160,10 @@ int64_t ecg_kernel_launches(const ecg_ctx* ctx);
 int ecg_set_gemm_timing(ecg_ctx* ctx, int enable);
 int ecg_gemm_time(ecg_ctx* ctx, double* ms, int64_t* launches, double* flops);
 
-/* The library's FP64 GEMM / permutation on host buffers (column-major),
- * for self-tests of the device kernels:
- * C = alpha op(A) op(B) + beta C  with op 'N' or 'T'. */
+/* The library's GEMM / permutation on host buffers (column-major), for
+ * self-tests of the device kernels:
+ * C = alpha op(A) op(B) + beta C  with op 'N' or 'T'.  With the context's
+ * precision set to ECG_PREC_MIXED the split-BF16 tensor-core GEMM is used. */
 int ecg_diag_gemm(ecg_ctx* ctx, char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha,
                   const double* A, int64_t lda, const double* B, int64_t ldb, double beta,
                   double* C, int64_t ldc);

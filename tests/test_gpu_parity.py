@@ -201,3 +201,26 @@ def test_diis_standalone(ctx, h2o_df):
         od.perform(vec, [ro])
         xo = vec[0]
         assert np.abs(x - xo).max() < 1e-10
+
+
+@pytest.mark.parametrize("ta,tb,m,n,k", [("N", "N", 1, 1, 1), ("N", "N", 128, 128, 64),
+                                         ("N", "T", 200, 130, 100), ("T", "N", 300, 257, 700),
+                                         ("T", "T", 129, 65, 1000), ("N", "N", 1216, 1216, 1216),
+                                         ("T", "N", 2926, 136, 2926)])
+def test_mixed_gemm_kernel(ta, tb, m, n, k):
+    """Split-BF16 tcgen05 GEMM: FP32-level error, below 4 (k/16 + 16) 2^-24 of
+    sum |a||b| (the bound of FP32 accumulation over k/16 MMA steps)."""
+    import ecgpu
+    rng = np.random.default_rng(m + 7 * n + 13 * k)
+    A = rng.standard_normal((k, m) if ta == "T" else (m, k))
+    B = rng.standard_normal((n, k) if tb == "T" else (k, n))
+    C = rng.standard_normal((m, n))
+    opA = A.T if ta == "T" else A
+    opB = B.T if tb == "T" else B
+    ref = 0.7 * (opA @ opB) - 0.3 * C
+    scale = 0.7 * (np.abs(opA) @ np.abs(opB)) + 0.3 * np.abs(C)
+    with ecgpu.Context(0) as c:
+        c.set_precision(ecgpu.ECG_PREC_MIXED)
+        out = c.diag_gemm(ta, tb, 0.7, A, B, -0.3, C)
+    err = np.abs(out - ref) / scale
+    assert err.max() < 4.0 * (k / 16 + 16) * 2.0 ** -24, err.max()
