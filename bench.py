@@ -49,6 +49,8 @@ def parse_args():
     p.add_argument("--method", default="ccsd", choices=["ccsd", "dcsd"])
     p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     p.add_argument("--cpu-sample", type=int, default=2, help="CPU-baseline iterations")
+    p.add_argument("--tts", action="store_true",
+                   help="CCSD(T) time-to-solution, FP64 vs mixed, on --workload (one line)")
     return p.parse_args()
 
 
@@ -161,8 +163,54 @@ def run_reference(a, wl):
     print(json.dumps(line), flush=True)
 
 
+def run_tts(a):
+    """CCSD(T) from the MP2 guess to the (T) energy, FP64 and mixed precision,
+    timed with CUDA events on the library's stream (one JSON line)."""
+    import torch
+    import ecgpu
+    from ecgpu.synthetic import WORKLOADS, make_workload
+    no, nv, nq = WORKLOADS[a.workload]
+    B, h1, e0, no = make_workload(a.workload)
+    ntrip = sum(1 for k in range(no) for j in range(k + 1) for i in range(j + 1)
+                if not (i == j == k))
+    ft = ntrip * (12.0 * nv**4 + 12.0 * no * nv**3)
+    fcc = algorithmic_flops(no, nv, nq)
+    out = {}
+    with ecgpu.Context(0) as ctx:
+        ctx.set_system(B, h1, e0, no)
+        stream = torch.cuda.ExternalStream(ctx.stream())
+        _, T1, T2 = ctx.mp2()
+        for prec, name in ((ecgpu.ECG_PREC_FP64, "fp64"), (ecgpu.ECG_PREC_MIXED, "mixed")):
+            ctx.set_precision(prec)
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            torch.cuda.synchronize()
+            ev[0].record(stream)
+            r = ctx.cc_solve(T1, T2)
+            ev[1].record(stream)
+            et, etb = ctx.pert_t(r["T1"], r["T2"])
+            ev[2].record(stream)
+            torch.cuda.synchronize()
+            tcc = ev[0].elapsed_time(ev[1]) / 1000.0
+            tt = ev[1].elapsed_time(ev[2]) / 1000.0
+            out[name] = {"ccsd_s": tcc, "pert_t_s": tt, "total_s": tcc + tt,
+                         "iterations": r["iterations"], "E_ccsd": r["E"], "E_T": et,
+                         "ccsd_tflops_per_iter": fcc * r["iterations"] / tcc / 1e12,
+                         "pert_t_tflops": ft / tt / 1e12}
+    f64, mx = out["fp64"], out["mixed"]
+    line = {"metric": "CCSD(T) time-to-solution", "workload": a.workload,
+            "shape": {"o": no, "v": nv, "nQ": nq}, "unit": "s", "fp64": f64, "mixed": mx,
+            "speedup": f64["total_s"] / mx["total_s"],
+            "dE_uEh": abs((mx["E_ccsd"] + mx["E_T"]) - (f64["E_ccsd"] + f64["E_T"])) * 1e6,
+            "dE_T_uEh": abs(mx["E_T"] - f64["E_T"]) * 1e6,
+            "data": "synthetic DF factors (see ecgpu/synthetic.py)"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse_args()
+    if a.tts:
+        run_tts(a)
+        return
     from ecgpu.synthetic import WORKLOADS, make_workload
     wl = WORKLOADS[a.workload]
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -297,6 +345,51 @@ def main():
         with open(tp) as f:
             traffic = json.load(f).get(f"{a.workload}_{a.method}_{a.precision}")
 
+    # time-to-solution, FP64 vs mixed (split-BF16 tensor-core products + FP64
+    # refinement), full solves from the MP2 guess; energy difference in uEh
+    def solve_timed(prec):
+        ctx.set_precision(prec)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        flush.zero_()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        r = ctx.cc_solve(T1, T2, dc=dc)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        return r, ev0.elapsed_time(ev1) / 1000.0
+    solve_timed(ecgpu.ECG_PREC_MIXED)  # warm the tensor-core path (split buffers)
+    r64, t64 = solve_timed(ecgpu.ECG_PREC_FP64)
+    rmx, tmx = solve_timed(ecgpu.ECG_PREC_MIXED)
+    # mixed-precision iteration rate (same step as above, tensor-core products)
+    ctx.set_precision(ecgpu.ECG_PREC_MIXED)
+    restart()
+    ctx.cc_step(dc=dc)
+    restart()
+    evm = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(a.steps)]
+    for k in range(a.steps):
+        if k and k % RESTART == 0:
+            restart()
+        flush.zero_()
+        torch.cuda.synchronize()
+        evm[k][0].record(stream)
+        ctx.cc_step(dc=dc)
+        evm[k][1].record(stream)
+    torch.cuda.synchronize()
+    total_mx = sum(s_.elapsed_time(e_) for s_, e_ in evm)
+    ctx.set_precision(ecgpu.ECG_PREC_FP64)
+    # (T) on the converged FP64 amplitudes
+    ntrip = sum(1 for k_ in range(no) for j_ in range(k_ + 1) for i_ in range(j_ + 1)
+                if not (i_ == j_ == k_))
+    ft = ntrip * (12.0 * nv**4 + 12.0 * no * nv**3)
+    evt0, evt1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    evt0.record(stream)
+    et, _ = ctx.pert_t(r64["T1"], r64["T2"])
+    evt1.record(stream)
+    torch.cuda.synchronize()
+    t_t = evt0.elapsed_time(evt1) / 1000.0
+
     value = world * a.steps / (total / 1000.0)
     line = {
         "metric": "CCSD iter/s", "value": value, "unit": "iter/s", "n_gpus": world,
@@ -320,6 +413,13 @@ def main():
                                     "MEASURED_PEAKS.json)",
                      "step_frac": F / (total / a.steps / 1000.0) / 1e12 / fp64_peak},
         "clocks": clk,
+        "mixed": {"iter_per_s": world * a.steps / (total_mx / 1000.0),
+                  "precision": "split-BF16 (3 slices, 6 products) tcgen05 GEMMs, FP32 accumulate",
+                  "tts_fp64_s": t64, "tts_mixed_s": tmx, "tts_speedup": t64 / tmx,
+                  "iterations_fp64": r64["iterations"], "iterations_mixed": rmx["iterations"],
+                  "dE_uEh": abs(rmx["E"] - r64["E"]) * 1e6, "E_corr_fp64": r64["E"]},
+        "pert_t": {"seconds": t_t, "tflops": ft / t_t / 1e12, "E_T": et, "triplets": ntrip,
+                   "algorithmic_flops": ft, "precision": "fp64"},
     }
     if rank == 0 and world == 1 and a.cpu_sample > 0:
         rate, dt = cpu_ccsd_rate(no, nv, nq, dc, a.cpu_sample)

@@ -253,7 +253,7 @@ static unsigned grid_for(int64_t n, int threads = 256, int64_t cap = 148 * 16);
 // the old buffer synchronises the device, so no kernel still uses it).
 static double* g_splitk = nullptr;
 static size_t g_splitk_len = 0;
-static double* splitk_buffer(size_t n) {
+double* splitk_buffer(size_t n) {
   if (n > g_splitk_len) {
     if (g_splitk) cudaFree(g_splitk);
     g_splitk = nullptr;
@@ -342,6 +342,13 @@ int gemm_splitk_noalloc(stream_t s, char ta, char tb, int64_t m, int64_t n, int6
   if (e) return e;
   splitk_reduce_kernel<<<grid_for(m * n), 256, 0, st>>>(m, n, (int)S, P, alpha, beta, C, 1, ldc);
   if (nsplit) *nsplit = (int)S;
+  return launched();
+}
+
+int splitk_reduce(stream_t s, int64_t m, int64_t n, int S, const double* P, double alpha,
+                  double beta, double* C, int64_t scm, int64_t scn) {
+  splitk_reduce_kernel<<<grid_for(m * n), 256, 0, (cudaStream_t)s>>>(m, n, S, P, alpha, beta, C,
+                                                                     scm, scn);
   return launched();
 }
 
@@ -908,6 +915,98 @@ int triples_x(stream_t s, int nv, const double* K, double eijk, const double* ev
   int e = launched();
   if (e || !eout) return e;
   final_sum_kernel<<<1, 256, 0, st>>>(RED_BLOCKS, 1, scratch, eout);
+  return launched();
+}
+
+// One 8x8x8 cube of K per block (512 threads, thread = (a,b,c) in the cube).
+// Each W_t cube is loaded in W_t's own memory order (coalesced along its first
+// index) into shared memory and read back at the permuted position.
+struct SumWArgs {
+  const double* W[6];
+};
+
+__global__ void __launch_bounds__(512) triples_sumw_kernel(int nv, SumWArgs w, double* K) {
+  __shared__ double cube[8 * 9 * 9];
+  const int64_t v = nv, nt = (v + 7) / 8;
+  const int tx = threadIdx.x & 7, ty = (threadIdx.x >> 3) & 7, tz = threadIdx.x >> 6;
+  for (int64_t t = blockIdx.x; t < nt * nt * nt; t += gridDim.x) {
+    const int64_t o[3] = {(t % nt) * 8, ((t / nt) % nt) * 8, (t / (nt * nt)) * 8};  // a0,b0,c0
+    // permutation p: W_t is indexed W_t[x,y,z] with (x,y,z) = (o[p0], o[p1], o[p2]) origins
+    const int P[6][3] = {{0, 1, 2}, {1, 0, 2}, {0, 2, 1}, {2, 1, 0}, {1, 2, 0}, {2, 0, 1}};
+    double acc = 0.0;
+    const int loc[3] = {tx, ty, tz};  // this thread's (a,b,c) offsets
+    for (int q = 0; q < 6; ++q) {
+      const int64_t x = o[P[q][0]] + tx, y = o[P[q][1]] + ty, z = o[P[q][2]] + tz;
+      cube[tx + 9 * (ty + 9 * tz)] = (x < v && y < v && z < v) ? w.W[q][x + v * y + v * v * z] : 0.0;
+      __syncthreads();
+      // this thread's element of K needs W_q at (loc[P0], loc[P1], loc[P2])
+      acc += cube[loc[P[q][0]] + 9 * (loc[P[q][1]] + 9 * loc[P[q][2]])];
+      __syncthreads();
+    }
+    const int64_t a = o[0] + tx, b = o[1] + ty, c = o[2] + tz;
+    if (a < v && b < v && c < v) K[a + v * b + v * v * c] = acc;
+  }
+}
+
+int triples_sumw(stream_t s, int nv, const double* const* W, double* K) {
+  SumWArgs w;
+  for (int q = 0; q < 6; ++q) w.W[q] = W[q];
+  int64_t nt = (nv + 7) / 8, cubes = nt * nt * nt;
+  unsigned g = (unsigned)(cubes < 148 * 8 ? cubes : 148 * 8);
+  triples_sumw_kernel<<<g, 512, 0, (cudaStream_t)s>>>(nv, w, K);
+  return launched();
+}
+
+// X = (4K_abc - 2K_acb - 2K_cba - 2K_bac + K_cab + K_bca) / D for one 8^3 cube per
+// block; the six permuted K cubes are staged through shared memory.
+__global__ void __launch_bounds__(512) triples_x_cube_kernel(int nv, const double* __restrict__ K,
+                                                            double eijk,
+                                                            const double* __restrict__ ev,
+                                                            double* __restrict__ X,
+                                                            double* part, int want_e) {
+  __shared__ double cube[6][8 * 9 * 9];
+  __shared__ double sh[32];
+  const int64_t v = nv, nt = (v + 7) / 8;
+  const int tx = threadIdx.x & 7, ty = (threadIdx.x >> 3) & 7, tz = threadIdx.x >> 6;
+  const int loc[3] = {tx, ty, tz};
+  // K permutations in X: (a,b,c) (a,c,b) (c,b,a) (b,a,c) (c,a,b) (b,c,a)
+  const int P[6][3] = {{0, 1, 2}, {0, 2, 1}, {2, 1, 0}, {1, 0, 2}, {2, 0, 1}, {1, 2, 0}};
+  const double cf[6] = {4.0, -2.0, -2.0, -2.0, 1.0, 1.0};
+  double eacc = 0.0;
+  for (int64_t t = blockIdx.x; t < nt * nt * nt; t += gridDim.x) {
+    const int64_t o[3] = {(t % nt) * 8, ((t / nt) % nt) * 8, (t / (nt * nt)) * 8};
+    for (int q = 0; q < 6; ++q) {
+      const int64_t x = o[P[q][0]] + tx, y = o[P[q][1]] + ty, z = o[P[q][2]] + tz;
+      cube[q][tx + 9 * (ty + 9 * tz)] = (x < v && y < v && z < v) ? K[x + v * y + v * v * z] : 0.0;
+    }
+    __syncthreads();
+    const int64_t a = o[0] + tx, b = o[1] + ty, c = o[2] + tz;
+    if (a < v && b < v && c < v) {
+      double x = 0.0;
+#pragma unroll
+      for (int q = 0; q < 6; ++q)
+        x += cf[q] * cube[q][loc[P[q][0]] + 9 * (loc[P[q][1]] + 9 * loc[P[q][2]])];
+      x /= (eijk - ev[a] - ev[b] - ev[c]);
+      X[a + v * b + v * v * c] = x;
+      eacc += cube[0][tx + 9 * (ty + 9 * tz)] * x;
+    }
+    __syncthreads();
+  }
+  if (want_e) {
+    double r = block_sum(eacc, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = r;
+  }
+}
+
+int triples_x_cube(stream_t s, int nv, const double* K, double eijk, const double* ev, double* X,
+                   double* scratch, double* eout) {
+  cudaStream_t st = (cudaStream_t)s;
+  int64_t nt = (nv + 7) / 8, cubes = nt * nt * nt;
+  int g = (int)(cubes < RED_BLOCKS ? cubes : RED_BLOCKS);
+  triples_x_cube_kernel<<<g, 512, 0, st>>>(nv, K, eijk, ev, X, scratch, eout ? 1 : 0);
+  int e = launched();
+  if (e || !eout) return e;
+  final_sum_kernel<<<1, 256, 0, st>>>(g, 1, scratch, eout);
   return launched();
 }
 

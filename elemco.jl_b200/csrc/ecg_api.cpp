@@ -215,6 +215,11 @@ int ecg_cc_step(ecg_ctx* c, int dc, int32_t nsteps, double* out) {
     need_system(*c);
     if (c->diis.len == 0) throw Error(ECG_ERR_STATE, "call ecg_cc_load first");
     IterResult r{};
+    c->mixed_active = (c->prec == ECG_PREC_MIXED);
+    struct Restore {
+      Ctx& c;
+      ~Restore() { c.mixed_active = false; }
+    } restore{*c};
     for (int32_t k = 0; k < nsteps; ++k) r = cc_iteration(*c, dc != 0);
     if (out) {
       out[0] = r.E;
@@ -249,8 +254,21 @@ int ecg_cc_solve(ecg_ctx* c, int dc, const ecg_cc_opts* opts, double* T1, double
     IterResult r{};
     int it = 0;
     bool conv = false;
+    // ECG_PREC_MIXED: iterate with split-BF16 tensor-core products until the
+    // squared residual is below 100 thr, then refine with FP64 iterations;
+    // convergence is only declared on an FP64 residual.
+    bool mixed_phase = (c->prec == ECG_PREC_MIXED);
+    struct Restore {
+      Ctx& c;
+      ~Restore() { c.mixed_active = false; }
+    } restore{*c};
     for (it = 1; it <= o.maxit; ++it) {
+      c->mixed_active = mixed_phase;
       r = cc_iteration(*c, dc != 0);
+      if (mixed_phase) {
+        if (r.normR < 100.0 * o.thr) mixed_phase = false;
+        continue;
+      }
       if (r.normR < o.thr && std::fabs(r.dE) < thren) {
         conv = true;
         break;
@@ -278,6 +296,11 @@ int ecg_pert_t(ecg_ctx* c, const double* T1, const double* T2, double* e_t, doub
     need_system(*c);
     load_T(*c, T1, T2);
     double et = 0, etb = 0;
+    c->mixed_active = (c->prec == ECG_PREC_MIXED);
+    struct Restore {
+      Ctx& c;
+      ~Restore() { c.mixed_active = false; }
+    } restore{*c};
     pert_triples(*c, nullptr, nullptr, &et, &etb);
     if (e_t) *e_t = et;
     if (e_tb) *e_tb = etb;
@@ -295,6 +318,11 @@ int ecg_lambda_pert_t(ecg_ctx* c, const double* T1, const double* T2, const doub
     check_finite(U1, c->n1(), "U1");
     check_finite(U2, c->n2(), "U2");
     double et = 0, etb = 0;
+    c->mixed_active = (c->prec == ECG_PREC_MIXED);
+    struct Restore {
+      Ctx& c;
+      ~Restore() { c.mixed_active = false; }
+    } restore{*c};
     pert_triples(*c, U1, U2, &et, &etb);
     if (e_t) *e_t = et;
     if (e_tb) *e_tb = etb;

@@ -70,6 +70,13 @@ double scal(Ctx& c, int i) { return c.hscal[i]; }
 void sync_scalars(Ctx& c, int count) {
   check(dev::d2h(c.hscal, c.dscal, sizeof(double) * count, c.st), "d2h scalars");
   check(dev::sync(c.st), "stream sync");
+  if (c.prec == ECG_PREC_MIXED) {
+    int tc = 0;
+    check(dev::tc_error(&tc), "tc_error");
+    if (tc)
+      throw Error(ECG_ERR_TIMEOUT,
+                  "tensor-core GEMM wait timed out (code " + std::to_string(tc) + ")");
+  }
 }
 
 // --------------------------------------------------------------- setup
@@ -316,15 +323,17 @@ void ladder(Ctx& c, const double* Bf, const double* BfT, const double* T2, doubl
   for (auto& b : c.lblocks) {
     const int64_t nb = v - b.a0;
     // V[c,a',d,b''] = sum_Q BfT[c,a0+a',Q] BfT[d,a0+b'',Q]
-    check(dev::gemm(s, 'N', 'T', v * b.na, v * nb, Q, 1.0, BfT + v * b.a0, v * v, BfT + v * b.a0,
-                    v * v, 0.0, V, v * b.na),
+    check(gemm_prec(c.mixed_active, s, 'N', 'T', v * b.na, v * nb, Q, 1.0, BfT + v * b.a0, v * v,
+                    BfT + v * b.a0, v * v, 0.0, V, v * b.na),
           "gemm ladder V");
     const int* pairs = c.pairs + 2 * b.poff;
     check(dev::ladder_pack_v(s, (int)v, b.a0, b.na, b.npp, pairs, c.cdp, V, Vp, Vm), "pack V");
-    check(dev::gemm(s, 'T', 'N', b.npp, nijp, ncdp, 1.0, Vp, ncdp, Ts, ncdp, 0.0, Lp, b.npp),
+    check(gemm_prec(c.mixed_active, s, 'T', 'N', b.npp, nijp, ncdp, 1.0, Vp, ncdp, Ts, ncdp, 0.0,
+                    Lp, b.npp),
           "gemm ladder +");
     if (b.npm > 0 && nijm > 0)
-      check(dev::gemm(s, 'T', 'N', b.npm, nijm, ncdm, 1.0, Vm, ncdm, Ta, ncdm, 0.0, Lm, b.npm),
+      check(gemm_prec(c.mixed_active, s, 'T', 'N', b.npm, nijm, ncdm, 1.0, Vm, ncdm, Ta, ncdm,
+                      0.0, Lm, b.npm),
             "gemm ladder -");
     check(dev::ladder_unpack(s, (int)v, (int)o, b.a0, b.npp, pairs, c.ijp, Lp, Lm, R2),
           "ladder unpack");

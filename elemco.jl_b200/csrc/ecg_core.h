@@ -30,6 +30,7 @@ struct Ctx {
   uint64_t memcap = 0, memused = 0;
   std::vector<std::pair<void*, size_t>> allocs;
   int prec = ECG_PREC_FP64;
+  bool mixed_active = false;  // route large GEMMs to the split-BF16 tensor-core GEMM
 
   // system
   bool have_system = false;
@@ -90,7 +91,7 @@ struct Ctx {
   void release_to(size_t nallocs);  // free allocations made after the first nallocs
   void ensure_ws(int64_t ndoubles);  // grow the workspace arena (outside any capture)
   void free_all();
-  Contractor con() { return Contractor(st, &ws, &ext); }
+  Contractor con() { return Contractor(st, &ws, &ext, mixed_active); }
 };
 
 // ecg_cc.cpp

@@ -50,6 +50,8 @@ struct Gemm {
   int64_t scm = 1, scn = 0, scb = 0;
 };
 int gemm_strided(stream_t s, const Gemm& g);
+// Split-BF16 tensor-core version of gemm_strided (batch must be 1).
+int gemm_strided_mixed(stream_t s, const Gemm& g);
 
 // out = alpha * permute(in) + beta * out.  in has rank nd with dims
 // in_dims (column-major, first fastest); out dimension d is in dimension
@@ -100,6 +102,13 @@ int combine(stream_t s, int64_t n, int m, const double* const* X, const double* 
 //   *eout    = sum K*X  (skipped when eout == nullptr)
 int triples_x(stream_t s, int nv, const double* K, double eijk, const double* ev, double* X,
               double* scratch, double* eout);
+// K[a,b,c] = W0[a,b,c] + W1[b,a,c] + W2[a,c,b] + W3[c,b,a] + W4[b,c,a] + W5[c,a,b]
+// (the six index permutations of W^{ijk}, W^{jik}, W^{ikj}, W^{kji}, W^{jki},
+// W^{kij}); 8^3 cubes staged through shared memory.
+int triples_sumw(stream_t s, int nv, const double* const* W, double* K);
+// Cube-tiled variant of triples_x (same result).
+int triples_x_cube(stream_t s, int nv, const double* K, double eijk, const double* ev, double* X,
+                   double* scratch, double* eout);
 // IntX[:,i] += fac X.M_jk, IntX[:,j] += fac X.M_ik, IntX[:,k] += fac X.M_ij and the same for
 // IntY with N_*; M/N are nv x nv slices.  One block per virtual index, fixed order.
 int triples_int(stream_t s, int nv, const double* X, const double* Mjk, const double* Mik,
@@ -121,6 +130,11 @@ int gemm_mixed(stream_t s, char ta, char tb, int64_t m, int64_t n, int64_t k, do
                const double* A, int64_t lda, const double* B, int64_t ldb, double beta,
                double* C, int64_t ldc);
 int tc_error(int* code);
+// Shared split-K scratch (grown on demand) and its fixed-order reduction
+// C(i,j) = alpha sum_z P[z][i + j m] + beta C(i,j), C at C[i*scm + j*scn].
+double* splitk_buffer(size_t n);
+int splitk_reduce(stream_t s, int64_t m, int64_t n, int S, const double* P, double alpha,
+                  double beta, double* C, int64_t scm, int64_t scn);
 
 // GEMM event timing (process-wide): enable, then read and reset the totals.
 void gemm_timing(bool enable);

@@ -11,6 +11,14 @@ void check(int code, const char* what) {
   if (code != 0) throw Error(ECG_ERR_CUDA, std::string(what) + ": " + dev::error_string(code));
 }
 
+int gemm_prec(bool mixed, dev::stream_t s, char ta, char tb, int64_t m, int64_t n, int64_t k,
+              double alpha, const double* A, int64_t lda, const double* B, int64_t ldb,
+              double beta, double* C, int64_t ldc) {
+  if (mixed && (double)m * (double)n * (double)k >= 67108864.0)
+    return dev::gemm_mixed(s, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+  return dev::gemm(s, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+}
+
 double* Arena::get(int64_t n) {
   int64_t need = (n + 31) & ~int64_t(31);  // 256-byte granularity
   if (top_ + need > cap_)
@@ -143,12 +151,14 @@ void Contractor::operator()(double alpha, const double* A, const char* ia_, cons
     cbeta = 0.0;
   }
   if (!bCT) {
-    check(dev::gemm(s_, ta, tb, mM, mN, mK, alpha, Ap, lda, Bp, ldb, cbeta, Cp, mM), "gemm");
+    check(gemm_prec(mixed_, s_, ta, tb, mM, mN, mK, alpha, Ap, lda, Bp, ldb, cbeta, Cp, mM),
+          "gemm");
   } else {
     // C^T(N,M) = opB^T (N,K) * opA^T (K,M)
     char tb2 = (tb == 'N') ? 'T' : 'N';
     char ta2 = (ta == 'N') ? 'T' : 'N';
-    check(dev::gemm(s_, tb2, ta2, mN, mM, mK, alpha, Bp, ldb, Ap, lda, cbeta, Cp, mN), "gemm");
+    check(gemm_prec(mixed_, s_, tb2, ta2, mN, mM, mK, alpha, Bp, ldb, Ap, lda, cbeta, Cp, mN),
+          "gemm");
   }
   if (cperm) permute(1.0, Cp, cform.c_str(), beta, C, ic_);
   ws_->release(mark);

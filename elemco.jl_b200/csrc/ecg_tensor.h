@@ -49,9 +49,16 @@ struct Extents {
   int64_t operator()(char c) const;
 };
 
+// FP64 GEMM, or — when `mixed` and the product has at least 2^26 multiply-adds —
+// the split-BF16 tensor-core GEMM (FP32-level accuracy).
+int gemm_prec(bool mixed, dev::stream_t s, char ta, char tb, int64_t m, int64_t n, int64_t k,
+              double alpha, const double* A, int64_t lda, const double* B, int64_t ldb,
+              double beta, double* C, int64_t ldc);
+
 class Contractor {
  public:
-  Contractor(dev::stream_t s, Arena* ws, const Extents* ext) : s_(s), ws_(ws), ext_(ext) {}
+  Contractor(dev::stream_t s, Arena* ws, const Extents* ext, bool mixed = false)
+      : s_(s), ws_(ws), ext_(ext), mixed_(mixed) {}
   void operator()(double alpha, const double* A, const char* ia, const double* B,
                   const char* ib, double beta, double* C, const char* ic);
   // out[io] = alpha * in[ii] + beta * out[io]   (pure permutation)
@@ -63,6 +70,7 @@ class Contractor {
   dev::stream_t s_;
   Arena* ws_;
   const Extents* ext_;
+  bool mixed_;
 };
 
 void check(int code, const char* what);

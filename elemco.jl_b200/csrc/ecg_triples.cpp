@@ -1,14 +1,16 @@
 // ecg_triples.cpp — closed-shell (T) and Lambda-(T).
 //
 // For each occupied triplet i <= j <= k (i = j = k skipped, weights 2/1 as in
-// cc_triples.jl:62-72) K[a,b,c] is accumulated from the 12 contractions of
-// cc_triples.jl:89-104, each one strided batched FP64 GEMM reading the
-// integrals in place:
-//   V[b,d,c,k] = (bd|ck) = <bc|dk>  (the reference's vvvo[b,c,d,k])
-//   O[l,j,c,k] = (lj|ck) = <lc|jk>  (the reference's ovoo[l,c,j,k])
-// both built once from the DF factors.  A fused kernel forms X and sum K*X,
-// a second one accumulates IntX/IntY.  Per-triplet energies are summed on the
-// host in triplet order, so the result is deterministic.
+// cc_triples.jl:62-72) the 12 contractions of cc_triples.jl:89-104 are
+// regrouped as K = P[W]:
+//   W^{xyz}[a,b,c] = sum_d T^{xy}_{ad} (bd|cz) - sum_l T^{xl}_{ab} (ly|cz)
+//   K[a,b,c] = W^{ijk}[a,b,c] + W^{jik}[b,a,c] + W^{ikj}[a,c,b]
+//            + W^{kji}[c,b,a] + W^{jki}[b,c,a] + W^{kij}[c,a,b]
+// so each W is two plain GEMMs (M=v N=v^2 K=v and M=v^2 N=v K=o) that read
+// vvvo[b,c,d,k] = <bc|dk> and ovoo in place, and a cube-tiled kernel sums the
+// six permuted W's.  A fused kernel forms X and sum K*X, another accumulates
+// IntX/IntY.  Per-triplet energies are summed on the host in triplet order,
+// so the result is deterministic.
 #include "ecg_triples.h"
 
 #include <cmath>
@@ -18,112 +20,33 @@ namespace ecg {
 
 namespace {
 
-struct TriplesCtx {
-  int64_t o, v;
-  const double* T2;  // amplitudes entering K
-  const double* Vn;
-  const double* On;
-};
-
-// K[a,b,c] (+)= the 12 terms of cc_triples.jl:89-104 for amplitudes tc.T2.
-void build_K(Ctx& c, const TriplesCtx& t, double* K, int i, int j, int k) {
-  const int64_t o = t.o, v = t.v, v2 = v * v, v3 = v2 * v, o2 = o * o;
+// W^{xyz} for amplitudes T (T2 or covariant U2) into Wout.
+void build_W(Ctx& c, const double* T, const double* V3, const double* On, double* Wout, int x,
+             int y, int z) {
+  const int64_t o = c.no, v = c.nv, v2 = v * v, v3 = v2 * v, o2 = o * o;
   dev::stream_t s = c.st;
-  check(dev::memset0(K, v3 * 8, s), "memset K");
-  auto Tij = [&](int x, int y) { return t.T2 + v2 * (x + o * y); };   // T2[:,:,x,y]
-  auto Tx = [&](int x) { return t.T2 + v2 * o * x; };                 // T2[:,:,:,x]
-  auto Vx = [&](int x) { return t.Vn + v3 * x; };                     // vvvo[:,:,:,x]
-  auto Oxy = [&](int x, int y) { return t.On + o * x + o2 * v * y; };  // ovoo[:,:,x,y]
-  auto run = [&](dev::Gemm g, const char* what) {
-    g.beta = 1.0;
-    g.C = K;
-    check(dev::gemm_strided(s, g), what);
-  };
   dev::Gemm g;
-  // 1. T2ij[a,d] vvvk[b,c,d]      M=a N=b K=d batch c
+  // W[a,(b,c)] = sum_d T[a,d,x,y] vvvo[(b,c),d,z]
+  g.m = v; g.n = v2; g.k = v; g.alpha = 1.0; g.beta = 0.0;
+  g.A = T + v2 * (x + o * y); g.sam = 1; g.sak = v;
+  g.B = V3 + v3 * z; g.sbk = v2; g.sbn = 1;
+  g.C = Wout; g.scm = 1; g.scn = v;
+  check(c.mixed_active ? dev::gemm_strided_mixed(s, g) : dev::gemm_strided(s, g), "W vvvo");
+  // W[(a,b),c] -= sum_l T[a,b,x,l] ovoo[l,c,y,z]
   g = dev::Gemm{};
-  g.m = v; g.n = v; g.k = v; g.batch = v; g.alpha = 1.0;
-  g.A = Tij(i, j); g.sam = 1; g.sak = v; g.sab = 0;
-  g.B = Vx(k); g.sbk = v; g.sbn = 1; g.sbb = v2;
-  g.scm = 1; g.scn = v; g.scb = v2;
-  run(g, "K1");
-  // 2. T2ij[d,b] vvvk[a,c,d]      M=a N=b K=d batch c
-  g = dev::Gemm{};
-  g.m = v; g.n = v; g.k = v; g.batch = v; g.alpha = 1.0;
-  g.A = Vx(k); g.sam = 1; g.sak = v; g.sab = v2;
-  g.B = Tij(i, j); g.sbk = 1; g.sbn = v; g.sbb = 0;
-  g.scm = 1; g.scn = v; g.scb = v2;
-  run(g, "K2");
-  // 3. T2ik[a,d] vvvj[c,b,d]      M=a N=c K=d batch b
-  g = dev::Gemm{};
-  g.m = v; g.n = v; g.k = v; g.batch = v; g.alpha = 1.0;
-  g.A = Tij(i, k); g.sam = 1; g.sak = v; g.sab = 0;
-  g.B = Vx(j); g.sbk = v; g.sbn = 1; g.sbb = v2;
-  g.scm = 1; g.scn = v2; g.scb = v;
-  run(g, "K3");
-  // 4. T2ik[d,c] vvvj[a,b,d]      M=a N=c K=d batch b
-  g = dev::Gemm{};
-  g.m = v; g.n = v; g.k = v; g.batch = v; g.alpha = 1.0;
-  g.A = Vx(j); g.sam = 1; g.sak = v; g.sab = v2;
-  g.B = Tij(i, k); g.sbk = 1; g.sbn = v; g.sbb = 0;
-  g.scm = 1; g.scn = v2; g.scb = v;
-  run(g, "K4");
-  // 5. T2jk[b,d] vvvi[c,a,d]      M=b N=c K=d batch a
-  g = dev::Gemm{};
-  g.m = v; g.n = v; g.k = v; g.batch = v; g.alpha = 1.0;
-  g.A = Tij(j, k); g.sam = 1; g.sak = v; g.sab = 0;
-  g.B = Vx(i); g.sbk = v; g.sbn = 1; g.sbb = v2;
-  g.scm = v; g.scn = v2; g.scb = 1;
-  run(g, "K5");
-  // 6. T2jk[d,c] vvvi[b,a,d]      M=b N=c K=d batch a
-  g = dev::Gemm{};
-  g.m = v; g.n = v; g.k = v; g.batch = v; g.alpha = 1.0;
-  g.A = Vx(i); g.sam = 1; g.sak = v; g.sab = v2;
-  g.B = Tij(j, k); g.sbk = 1; g.sbn = v; g.sbb = 0;
-  g.scm = v; g.scn = v2; g.scb = 1;
-  run(g, "K6");
-  // 7. -T2i[b,a,l] ovjk[l,c]      M=b N=c K=l batch a
-  g = dev::Gemm{};
-  g.m = v; g.n = v; g.k = o; g.batch = v; g.alpha = -1.0;
-  g.A = Tx(i); g.sam = 1; g.sak = v2; g.sab = v;
-  g.B = Oxy(j, k); g.sbk = 1; g.sbn = o2; g.sbb = 0;
-  g.scm = v; g.scn = v2; g.scb = 1;
-  run(g, "K7");
-  // 8. -T2j[a,b,l] ovik[l,c]      M=(a,b) N=c K=l
-  g = dev::Gemm{};
-  g.m = v2; g.n = v; g.k = o; g.batch = 1; g.alpha = -1.0;
-  g.A = Tx(j); g.sam = 1; g.sak = v2;
-  g.B = Oxy(i, k); g.sbk = 1; g.sbn = o2;
-  g.scm = 1; g.scn = v2;
-  run(g, "K8");
-  // 9. -T2i[c,a,l] ovkj[l,b]      M=c N=b K=l batch a
-  g = dev::Gemm{};
-  g.m = v; g.n = v; g.k = o; g.batch = v; g.alpha = -1.0;
-  g.A = Tx(i); g.sam = 1; g.sak = v2; g.sab = v;
-  g.B = Oxy(k, j); g.sbk = 1; g.sbn = o2; g.sbb = 0;
-  g.scm = v2; g.scn = v; g.scb = 1;
-  run(g, "K9");
-  // 10. -T2k[a,c,l] ovij[l,b]     M=a N=b K=l batch c
-  g = dev::Gemm{};
-  g.m = v; g.n = v; g.k = o; g.batch = v; g.alpha = -1.0;
-  g.A = Tx(k); g.sam = 1; g.sak = v2; g.sab = v;
-  g.B = Oxy(i, j); g.sbk = 1; g.sbn = o2; g.sbb = 0;
-  g.scm = 1; g.scn = v; g.scb = v2;
-  run(g, "K10");
-  // 11. -T2j[c,b,l] ovki[l,a]     M=c N=a K=l batch b
-  g = dev::Gemm{};
-  g.m = v; g.n = v; g.k = o; g.batch = v; g.alpha = -1.0;
-  g.A = Tx(j); g.sam = 1; g.sak = v2; g.sab = v;
-  g.B = Oxy(k, i); g.sbk = 1; g.sbn = o2; g.sbb = 0;
-  g.scm = v2; g.scn = 1; g.scb = v;
-  run(g, "K11");
-  // 12. -T2k[b,c,l] ovji[l,a]     M=(b,c) N=a K=l
-  g = dev::Gemm{};
-  g.m = v2; g.n = v; g.k = o; g.batch = 1; g.alpha = -1.0;
-  g.A = Tx(k); g.sam = 1; g.sak = v2;
-  g.B = Oxy(j, i); g.sbk = 1; g.sbn = o2;
-  g.scm = v; g.scn = 1;
-  run(g, "K12");
+  g.m = v2; g.n = v; g.k = o; g.alpha = -1.0; g.beta = 1.0;
+  g.A = T + v2 * x; g.sam = 1; g.sak = v2 * o;
+  g.B = On + o * y + o2 * v * z; g.sbk = 1; g.sbn = o2;
+  g.C = Wout; g.scm = 1; g.scn = v2;
+  check(c.mixed_active ? dev::gemm_strided_mixed(s, g) : dev::gemm_strided(s, g), "W ovoo");
+}
+
+// K^{ijk} = P[W] for amplitudes T.
+void build_K(Ctx& c, const double* T, const double* V3, const double* On, double* const* W,
+             double* K, int i, int j, int k) {
+  const int perm[6][3] = {{i, j, k}, {j, i, k}, {i, k, j}, {k, j, i}, {j, k, i}, {k, i, j}};
+  for (int q = 0; q < 6; ++q) build_W(c, T, V3, On, W[q], perm[q][0], perm[q][1], perm[q][2]);
+  check(dev::triples_sumw(c.st, (int)c.nv, W, K), "sum W");
 }
 
 }  // namespace
@@ -138,8 +61,10 @@ void pert_triples(Ctx& c, const double* U1h, const double* U2h, double* et, doub
     size_t n0;
     ~Scope() { c.release_to(n0); }
   } scope{c, c.allocs.size()};
-  double* Vn = c.alloc(v3 * o, "(T) vvvo");
+  double* V3 = c.alloc(v3 * o, "(T) vvvo");
   double* On = c.alloc(o * o * o * v, "(T) ovoo");
+  double* Wb[6];
+  for (int q = 0; q < 6; ++q) Wb[q] = c.alloc(v3, "(T) W");
   double* K = c.alloc(v3, "(T) K");
   double* X = c.alloc(v3, "(T) X");
   double* KU = lam ? c.alloc(v3, "(T) K(Lambda)") : nullptr;
@@ -153,7 +78,15 @@ void pert_triples(Ctx& c, const double* U1h, const double* U2h, double* et, doub
         if (!(ii == jj && jj == kk)) ++ntrip;
   double* Et = c.alloc(std::max<int64_t>(ntrip, 1), "(T) energies");
   Contractor con = c.con();
-  con(1.0, c.Bvv, "bdQ", c.Bvo, "ckQ", 0.0, Vn, "bdck");
+  // vvvo[b,c,d,k] = (bd|ck): per k, a GEMM batched over d
+  for (int64_t kk = 0; kk < o; ++kk) {
+    dev::Gemm g;
+    g.m = v; g.n = v; g.k = Q; g.batch = v; g.alpha = 1.0; g.beta = 0.0;
+    g.A = c.Bvv; g.sam = 1; g.sak = v * v; g.sab = v;
+    g.B = c.Bvo + v * kk; g.sbk = v * o; g.sbn = 1; g.sbb = 0;
+    g.C = V3 + v3 * kk; g.scm = 1; g.scn = v; g.scb = v * v;
+    check(dev::gemm_strided(s, g), "vvvo");
+  }
   con(1.0, c.Boo, "ljQ", c.Bvo, "ckQ", 0.0, On, "ljck");
   check(dev::memset0(IntXY, 2 * v * o * 8, s), "memset");
   double* IntX = IntXY;
@@ -169,8 +102,6 @@ void pert_triples(Ctx& c, const double* U1h, const double* U2h, double* et, doub
   const double* eps = c.fock_host.data();
   const int64_t n = c.n;
   const double* ev = c.eps + o;
-  TriplesCtx tT{o, v, c.T2(), Vn, On};
-  TriplesCtx tU{o, v, U2c, Vn, On};
   const double* Nsrc = lam ? U2c : c.T2();
   int64_t t = 0;
   for (int k = 0; k < o; ++k)
@@ -183,12 +114,12 @@ void pert_triples(Ctx& c, const double* U1h, const double* U2h, double* et, doub
           f = 1.0;
         }
         const double eijk = eps[i + i * n] + eps[j + j * n] + eps[k + k * n];
-        build_K(c, tT, K, i, j, k);
+        build_K(c, c.T2(), V3, On, Wb, K, i, j, k);
         if (!lam) {
-          check(dev::triples_x(s, (int)v, K, eijk, ev, X, c.red, Et + t), "triples X");
+          check(dev::triples_x_cube(s, (int)v, K, eijk, ev, X, c.red, Et + t), "triples X");
         } else {
-          check(dev::triples_x(s, (int)v, K, eijk, ev, X, c.red, nullptr), "triples X");
-          build_K(c, tU, KU, i, j, k);
+          check(dev::triples_x_cube(s, (int)v, K, eijk, ev, X, c.red, nullptr), "triples X");
+          build_K(c, U2c, V3, On, Wb, KU, i, j, k);
           check(dev::dot(s, v3, KU, X, c.red, Et + t), "triples E");
         }
         const int64_t v2 = v * v;
@@ -207,6 +138,11 @@ void pert_triples(Ctx& c, const double* U1h, const double* U2h, double* et, doub
   std::vector<double> T1h(v * o);
   check(dev::d2h(T1h.data(), c.T1(), v * o * 8, s), "d2h");
   check(dev::sync(s), "sync");
+  if (c.mixed_active) {
+    int tc = 0;
+    check(dev::tc_error(&tc), "tc_error");
+    if (tc) throw Error(ECG_ERR_TIMEOUT, "tensor-core GEMM wait timed out in (T)");
+  }
   double Enb3 = 0.0;
   for (int64_t q = 0; q < ntrip; ++q) Enb3 += fac[q] * Eh[q];
   // singles and Fock contributions (cc_triples.jl:143-156 / :286-294)

@@ -5,7 +5,9 @@ engine is available: ``B[p,q,Q]`` is symmetric in (p,q) with a geometric
 decay of the auxiliary weights (1 -> 1e-6 over Q), orbital energies are drawn
 uniformly from [-1.4, -0.4] Eh (occupied) and [0.1, 4.0] Eh (virtual), and the
 one-electron matrix is chosen so that the Fock matrix built from B is exactly
-diag(eps) — a canonical Hartree-Fock reference.
+diag(eps) — a canonical Hartree-Fock reference.  B is scaled so that the MP2
+correlation energy is -0.05 Eh per occupied orbital (water: -0.2 Eh for four
+valence pairs), which keeps CCSD well conditioned at every size.
 
 Shapes of the named workloads (active orbitals after freezing O/C 1s):
   (H2O)_2/cc-pVDZ  o=8  v=38  nQ=168
@@ -26,17 +28,27 @@ WORKLOADS = {
 }
 
 
-def make_system(no, nv, nq, seed=1234, scale=0.35):
+def _mp2(B, eps, no):
+    o, v = slice(0, no), slice(no, None)
+    ovov = np.einsum("iaQ,jbQ->iajb", B[o, v, :], B[o, v, :], optimize=True)
+    D = (eps[o][:, None, None, None] - eps[v][None, :, None, None]
+         + eps[o][None, None, :, None] - eps[v][None, None, None, :])
+    return float(np.sum(ovov * (2.0 * ovov - ovov.transpose(0, 3, 2, 1)) / D))
+
+
+def make_system(no, nv, nq, seed=1234, emp2_per_occ=-0.05):
     """Return (B[p,q,Q] Fortran-ordered, h1, e0, eps)."""
     rng = np.random.default_rng(seed)
     n = no + nv
     eps = np.concatenate([np.sort(rng.uniform(-1.4, -0.4, no)),
                           np.sort(rng.uniform(0.1, 4.0, nv))])
-    w = scale * 10.0 ** (-6.0 * np.arange(nq) / max(nq - 1, 1))
+    w = 10.0 ** (-6.0 * np.arange(nq) / max(nq - 1, 1))
     B = np.empty((n, n, nq), order="F")
     for q in range(nq):
         G = rng.standard_normal((n, n))
         B[:, :, q] = w[q] * (G + G.T) / np.sqrt(2.0 * n)
+    # MP2 energy scales with the 4th power of B
+    B *= (emp2_per_occ * no / _mp2(B, eps, no)) ** 0.25
     # Fock from B:  f = h + 2 J - K  with the occupied block; choose h so f = diag(eps)
     o = slice(0, no)
     Jq = np.einsum("kkQ->Q", B[o, o, :])

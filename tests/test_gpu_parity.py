@@ -206,7 +206,7 @@ def test_diis_standalone(ctx, h2o_df):
 @pytest.mark.parametrize("ta,tb,m,n,k", [("N", "N", 1, 1, 1), ("N", "N", 128, 128, 64),
                                          ("N", "T", 200, 130, 100), ("T", "N", 300, 257, 700),
                                          ("T", "T", 129, 65, 1000), ("N", "N", 1216, 1216, 1216),
-                                         ("T", "N", 2926, 136, 2926)])
+                                         ("T", "N", 2926, 136, 2926), ("N", "T", 2000, 3000, 320)])
 def test_mixed_gemm_kernel(ta, tb, m, n, k):
     """Split-BF16 tcgen05 GEMM: FP32-level error, below 4 (k/16 + 16) 2^-24 of
     sum |a||b| (the bound of FP32 accumulation over k/16 MMA steps)."""
@@ -224,3 +224,44 @@ def test_mixed_gemm_kernel(ta, tb, m, n, k):
         out = c.diag_gemm(ta, tb, 0.7, A, B, -0.3, C)
     err = np.abs(out - ref) / scale
     assert err.max() < 4.0 * (k / 16 + 16) * 2.0 ** -24, err.max()
+
+
+@pytest.mark.parametrize("dc", [False, True])
+def test_mixed_precision_solve_within_1_uEh(dc):
+    """ECG_PREC_MIXED (split-BF16 tensor-core products, then FP64 refinement)
+    converges to the FP64 energy within 1 microhartree on an (H2O)_3/cc-pVDZ-
+    sized system, where the ring and ladder GEMMs take the tensor-core path."""
+    import ecgpu
+    from ecgpu.synthetic import make_workload
+    B, h1, e0, no = make_workload("h2o3_vdz")
+    out = {}
+    for prec in (ecgpu.ECG_PREC_FP64, ecgpu.ECG_PREC_MIXED):
+        with ecgpu.Context(0) as c:
+            c.set_precision(prec)
+            c.set_system(B, h1, e0, no)
+            _, T1, T2 = c.mp2()
+            r = c.cc_solve(T1, T2, dc=dc)
+            assert r["converged"]
+            out[prec] = r
+    dE = abs(out[ecgpu.ECG_PREC_MIXED]["E"] - out[ecgpu.ECG_PREC_FP64]["E"])
+    assert dE < 1e-6, dE
+
+
+def test_mixed_precision_triples():
+    """(T) and Lambda-(T) with split-BF16 tensor-core W products agree with FP64
+    to 1e-8 Eh on the (H2O)_3/cc-pVDZ-sized system."""
+    import ecgpu
+    from ecgpu.synthetic import make_workload
+    B, h1, e0, no = make_workload("h2o3_vdz")
+    with ecgpu.Context(0) as c:
+        c.set_system(B, h1, e0, no)
+        _, T1, T2 = c.mp2()
+        r = c.cc_solve(T1, T2)
+        lr = c.lambda_solve(r["T1"], r["T2"])
+        e64 = c.pert_t(r["T1"], r["T2"])
+        l64 = c.lambda_pert_t(r["T1"], r["T2"], lr["U1"], lr["U2"])
+        c.set_precision(ecgpu.ECG_PREC_MIXED)
+        emx = c.pert_t(r["T1"], r["T2"])
+        lmx = c.lambda_pert_t(r["T1"], r["T2"], lr["U1"], lr["U2"])
+    assert abs(emx[0] - e64[0]) < 1e-8 and abs(emx[1] - e64[1]) < 1e-8
+    assert abs(lmx[0] - l64[0]) < 1e-8
