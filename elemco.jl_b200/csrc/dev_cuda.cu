@@ -17,6 +17,7 @@ namespace dev {
 
 static std::atomic<int64_t> g_launches{0};
 int64_t launches() { return g_launches.load(); }
+void note_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 static inline int launched() {
   g_launches.fetch_add(1, std::memory_order_relaxed);
   return (int)cudaGetLastError();
@@ -91,6 +92,12 @@ struct GemmArgs {
   double alpha, beta;
   int a_kfast, b_nfast;  // loader thread order follows the unit-stride index
   int64_t klast;         // split-K: depth of the last z-slice (0 = all slices use k)
+  int64_t dn = 0, scn2 = 0;  // dn > 0: column n at (n % dn)*scn + (n / dn)*scn2
+  int64_t kseg = 0;          // kseg > 0: k >= kseg reads A1/B1 with strides sak1/sbk1
+  const double* A1 = nullptr;
+  int64_t sak1 = 0;
+  const double* B1 = nullptr;
+  int64_t sbk1 = 0;
 };
 
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool pred) {
@@ -159,7 +166,10 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, BK, WM, WN, STAGES>::THREADS, 
         if (!g.a_kfast) { mm = e % BM; kk = e / BM; } else { kk = e % BK; mm = e / BK; }
         int64_t gm = m0 + mm, gk = k0 + kk;
         bool ok = gm < g.m && gk < kdep;
-        const double* src = ok ? A + gm * g.sam + gk * g.sak : A;
+        const double* src = A;
+        if (ok)
+          src = (g.kseg > 0 && gk >= g.kseg) ? g.A1 + gm * g.sam + (gk - g.kseg) * g.sak1
+                                              : A + gm * g.sam + gk * g.sak;
         cp_async8(as + kk * Cfg::LDA_S + mm, src, ok);
       }
     }
@@ -171,7 +181,10 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, BK, WM, WN, STAGES>::THREADS, 
         if (!g.b_nfast) { kk = e % BK; nn = e / BK; } else { nn = e % BN; kk = e / BN; }
         int64_t gn = n0 + nn, gk = k0 + kk;
         bool ok = gn < g.n && gk < kdep;
-        const double* src = ok ? B + gk * g.sbk + gn * g.sbn : B;
+        const double* src = B;
+        if (ok)
+          src = (g.kseg > 0 && gk >= g.kseg) ? g.B1 + (gk - g.kseg) * g.sbk1 + gn * g.sbn
+                                              : B + gk * g.sbk + gn * g.sbn;
         cp_async8(bs + kk * Cfg::LDB_S + nn, src, ok);
       }
     }
@@ -211,6 +224,14 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, BK, WM, WN, STAGES>::THREADS, 
   }
   cp_async_wait<0>();
 
+  int64_t coff[NTL][2];
+#pragma unroll
+  for (int j = 0; j < NTL; ++j)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int64_t col = n0 + wn0 + j * 8 + 2 * tq + h;
+      coff[j][h] = g.dn > 0 ? (col % g.dn) * g.scn + (col / g.dn) * g.scn2 : col * g.scn;
+    }
 #pragma unroll
   for (int i = 0; i < MT; ++i) {
     int64_t row = m0 + wm0 + i * 8 + gq;
@@ -221,7 +242,7 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, BK, WM, WN, STAGES>::THREADS, 
       for (int h = 0; h < 2; ++h) {
         int64_t col = n0 + wn0 + j * 8 + 2 * tq + h;
         if (col < g.n) {
-          double* cp = C + row * g.scm + col * g.scn;
+          double* cp = C + row * g.scm + coff[j][h];
           double v = g.alpha * acc[i][j][h];
           if (g.beta != 0.0) v += g.beta * *cp;
           *cp = v;
@@ -415,6 +436,18 @@ static int gemm_launch(stream_t s, const Gemm& q) {
   GemmArgs g{q.A, q.B, q.C, q.m, q.n, q.k, q.sam, q.sak, q.sab, q.sbk, q.sbn, q.sbb,
              q.scm, q.scn, q.scb, q.alpha, q.beta, (q.sam != 1 && q.sak == 1) ? 1 : 0,
              (q.sbk != 1 && q.sbn == 1) ? 1 : 0, 0};
+  if (q.dn > 0 || q.kseg > 0) {
+    if (q.batch != 1 || (q.kseg > 0 && (q.kseg >= q.k || !q.A1 || !q.B1)))
+      return (int)cudaErrorInvalidValue;
+    g.dn = q.dn;
+    g.scn2 = q.scn2;
+    g.kseg = q.kseg;
+    g.A1 = q.A1;
+    g.sak1 = q.sak1;
+    g.B1 = q.B1;
+    g.sbk1 = q.sbk1;
+    return launch_gemm<64, 64, 16, 32, 32, 3, 3>(g, 1, st);
+  }
   // Split-K for GEMMs whose output covers too few tiles to fill the SMs:
   // each z-slice writes a partial product, a fixed-order reduction sums them.
   const int64_t tiles64 = ((q.m + 63) / 64) * ((q.n + 63) / 64);
@@ -885,167 +918,224 @@ int ladder_unpack(stream_t s, int nv, int no, int a0, int npairs, const int* pai
 }
 
 // ---------------------------------------------------------------- (T)
+//
+// Permutations s of (0,1,2) in the order (012)(021)(102)(120)(201)(210).
+__host__ __device__ constexpr int perm3(int q, int d) {
+  return q == 0   ? d
+         : q == 1 ? (d == 0 ? 0 : 3 - d)
+         : q == 2 ? (d == 2 ? 2 : 1 - d)
+         : q == 3 ? (d == 0 ? 1 : d == 1 ? 2 : 0)
+         : q == 4 ? (d == 0 ? 2 : d - 1)
+                  : 2 - d;
+}
+__host__ __device__ constexpr int perm3_index(int t0, int t1) {
+  return 2 * t0 + (t0 == 0 ? (t1 == 2) : t0 == 1 ? (t1 == 2) : (t1 == 1));
+}
+// X terms: K at (a,b,c) (a,c,b) (c,b,a) (b,a,c) (c,a,b) (b,c,a), weights 4 -2 -2 -2 1 1
+__host__ __device__ constexpr int xp(int r, int d) {
+  return r == 0   ? d
+         : r == 1 ? (d == 0 ? 0 : 3 - d)
+         : r == 2 ? 2 - d
+         : r == 3 ? (d == 2 ? 2 : 1 - d)
+         : r == 4 ? (d == 0 ? 2 : d - 1)
+                  : (d == 2 ? 0 : d + 1);
+}
+// For the ordering q of an element, the ordering that X term r reads.
+__host__ __device__ constexpr int xcomp(int q, int r) {
+  return perm3_index(perm3(q, xp(r, 0)), perm3(q, xp(r, 1)));
+}
+// Index of the ordered position pair (x, y), x != y, in [0, 6).
+__host__ __device__ constexpr int pair_index(int x, int y) { return 2 * x + (y > x ? y - 1 : y); }
 
-__global__ void triples_x_kernel(int nv, const double* __restrict__ K, double eijk,
-                                 const double* __restrict__ ev, double* __restrict__ X,
-                                 double* part, int want_e) {
+constexpr int TCUBE = 8;
+constexpr int TPITCH = 9;                             // padded row pitch of a staged cube
+constexpr int TCUBE_ELEMS = TCUBE * TPITCH * TPITCH;  // 648
+constexpr int TS_MAT = 6 * 6 * 64;  // M0 M1 M2 N0 N1 N2 over the 6 ordered block pairs
+constexpr int TS_VEC = 7 * 3 * 8;   // g0 g1 g2 f0 f1 f2 ev over the 3 blocks
+constexpr int TS_STAGE = TS_MAT + TS_VEC;
+
+int64_t triples_cube_count(int nv) {
+  const int64_t nt = (nv + TCUBE - 1) / TCUBE;
+  return nt * (nt + 1) * (nt + 2) / 6;
+}
+
+void triples_cube_table(int nv, int* tri) {
+  const int nt = (nv + TCUBE - 1) / TCUBE;
+  int64_t t = 0;
+  for (int C = 0; C < nt; ++C)
+    for (int B = 0; B <= C; ++B)
+      for (int A = 0; A <= B; ++A) {
+        tri[3 * t] = A;
+        tri[3 * t + 1] = B;
+        tri[3 * t + 2] = C;
+        ++t;
+      }
+}
+
+__device__ __forceinline__ int pick3(int i, int s0, int s1, int s2) {
+  return i == 0 ? s0 : (i == 1 ? s1 : s2);
+}
+
+// One block per orbit of cube triples A <= B <= C.  The six cubes K[S_s0 +
+// x, S_s1 + y, S_s2 + z] (s a permutation, S = 8*(A,B,C)) are staged in
+// shared memory with the M/N blocks and the vectors they need.  Thread
+// (x,y,z) then owns the element e0 = S + (x,y,z) and its six orderings: it
+// reads K at each ordering (one value per cube), forms their six X values
+// with one reciprocal of the common denominator, and adds
+// sum_e K_e X_e and sum_e X_e Y_e over the orderings.  Every ordered element
+// of the orbit is reached |stabiliser| times (1, 2 or 6 when two or three of
+// A, B, C coincide), which the weight undoes.
+template <typename T, bool HAS_U>
+__global__ void __launch_bounds__(512, 2) triples_energy_kernel(int nv, const T* __restrict__ K,
+                                                                const T* __restrict__ KU,
+                                                                double eijk,
+                                                                const double* __restrict__ ev,
+                                                                TriplesTerms tt,
+                                                                const int* __restrict__ tri,
+                                                                int ntri, double* part) {
+  extern __shared__ double tsm[];
+  double* cubeK = tsm;                                   // [6][648]
+  double* cubeU = cubeK + 6 * TCUBE_ELEMS;               // [6][648] (HAS_U)
+  double* pmat = cubeU + (HAS_U ? 6 * TCUBE_ELEMS : 0);  // [w][pair][64]
+  double* pvec = pmat + TS_MAT;                          // [w][pos][8]
   __shared__ double sh[32];
-  const int64_t v = nv, n = v * v * v;
-  double acc = 0.0;
-  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < n;
-       idx += (int64_t)gridDim.x * blockDim.x) {
-    int64_t a = idx % v, b = (idx / v) % v, c = idx / (v * v);
-    double kabc = K[idx];
-    double x = 4.0 * kabc - 2.0 * K[a + v * c + v * v * b] - 2.0 * K[c + v * b + v * v * a] -
-               2.0 * K[b + v * a + v * v * c] + K[c + v * a + v * v * b] + K[b + v * c + v * v * a];
-    x /= (eijk - ev[a] - ev[b] - ev[c]);
-    X[idx] = x;
-    acc += kabc * x;
-  }
-  if (want_e) {
-    double r = block_sum(acc, sh);
-    if (threadIdx.x == 0) part[blockIdx.x] = r;
-  }
-}
-
-int triples_x(stream_t s, int nv, const double* K, double eijk, const double* ev, double* X,
-              double* scratch, double* eout) {
-  cudaStream_t st = (cudaStream_t)s;
-  triples_x_kernel<<<RED_BLOCKS, 256, 0, st>>>(nv, K, eijk, ev, X, scratch, eout ? 1 : 0);
-  int e = launched();
-  if (e || !eout) return e;
-  final_sum_kernel<<<1, 256, 0, st>>>(RED_BLOCKS, 1, scratch, eout);
-  return launched();
-}
-
-// One 8x8x8 cube of K per block (512 threads, thread = (a,b,c) in the cube).
-// Each W_t cube is loaded in W_t's own memory order (coalesced along its first
-// index) into shared memory and read back at the permuted position.
-struct SumWArgs {
-  const double* W[6];
-};
-
-__global__ void __launch_bounds__(512) triples_sumw_kernel(int nv, SumWArgs w, double* K) {
-  __shared__ double cube[8 * 9 * 9];
-  const int64_t v = nv, nt = (v + 7) / 8;
-  const int tx = threadIdx.x & 7, ty = (threadIdx.x >> 3) & 7, tz = threadIdx.x >> 6;
-  for (int64_t t = blockIdx.x; t < nt * nt * nt; t += gridDim.x) {
-    const int64_t o[3] = {(t % nt) * 8, ((t / nt) % nt) * 8, (t / (nt * nt)) * 8};  // a0,b0,c0
-    // permutation p: W_t is indexed W_t[x,y,z] with (x,y,z) = (o[p0], o[p1], o[p2]) origins
-    const int P[6][3] = {{0, 1, 2}, {1, 0, 2}, {0, 2, 1}, {2, 1, 0}, {1, 2, 0}, {2, 0, 1}};
-    double acc = 0.0;
-    const int loc[3] = {tx, ty, tz};  // this thread's (a,b,c) offsets
-    for (int q = 0; q < 6; ++q) {
-      const int64_t x = o[P[q][0]] + tx, y = o[P[q][1]] + ty, z = o[P[q][2]] + tz;
-      cube[tx + 9 * (ty + 9 * tz)] = (x < v && y < v && z < v) ? w.W[q][x + v * y + v * v * z] : 0.0;
-      __syncthreads();
-      // this thread's element of K needs W_q at (loc[P0], loc[P1], loc[P2])
-      acc += cube[loc[P[q][0]] + 9 * (loc[P[q][1]] + 9 * loc[P[q][2]])];
-      __syncthreads();
-    }
-    const int64_t a = o[0] + tx, b = o[1] + ty, c = o[2] + tz;
-    if (a < v && b < v && c < v) K[a + v * b + v * v * c] = acc;
-  }
-}
-
-int triples_sumw(stream_t s, int nv, const double* const* W, double* K) {
-  SumWArgs w;
-  for (int q = 0; q < 6; ++q) w.W[q] = W[q];
-  int64_t nt = (nv + 7) / 8, cubes = nt * nt * nt;
-  unsigned g = (unsigned)(cubes < 148 * 8 ? cubes : 148 * 8);
-  triples_sumw_kernel<<<g, 512, 0, (cudaStream_t)s>>>(nv, w, K);
-  return launched();
-}
-
-// X = (4K_abc - 2K_acb - 2K_cba - 2K_bac + K_cab + K_bca) / D for one 8^3 cube per
-// block; the six permuted K cubes are staged through shared memory.
-__global__ void __launch_bounds__(512) triples_x_cube_kernel(int nv, const double* __restrict__ K,
-                                                            double eijk,
-                                                            const double* __restrict__ ev,
-                                                            double* __restrict__ X,
-                                                            double* part, int want_e) {
-  __shared__ double cube[6][8 * 9 * 9];
-  __shared__ double sh[32];
-  const int64_t v = nv, nt = (v + 7) / 8;
-  const int tx = threadIdx.x & 7, ty = (threadIdx.x >> 3) & 7, tz = threadIdx.x >> 6;
-  const int loc[3] = {tx, ty, tz};
-  // K permutations in X: (a,b,c) (a,c,b) (c,b,a) (b,a,c) (c,a,b) (b,c,a)
-  const int P[6][3] = {{0, 1, 2}, {0, 2, 1}, {2, 1, 0}, {1, 0, 2}, {2, 0, 1}, {1, 2, 0}};
-  const double cf[6] = {4.0, -2.0, -2.0, -2.0, 1.0, 1.0};
-  double eacc = 0.0;
-  for (int64_t t = blockIdx.x; t < nt * nt * nt; t += gridDim.x) {
-    const int64_t o[3] = {(t % nt) * 8, ((t / nt) % nt) * 8, (t / (nt * nt)) * 8};
-    for (int q = 0; q < 6; ++q) {
-      const int64_t x = o[P[q][0]] + tx, y = o[P[q][1]] + ty, z = o[P[q][2]] + tz;
-      cube[q][tx + 9 * (ty + 9 * tz)] = (x < v && y < v && z < v) ? K[x + v * y + v * v * z] : 0.0;
-    }
-    __syncthreads();
-    const int64_t a = o[0] + tx, b = o[1] + ty, c = o[2] + tz;
-    if (a < v && b < v && c < v) {
-      double x = 0.0;
+  const int v = nv, tid = threadIdx.x;
+  const int l[3] = {tid & 7, (tid >> 3) & 7, tid >> 6};
+  const int lme = l[0] + TPITCH * (l[1] + TPITCH * l[2]);
+  // this thread's element in each cube of the orbit: ordering q of e0
+  int koff[6];
 #pragma unroll
-      for (int q = 0; q < 6; ++q)
-        x += cf[q] * cube[q][loc[P[q][0]] + 9 * (loc[P[q][1]] + 9 * loc[P[q][2]])];
-      x /= (eijk - ev[a] - ev[b] - ev[c]);
-      X[a + v * b + v * v * c] = x;
-      eacc += cube[0][tx + 9 * (ty + 9 * tz)] * x;
+  for (int q = 0; q < 6; ++q)
+    koff[q] = q * TCUBE_ELEMS + l[perm3(q, 0)] + TPITCH * (l[perm3(q, 1)] + TPITCH * l[perm3(q, 2)]);
+  constexpr int NSTAGE = (TS_STAGE + 511) / 512;
+  const double XW[6] = {4.0, -2.0, -2.0, -2.0, 1.0, 1.0};
+  double eK = 0.0, eY = 0.0;
+  for (int t = blockIdx.x; t < ntri; t += gridDim.x) {
+    const int S0 = tri[3 * t] * TCUBE, S1 = tri[3 * t + 1] * TCUBE, S2 = tri[3 * t + 2] * TCUBE;
+    // global loads of the orbit, then the shared-memory stores
+    double kv[6], uv[HAS_U ? 6 : 1], sv[NSTAGE];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      const int x = pick3(perm3(q, 0), S0, S1, S2) + l[0];
+      const int y = pick3(perm3(q, 1), S0, S1, S2) + l[1];
+      const int z = pick3(perm3(q, 2), S0, S1, S2) + l[2];
+      const bool ok = x < v && y < v && z < v;
+      const int idx = x + v * (y + v * z);
+      kv[q] = ok ? (double)K[idx] : 0.0;
+      if (HAS_U) uv[HAS_U ? q : 0] = ok ? (double)KU[idx] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < NSTAGE; ++u) {
+      const int e = tid + 512 * u;
+      double val = 0.0;
+      if (e < TS_MAT) {
+        const int w = e / 384, pr = (e >> 6) % 6, i = e & 7, j = (e >> 3) & 7;
+        const int px = pr >> 1, py0 = pr & 1, py = py0 < px ? py0 : py0 + 1;
+        const int r0 = pick3(px, S0, S1, S2) + i, c0 = pick3(py, S0, S1, S2) + j;
+        const double* src = w == 0 ? tt.M[0] : w == 1 ? tt.M[1] : w == 2 ? tt.M[2]
+                          : w == 3 ? tt.N[0] : w == 4 ? tt.N[1] : tt.N[2];
+        if (r0 < v && c0 < v) val = src[r0 + v * c0];
+      } else if (e < TS_STAGE) {
+        const int f = e - TS_MAT, w = f / 24, pos = (f >> 3) % 3, i = f & 7;
+        const int x = pick3(pos, S0, S1, S2) + i;
+        const double* src = w == 0 ? tt.g[0] : w == 1 ? tt.g[1] : w == 2 ? tt.g[2]
+                          : w == 3 ? tt.f[0] : w == 4 ? tt.f[1] : w == 5 ? tt.f[2] : ev;
+        if (x < v) val = src[x];
+      }
+      sv[u] = val;
+    }
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      cubeK[q * TCUBE_ELEMS + lme] = kv[q];
+      if (HAS_U) cubeU[q * TCUBE_ELEMS + lme] = uv[HAS_U ? q : 0];
+    }
+#pragma unroll
+    for (int u = 0; u < NSTAGE; ++u) {
+      const int e = tid + 512 * u;
+      if (e < TS_STAGE) pmat[e] = sv[u];
+    }
+    __syncthreads();
+    const int a0 = S0 + l[0], b0 = S1 + l[1], c0 = S2 + l[2];
+    if (a0 < v && b0 < v && c0 < v) {
+      double k[6];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) k[q] = cubeK[koff[q]];
+      const double dinv =
+          __drcp_rn(eijk - pvec[144 + l[0]] - pvec[152 + l[1]] - pvec[160 + l[2]]);
+      double X[6];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        double x = 0.0;
+#pragma unroll
+        for (int r = 0; r < 6; ++r) x += XW[r] * k[xcomp(q, r)];
+        X[q] = x * dinv;
+      }
+      // vectors at the three positions: vg[w][pos]
+      double vg[6][3];
+#pragma unroll
+      for (int w = 0; w < 6; ++w)
+#pragma unroll
+        for (int pos = 0; pos < 3; ++pos) vg[w][pos] = pvec[w * 24 + pos * 8 + l[pos]];
+      double ek = 0.0, ey = 0.0;
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        const int p0 = perm3(q, 0), p1 = perm3(q, 1), p2 = perm3(q, 2);
+        auto mat = [&](int w, int x, int y) {
+          return pmat[(w * 6 + pair_index(x, y)) * 64 + l[x] + 8 * l[y]];
+        };
+        const double y = vg[0][p0] * mat(0, p1, p2) + vg[1][p1] * mat(1, p0, p2) +
+                         vg[2][p2] * mat(2, p0, p1) + vg[3][p0] * mat(3, p1, p2) +
+                         vg[4][p1] * mat(4, p0, p2) + vg[5][p2] * mat(5, p0, p1);
+        ek += (HAS_U ? cubeU[koff[q]] : k[q]) * X[q];
+        ey += X[q] * y;
+      }
+      const bool ab = (S0 == S1), bc = (S1 == S2);
+      const double wgt = (ab && bc) ? (1.0 / 6.0) : (ab || bc) ? 0.5 : 1.0;
+      eK += wgt * ek;
+      eY += wgt * ey;
     }
     __syncthreads();
   }
-  if (want_e) {
-    double r = block_sum(eacc, sh);
-    if (threadIdx.x == 0) part[blockIdx.x] = r;
-  }
-}
-
-int triples_x_cube(stream_t s, int nv, const double* K, double eijk, const double* ev, double* X,
-                   double* scratch, double* eout) {
-  cudaStream_t st = (cudaStream_t)s;
-  int64_t nt = (nv + 7) / 8, cubes = nt * nt * nt;
-  int g = (int)(cubes < RED_BLOCKS ? cubes : RED_BLOCKS);
-  triples_x_cube_kernel<<<g, 512, 0, st>>>(nv, K, eijk, ev, X, scratch, eout ? 1 : 0);
-  int e = launched();
-  if (e || !eout) return e;
-  final_sum_kernel<<<1, 256, 0, st>>>(g, 1, scratch, eout);
-  return launched();
-}
-
-__global__ void triples_int_kernel(int nv, const double* __restrict__ X, const double* Mjk,
-                                   const double* Mik, const double* Mij, const double* Njk,
-                                   const double* Nik, const double* Nij, double fac, double* IntX,
-                                   double* IntY, int i, int j, int k) {
-  __shared__ double sh[32];
-  const int64_t v = nv, x = blockIdx.x;
-  double s[6] = {0, 0, 0, 0, 0, 0};
-  for (int64_t e = threadIdx.x; e < v * v; e += blockDim.x) {
-    int64_t p = e % v, q = e / v;
-    double x0 = X[x + v * p + v * v * q];  // X[x,b,c], (b,c) = (p,q)
-    double x1 = X[p + v * x + v * v * q];  // X[a,x,c], (a,c) = (p,q)
-    double x2 = X[p + v * q + v * v * x];  // X[a,b,x], (a,b) = (p,q)
-    s[0] += x0 * Mjk[e];
-    s[1] += x1 * Mik[e];
-    s[2] += x2 * Mij[e];
-    s[3] += x0 * Njk[e];
-    s[4] += x1 * Nik[e];
-    s[5] += x2 * Nij[e];
-  }
-  double r[6];
-  for (int t = 0; t < 6; ++t) r[t] = block_sum(s[t], sh);
+  const double r0 = block_sum(eK, sh);
+  const double r1 = block_sum(eY, sh);
   if (threadIdx.x == 0) {
-    IntX[x + v * i] += fac * r[0];
-    IntX[x + v * j] += fac * r[1];
-    IntX[x + v * k] += fac * r[2];
-    IntY[x + v * i] += fac * r[3];
-    IntY[x + v * j] += fac * r[4];
-    IntY[x + v * k] += fac * r[5];
+    part[blockIdx.x] = r0;
+    part[RED_BLOCKS + blockIdx.x] = r1;
   }
 }
 
-int triples_int(stream_t s, int nv, const double* X, const double* Mjk, const double* Mik,
-                const double* Mij, const double* Njk, const double* Nik, const double* Nij,
-                double fac, double* IntX, double* IntY, int i, int j, int k) {
-  triples_int_kernel<<<nv, 256, 0, (cudaStream_t)s>>>(nv, X, Mjk, Mik, Mij, Njk, Nik, Nij, fac,
-                                                      IntX, IntY, i, j, k);
+int triples_energy(stream_t s, int nv, const void* K, const void* KU, bool k_f32, double eijk,
+                   const double* ev, const TriplesTerms& t, const int* tri, double* scratch,
+                   double* out) {
+  cudaStream_t st = (cudaStream_t)s;
+  const int64_t ntri = triples_cube_count(nv);
+  const int g = (int)(ntri < RED_BLOCKS ? ntri : RED_BLOCKS);
+  if (nv > 1290) return (int)cudaErrorInvalidValue;  // 32-bit element offsets
+  const size_t smem = ((KU ? 12 : 6) * TCUBE_ELEMS + TS_STAGE) * sizeof(double);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(triples_energy_kernel<double, false>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 1024);
+    cudaFuncSetAttribute(triples_energy_kernel<float, false>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 1024);
+    cudaFuncSetAttribute(triples_energy_kernel<double, true>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 1024);
+    cudaFuncSetAttribute(triples_energy_kernel<float, true>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 1024);
+    attr = true;
+  }
+  if (k_f32) {
+    auto k = KU ? triples_energy_kernel<float, true> : triples_energy_kernel<float, false>;
+    k<<<g, 512, smem, st>>>(nv, (const float*)K, (const float*)KU, eijk, ev, t, tri, (int)ntri,
+                            scratch);
+  } else {
+    auto k = KU ? triples_energy_kernel<double, true> : triples_energy_kernel<double, false>;
+    k<<<g, 512, smem, st>>>(nv, (const double*)K, (const double*)KU, eijk, ev, t, tri,
+                            (int)ntri, scratch);
+  }
+  int e = launched();
+  if (e) return e;
+  final_sum_kernel<<<1, 256, 0, st>>>(g, 2, scratch, out);
   return launched();
 }
 

@@ -1,26 +1,29 @@
 // dev_tc.cu — split-BF16 GEMM on the sm_100a tensor cores (tcgen05 + TMA).
 //
-// C = alpha * op(A) op(B) + beta * C with FP64 operands and result.  Each
-// operand is split into three BF16 slices x = x0 + x1 + x2 (x0 = bf16(x),
-// x1 = bf16(x - x0), x2 = bf16(x - x0 - x1)) stored K-major and zero padded
-// (M, N to 128, K to 64).  The six products x0y0, x0y1, x1y0, x1y1, x0y2, x2y0
-// are accumulated in FP32 in tensor memory, which reproduces an FP32-accurate
-// product (relative error ~2^-24 of sum |a||b|).
+// C = alpha * op(A) op(B) + beta * C with FP64 operands.  Each operand is split
+// into NSL BF16 slices x = x0 + x1 (+ x2) (x0 = bf16(x), x1 = bf16(x - x0),
+// x2 = bf16(x - x0 - x1)) stored K-major and zero padded (rows to 128, K to 64).
+// NSL = 3 accumulates the six products x0y0 x0y1 x1y0 x1y1 x0y2 x2y0 in FP32
+// (relative error ~2^-24 of sum |a||b|, FP32-like); NSL = 2 accumulates
+// x0y0 x0y1 x1y0 (~2^-16, for sums whose element errors average out, such as
+// the (T) energy).
 //
 // Kernel: persistent, one CTA per SM over 128x128 output tiles.  TMA loads
 // (3-D tensor maps: k, row, slice; 64x128 boxes, 128-byte swizzle) feed a
-// two-stage shared-memory ring; tcgen05.mma kind::f16 (BF16 x BF16 -> F32,
-// M=128 N=128 K=16) accumulates in one of two tensor-memory accumulators
-// while four epilogue warps drain the other with tcgen05.ld and write FP64 C.
-// Every mbarrier wait is bounded (1 s); on time-out the kernel records an
-// error code, lets its own loads land (bounded), frees its tensor memory and
-// returns.
+// ring of 192 KiB (2 stages of 3 slices or 3 stages of 2 slices);
+// tcgen05.mma kind::f16 (BF16 x BF16 -> F32, M=128 N=128 K=16) accumulates in
+// one of two tensor-memory accumulators while eight epilogue warps drain the
+// other with tcgen05.ld and write C (FP64 or FP32, through an index map whose
+// rows run along the lanes).  Every mbarrier wait is bounded (1 s); on
+// time-out the kernel records an error code, lets its own loads and MMAs in
+// flight finish (bounded), frees its tensor memory and returns.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cstdint>
+#include <cstring>
 #include <mutex>
 
 #include "ecg_dev.h"
@@ -30,12 +33,23 @@ namespace dev {
 
 namespace {
 
-constexpr int TM = 128, TN = 128, TK = 64, STAGES = 2, SLICES = 3;
+constexpr int TM = 128, TN = 128, TK = 64;
 constexpr int TILE_BYTES_A = TM * TK * 2;  // 16 KiB per slice
 constexpr int TILE_BYTES_B = TN * TK * 2;
-constexpr int STAGE_BYTES = SLICES * (TILE_BYTES_A + TILE_BYTES_B);  // 96 KiB
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*barriers*/ + 1024 /*align*/;
+constexpr int RING_BYTES = 192 * 1024;
 constexpr unsigned long long WAIT_NS = 1000000000ull;  // 1 s bound on every mbarrier wait
+
+template <int NSL>
+struct TcCfg {
+  static constexpr int STAGE_BYTES = NSL * (TILE_BYTES_A + TILE_BYTES_B);
+  static constexpr int STAGES = RING_BYTES / STAGE_BYTES;
+  static constexpr int NPAIR = NSL == 3 ? 6 : 3;
+  static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*barriers*/ + 1024 /*align*/;
+};
+// slice pairs (a, b): hi*hi, hi*mid, mid*hi, mid*mid, hi*lo, lo*hi (the first
+// three for NSL = 2)
+__host__ __device__ constexpr int pair_a(int p) { return p == 2 || p == 3 ? 1 : p == 5 ? 2 : 0; }
+__host__ __device__ constexpr int pair_b(int p) { return p == 1 || p == 3 ? 1 : p == 4 ? 2 : 0; }
 
 __device__ int g_tc_error = 0;
 
@@ -116,20 +130,101 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
 // work items (m-tile, n-tile, k-slice).  Warp 0 lane 0: TMA producer over a
 // STAGES-deep shared-memory ring (full/empty mbarriers).  Warp 1: owns the
 // 256-column tensor-memory allocation, lane 0 issues the MMAs into one of two
-// 128-column accumulators and commits.  Warps 2..5: epilogue, each reading
-// the 32 accumulator lanes its warp index (mod 4) may access, writing FP64 C
-// and releasing the accumulator, so the epilogue of one tile overlaps the
-// MMAs of the next.
-constexpr int EPI_WARPS = 4;
+// 128-column accumulators and commits.  Warps 2..9: epilogue, each reading
+// the 32 accumulator lanes its warp index (mod 4) may access and one half of
+// the columns, writing C and releasing the accumulator, so the epilogue of
+// one tile overlaps the MMAs of the next.
+constexpr int EPI_WARPS = 8;  // two per TMEM lane quarter, 64 columns each
 constexpr int THREADS_TC = 32 * (2 + EPI_WARPS);
 constexpr uint32_t TMEM_COLS_P = 2 * TN;
 
+// TMA descriptors of the two K segments: k-blocks [0, kb_seg0) read (a0, b0),
+// the rest read (a1, b1) from their own k = 0.
+struct TcMaps {
+  CUtensorMap a0, b0, a1, b1;
+};
+
+// Output element (m, n) lives at C[rowoff(m) + coloff(n)] (FP64, or FP32 when
+// f32) with rowoff(m) = (m % dm)*scm + (m / dm)*scm2 (dm = 0: m*scm) and
+// coloff(n) = (n % dn)*scn + (n / dn)*scn2 (dn = 0: n*scn).  Lanes of an
+// epilogue warp hold consecutive rows, so scm == 1 gives coalesced stores.
+struct TcOut {
+  void* C;
+  int64_t scm, scn, dn, scn2, dm, scm2;
+  int f32;
+};
+
+// Epilogue of one 16-column chunk: this lane's row (offset rowoff), columns
+// col0 .. col0+15.  Read-modify-write loads are all issued before the stores.
+template <typename CT>
+__device__ __forceinline__ void epi_chunk(CT* __restrict__ C, int64_t rowoff, const uint32_t* r,
+                                          int64_t col0, int64_t N, const TcOut& out,
+                                          double alpha, double beta) {
+  int64_t off[16];
+  if (out.dn == 0) {
+    const int64_t b = rowoff + col0 * out.scn;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) off[j] = b + j * out.scn;
+  } else {
+    const int64_t nq = col0 / out.dn;
+    int64_t nr = col0 - nq * out.dn;
+    int64_t coff = nr * out.scn + nq * out.scn2;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      off[j] = rowoff + coff;
+      ++nr;
+      coff += out.scn;
+      if (nr == out.dn) {
+        nr = 0;
+        coff += out.scn2 - out.dn * out.scn;
+      }
+    }
+  }
+  if (beta != 0.0) {
+    CT old[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) old[j] = (col0 + j < N) ? C[off[j]] : (CT)0;
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+      if (col0 + j < N)
+        C[off[j]] = (CT)(alpha * (double)__uint_as_float(r[j]) + beta * (double)old[j]);
+  } else {
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+      if (col0 + j < N) C[off[j]] = (CT)(alpha * (double)__uint_as_float(r[j]));
+  }
+}
+
+// L2 prefetch of the C elements (row offset rowoff, columns col0 .. col0+n-1)
+// that a read-modify-write epilogue will load, issued while the MMAs of the
+// tile still run.
+template <typename CT>
+__device__ __forceinline__ void prefetch_cols(const CT* C, int64_t rowoff, int64_t col0, int n,
+                                              int64_t N, const TcOut& out) {
+  int64_t nq = 0, nr = col0;
+  if (out.dn > 0) {
+    nq = col0 / out.dn;
+    nr = col0 - nq * out.dn;
+  }
+  int64_t coff = nr * out.scn + nq * out.scn2;
+  for (int j = 0; j < n && col0 + j < N; ++j) {
+    asm volatile("prefetch.global.L2 [%0];\n" ::"l"(C + rowoff + coff));
+    ++nr;
+    coff += out.scn;
+    if (out.dn > 0 && nr == out.dn) {
+      nr = 0;
+      coff += out.scn2 - out.dn * out.scn;
+    }
+  }
+}
+
+template <int NSL>
 __global__ void __launch_bounds__(THREADS_TC, 1)
-    mgemm_bf16x3_kernel(const __grid_constant__ CUtensorMap tmA,
-                        const __grid_constant__ CUtensorMap tmB, double* __restrict__ C,
-                        int64_t M, int64_t N, int64_t scm, int64_t scn, double alpha, double beta,
-                        int kb_per_split, int kblocks_total, int64_t split_stride, int mtiles,
-                        int ntiles, int nsplit) {
+    mgemm_bf16_kernel(const __grid_constant__ TcMaps maps, TcOut out, int64_t M, int64_t N,
+                      double alpha, double beta, int kb_seg0, int kb_per_split, int kblocks_total,
+                      int64_t split_stride, int mtiles, int ntiles, int nsplit) {
+  using Cfg = TcCfg<NSL>;
+  constexpr int STAGES = Cfg::STAGES, STAGE_BYTES = Cfg::STAGE_BYTES;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint8_t* tiles = smem;
@@ -167,9 +262,17 @@ __global__ void __launch_bounds__(THREADS_TC, 1)
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
   const uint32_t tmem = *tmem_slot;
 
+  // the dimension with fewer tiles runs fastest, so that CTAs working at the
+  // same time share the tiles of the larger operand through L2
+  const bool mfast = mtiles <= ntiles;
   auto item_coords = [&](int64_t it, int& mt, int& nt, int& z) {
-    mt = (int)(it % mtiles);
-    nt = (int)((it / mtiles) % ntiles);
+    if (mfast) {
+      mt = (int)(it % mtiles);
+      nt = (int)((it / mtiles) % ntiles);
+    } else {
+      nt = (int)(it % ntiles);
+      mt = (int)((it / ntiles) % mtiles);
+    }
     z = (int)(it / ((int64_t)mtiles * ntiles));
   };
   auto item_kblocks = [&](int z) { return min(kb_per_split, kblocks_total - z * kb_per_split); };
@@ -190,11 +293,15 @@ __global__ void __launch_bounds__(THREADS_TC, 1)
             break;
           }
           uint8_t* st = tiles + s * STAGE_BYTES;
+          const int kg = kb0 + kb;
+          const bool s1 = kg >= kb_seg0;
+          const CUtensorMap* ma = s1 ? &maps.a1 : &maps.a0;
+          const CUtensorMap* mb = s1 ? &maps.b1 : &maps.b0;
+          const int kx = (s1 ? kg - kb_seg0 : kg) * TK;
           mbar_expect_tx(&full[s], STAGE_BYTES);
-          for (int t = 0; t < SLICES; ++t) {
-            tma_load_3d(st + t * TILE_BYTES_A, &tmA, &full[s], (kb0 + kb) * TK, mt * TM, t);
-            tma_load_3d(st + SLICES * TILE_BYTES_A + t * TILE_BYTES_B, &tmB, &full[s],
-                        (kb0 + kb) * TK, nt * TN, t);
+          for (int t = 0; t < NSL; ++t) {
+            tma_load_3d(st + t * TILE_BYTES_A, ma, &full[s], kx, mt * TM, t);
+            tma_load_3d(st + NSL * TILE_BYTES_A + t * TILE_BYTES_B, mb, &full[s], kx, nt * TN, t);
           }
         }
       }
@@ -233,13 +340,11 @@ __global__ void __launch_bounds__(THREADS_TC, 1)
           asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
           const uint8_t* st = tiles + s * STAGE_BYTES;
           const uint8_t* As = st;
-          const uint8_t* Bs = st + SLICES * TILE_BYTES_A;
-          // slice pairs (a, b): hi*hi, hi*mid, mid*hi, mid*mid, hi*lo, lo*hi
-          const int pa[6] = {0, 0, 1, 1, 0, 2}, pb[6] = {0, 1, 0, 1, 2, 0};
+          const uint8_t* Bs = st + NSL * TILE_BYTES_A;
 #pragma unroll
-          for (int p = 0; p < 6; ++p) {
-            const uint64_t da = umma_desc(As + pa[p] * TILE_BYTES_A);
-            const uint64_t db = umma_desc(Bs + pb[p] * TILE_BYTES_B);
+          for (int p = 0; p < Cfg::NPAIR; ++p) {
+            const uint64_t da = umma_desc(As + pair_a(p) * TILE_BYTES_A);
+            const uint64_t db = umma_desc(Bs + pair_b(p) * TILE_BYTES_B);
 #pragma unroll
             for (int kk = 0; kk < TK / 16; ++kk)
               umma(dcol, da + (uint64_t)(kk * 2), db + (uint64_t)(kk * 2),
@@ -255,14 +360,29 @@ __global__ void __launch_bounds__(THREADS_TC, 1)
       if (last >= 0) mbar_wait(&tfull[last & 1], (uint32_t)((last >> 1) & 1));
     }
   } else {
-    // epilogue warps 2..5: TMEM lane quarter q = warp % 4
-    const int q = warp & 3;
+    // epilogue warps 2..9: TMEM lane quarter q = warp % 4, column half hw
+    const int q = warp & 3, hw = (warp - 2) >> 2;
     const uint32_t lane_base = (uint32_t)(q * 32) << 16;
     int64_t lt = 0;
     for (int64_t it = blockIdx.x; it < items; it += gridDim.x, ++lt) {
       int mt, nt, z;
       item_coords(it, mt, nt, z);
       const int acc = (int)(lt & 1);
+      const int64_t row = (int64_t)mt * TM + q * 32 + lane;
+      int64_t rowoff = (int64_t)z * split_stride;
+      if (out.dm > 0) {
+        const int64_t mq = row / out.dm;
+        rowoff += (row - mq * out.dm) * out.scm + mq * out.scm2;
+      } else {
+        rowoff += row * out.scm;
+      }
+      if (beta != 0.0 && row < M) {
+        const int64_t col0 = (int64_t)nt * TN + hw * (TN / 2);
+        if (out.f32)
+          prefetch_cols((const float*)out.C, rowoff, col0, TN / 2, N, out);
+        else
+          prefetch_cols((const double*)out.C, rowoff, col0, TN / 2, N, out);
+      }
       if (!mbar_wait(&tfull[acc], (uint32_t)((lt >> 1) & 1))) {
         atomicExch(&g_tc_error, 3);
         atomicExch(abort_flag, 1);
@@ -270,33 +390,23 @@ __global__ void __launch_bounds__(THREADS_TC, 1)
       }
       if (*(volatile int*)abort_flag) break;
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
-      double* Cz = C + (int64_t)z * split_stride;
-      const int64_t row = (int64_t)mt * TM + q * 32 + lane;
 #pragma unroll 1
-      for (int c = 0; c < TN; c += 32) {
-        uint32_t r[32];
+      for (int c = hw * (TN / 2); c < (hw + 1) * (TN / 2); c += 16) {
+        uint32_t r[16];
         asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
-            "%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
+            "%13,%14,%15}, [%16];\n"
             : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
               "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
-              "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
-              "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
-              "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
-              "=r"(r[31])
+              "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
             : "r"(tmem + lane_base + (uint32_t)(acc * TN + c)));
         asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::);
         if (row < M) {
-#pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            const int64_t col = (int64_t)nt * TN + c + j;
-            if (col < N) {
-              double* cp = Cz + row * scm + col * scn;
-              double v = alpha * (double)__uint_as_float(r[j]);
-              if (beta != 0.0) v += beta * *cp;
-              *cp = v;
-            }
-          }
+          const int64_t col0 = (int64_t)nt * TN + c;
+          if (out.f32)
+            epi_chunk((float*)out.C, rowoff, r, col0, N, out, alpha, beta);
+          else
+            epi_chunk((double*)out.C, rowoff, r, col0, N, out, alpha, beta);
         }
       }
       asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
@@ -314,11 +424,12 @@ __global__ void __launch_bounds__(THREADS_TC, 1)
   }
 }
 
-// X(r,k) = src[r*sr + k*sk] (FP64, R x K) -> dst[s][r][k] BF16, zero padded to
-// Rp x Kp.  32x32 tiles through shared memory so that reads are coalesced
-// whichever of sr / sk is the unit stride.
-__global__ void split3_kernel(const double* __restrict__ src, int64_t R, int64_t K, int64_t sr,
-                              int64_t sk, int64_t Rp, int64_t Kp, __nv_bfloat16* __restrict__ dst) {
+// X(r,k) = src[r*sr + k*sk] (FP64, R x K) -> dst[s][r][k] BF16 (s < nsl), zero
+// padded to Rp x Kp.  32x32 tiles through shared memory so that reads are
+// coalesced whichever of sr / sk is the unit stride.
+__global__ void split_kernel(const double* __restrict__ src, int64_t R, int64_t K, int64_t sr,
+                             int64_t sk, int64_t Rp, int64_t Kp, int nsl,
+                             __nv_bfloat16* __restrict__ dst) {
   __shared__ double tile[32][33];
   const int64_t tk = (Kp + 31) / 32, tr = (Rp + 31) / 32, ntile = tk * tr;
   const bool rfast = (sr == 1);
@@ -340,11 +451,10 @@ __global__ void split3_kernel(const double* __restrict__ src, int64_t R, int64_t
         const double e1 = x - (double)__bfloat162float(h0);
         const __nv_bfloat16 h1 = __double2bfloat16(e1);
         const double e2 = e1 - (double)__bfloat162float(h1);
-        const __nv_bfloat16 h2 = __double2bfloat16(e2);
         const int64_t o = r * Kp + k, sl = Rp * Kp;
         dst[o] = h0;
         dst[o + sl] = h1;
-        dst[o + 2 * sl] = h2;
+        if (nsl == 3) dst[o + 2 * sl] = __double2bfloat16(e2);
       }
     }
     __syncthreads();
@@ -391,77 +501,153 @@ __nv_bfloat16* split_buffer(size_t n) {
   return g_split;
 }
 
-int make_map(EncodeFn enc, CUtensorMap* m, __nv_bfloat16* base, int64_t rows_p, int64_t k_p) {
-  cuuint64_t dims[3] = {(cuuint64_t)k_p, (cuuint64_t)rows_p, (cuuint64_t)SLICES};
+int make_map(EncodeFn enc, CUtensorMap* m, const void* base, int64_t rows_p, int64_t k_p,
+             int nsl) {
+  cuuint64_t dims[3] = {(cuuint64_t)k_p, (cuuint64_t)rows_p, (cuuint64_t)nsl};
   cuuint64_t strides[2] = {(cuuint64_t)(k_p * 2), (cuuint64_t)(rows_p * k_p * 2)};
   cuuint32_t box[3] = {(cuuint32_t)TK, (cuuint32_t)TM, 1};
   cuuint32_t es[3] = {1, 1, 1};
-  CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, (void*)base, dims, strides, box, es,
-                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+  CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(base), dims, strides,
+                   box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? 0 : (int)cudaErrorInvalidValue;
 }
 
+int64_t pad_rows(int64_t r) { return (r + TM - 1) / TM * TM; }
+int64_t pad_k(int64_t k) { return (k + TK - 1) / TK * TK; }
+
+void launch_split(cudaStream_t st, const double* src, int64_t R, int64_t K, int64_t sr,
+                  int64_t sk, int64_t Rp, int64_t Kp, int nsl, __nv_bfloat16* dst) {
+  const int64_t tiles = ((Rp + 31) / 32) * ((Kp + 31) / 32);
+  const unsigned g = (unsigned)(tiles < 148 * 16 ? tiles : 148 * 16);
+  split_kernel<<<g, dim3(32, 8), 0, st>>>(src, R, K, sr, sk, Rp, Kp, nsl, dst);
+  note_launches(1);
+}
+
+// Launch over pre-split operands; S > 1 splits the combined k-blocks into S
+// slices that write FP64 partial products P[z][n][m] (column-major m x n).
+template <int NSL>
+int launch_tc(cudaStream_t st, const TcMaps& maps, int kb0, int kbt, int64_t m, int64_t n,
+              int64_t mp, int64_t np, double alpha, double beta, const TcOut& out, int S) {
+  using Cfg = TcCfg<NSL>;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(mgemm_bf16_kernel<NSL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         Cfg::SMEM_BYTES);
+    attr = true;
+  }
+  const int mt = (int)(mp / TM), nt = (int)(np / TN);
+  const int kps = (kbt + S - 1) / S;
+  S = (kbt + kps - 1) / kps;
+  const int64_t items = (int64_t)mt * nt * S;
+  const unsigned grid = (unsigned)(items < 148 ? items : 148);
+  if (S == 1) {
+    mgemm_bf16_kernel<NSL><<<grid, THREADS_TC, Cfg::SMEM_BYTES, st>>>(
+        maps, out, m, n, alpha, beta, kb0, kps, kbt, 0, mt, nt, 1);
+    note_launches(1);
+    return (int)cudaGetLastError();
+  }
+  if (out.f32 || out.dn > 0 || out.dm > 0) return (int)cudaErrorInvalidValue;
+  double* P = splitk_buffer((size_t)S * m * n);
+  if (!P) return (int)cudaErrorMemoryAllocation;
+  TcOut po{P, 1, m, 0, 0, 0, 0, 0};
+  mgemm_bf16_kernel<NSL><<<grid, THREADS_TC, Cfg::SMEM_BYTES, st>>>(
+      maps, po, m, n, 1.0, 0.0, kb0, kps, kbt, m * n, mt, nt, S);
+  note_launches(1);
+  int e = (int)cudaGetLastError();
+  if (e) return e;
+  return splitk_reduce((stream_t)st, m, n, S, P, alpha, beta, (double*)out.C, out.scm, out.scn);
+}
+
 }  // namespace
 
+size_t tc_operand_elems(int64_t rows, int64_t k, int slices) {
+  return (size_t)slices * (size_t)pad_rows(rows) * (size_t)pad_k(k);
+}
+
+int tc_split(stream_t s, const double* src, int64_t rows, int64_t k, int64_t sr, int64_t sk,
+             int slices, void* dst, TcOperand* op) {
+  if (rows <= 0 || k <= 0 || !dst || !op || (slices != 2 && slices != 3))
+    return (int)cudaErrorInvalidValue;
+  if (((uintptr_t)dst & 15) != 0) return (int)cudaErrorMisalignedAddress;
+  EncodeFn enc = nullptr;
+  int e = encode_fn(&enc);
+  if (e) return e;
+  static_assert(sizeof(CUtensorMap) == sizeof(op->map), "tensor map storage");
+  op->rows = rows;
+  op->k = k;
+  op->rows_p = pad_rows(rows);
+  op->k_p = pad_k(k);
+  op->slices = slices;
+  launch_split((cudaStream_t)s, src, rows, k, sr, sk, op->rows_p, op->k_p, slices,
+               (__nv_bfloat16*)dst);
+  e = (int)cudaGetLastError();
+  if (e) return e;
+  return make_map(enc, reinterpret_cast<CUtensorMap*>(op->map), dst, op->rows_p, op->k_p,
+                  slices);
+}
+
+int tc_gemm(stream_t s, const TcGemm& g) {
+  if (g.m <= 0 || g.n <= 0) return 0;
+  const TcOperand* A0 = g.A[0];
+  const TcOperand* B0 = g.B[0];
+  if (!A0 || !B0 || A0->k != B0->k || A0->rows < g.m || B0->rows < g.n ||
+      A0->slices != B0->slices)
+    return (int)cudaErrorInvalidValue;
+  const TcOperand* A1 = g.A[1];
+  const TcOperand* B1 = g.B[1];
+  if ((A1 == nullptr) != (B1 == nullptr)) return (int)cudaErrorInvalidValue;
+  if (A1 && (A1->k != B1->k || A1->rows < g.m || B1->rows < g.n || A1->rows_p != A0->rows_p ||
+             B1->rows_p != B0->rows_p || A1->slices != A0->slices || B1->slices != A0->slices))
+    return (int)cudaErrorInvalidValue;
+  TcMaps maps;
+  std::memcpy(&maps.a0, A0->map, sizeof(CUtensorMap));
+  std::memcpy(&maps.b0, B0->map, sizeof(CUtensorMap));
+  std::memcpy(&maps.a1, (A1 ? A1 : A0)->map, sizeof(CUtensorMap));
+  std::memcpy(&maps.b1, (B1 ? B1 : B0)->map, sizeof(CUtensorMap));
+  const int kb0 = (int)(A0->k_p / TK);
+  const int kbt = kb0 + (A1 ? (int)(A1->k_p / TK) : 0);
+  TcOut out{g.C, g.scm, g.scn, g.dn, g.scn2, g.dm, g.scm2, g.f32 ? 1 : 0};
+  if (A0->slices == 3)
+    return launch_tc<3>((cudaStream_t)s, maps, kb0, kbt, g.m, g.n, A0->rows_p, B0->rows_p,
+                        g.alpha, g.beta, out, 1);
+  return launch_tc<2>((cudaStream_t)s, maps, kb0, kbt, g.m, g.n, A0->rows_p, B0->rows_p, g.alpha,
+                      g.beta, out, 1);
+}
+
 // C(m,n) = alpha sum_k A(m,k) B(k,n) + beta C(m,n) with the strided operands of
-// gemm_strided (batch 1): split both operands, run the tensor-core kernel.
+// gemm_strided (batch 1): split both operands into three slices, run the
+// tensor-core kernel.
 int gemm_strided_mixed(stream_t s, const Gemm& q) {
-  if (q.batch != 1) return (int)cudaErrorInvalidValue;
+  if (q.batch != 1 || q.dn != 0 || q.kseg != 0) return (int)cudaErrorInvalidValue;
   if (q.m <= 0 || q.n <= 0) return 0;
   if (q.k <= 0 || q.alpha == 0.0) return gemm_strided(s, q);
   EncodeFn enc = nullptr;
   int e = encode_fn(&enc);
   if (e) return e;
   static_assert(TM == TN, "one padding rule for A and B");
+  constexpr int NSL = 3;
   const int64_t m = q.m, n = q.n, k = q.k;
-  const int64_t mp = (m + TM - 1) / TM * TM, np = (n + TN - 1) / TN * TN;
-  const int64_t kp = (k + TK - 1) / TK * TK;
-  __nv_bfloat16* buf = split_buffer((size_t)SLICES * (mp + np) * kp);
+  const int64_t mp = pad_rows(m), np = pad_rows(n), kp = pad_k(k);
+  __nv_bfloat16* buf = split_buffer((size_t)NSL * (mp + np) * kp);
   if (!buf) return (int)cudaErrorMemoryAllocation;
   __nv_bfloat16* As = buf;
-  __nv_bfloat16* Bs = buf + (size_t)SLICES * mp * kp;
+  __nv_bfloat16* Bs = buf + (size_t)NSL * mp * kp;
   cudaStream_t st = (cudaStream_t)s;
-  auto launch_split = [&](const double* src, int64_t R, int64_t sr, int64_t sk, int64_t Rp,
-                          __nv_bfloat16* dst) {
-    int64_t tiles = ((Rp + 31) / 32) * ((kp + 31) / 32);
-    unsigned g = (unsigned)(tiles < 148 * 16 ? tiles : 148 * 16);
-    split3_kernel<<<g, dim3(32, 8), 0, st>>>(src, R, k, sr, sk, Rp, kp, dst);
-  };
-  launch_split(q.A, m, q.sam, q.sak, mp, As);  // A(m,k) = A[m sam + k sak]
-  launch_split(q.B, n, q.sbn, q.sbk, np, Bs);  // B(k,n) = B[k sbk + n sbn]
-  CUtensorMap mA, mB;
-  if ((e = make_map(enc, &mA, As, mp, kp))) return e;
-  if ((e = make_map(enc, &mB, Bs, np, kp))) return e;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(mgemm_bf16x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         SMEM_BYTES);
-    attr = true;
-  }
+  launch_split(st, q.A, m, k, q.sam, q.sak, mp, kp, NSL, As);  // A(m,k) = A[m sam + k sak]
+  launch_split(st, q.B, n, k, q.sbn, q.sbk, np, kp, NSL, Bs);  // B(k,n) = B[k sbk + n sbn]
+  TcMaps maps;
+  if ((e = make_map(enc, &maps.a0, As, mp, kp, NSL))) return e;
+  if ((e = make_map(enc, &maps.b0, Bs, np, kp, NSL))) return e;
+  maps.a1 = maps.a0;
+  maps.b1 = maps.b0;
   const int kbt = (int)(kp / TK);
   const int64_t tiles = (mp / TM) * (np / TN);
   // split K when the output has fewer tiles than SMs (at least 4 k-blocks per slice)
   int S = 1;
   if (tiles < 148 && kbt >= 8) S = (int)std::min<int64_t>((148 + tiles - 1) / tiles, kbt / 4);
-  const int kps = (kbt + S - 1) / S;
-  S = (kbt + kps - 1) / kps;
-  const int mt = (int)(mp / TM), nt = (int)(np / TN);
-  const int64_t items = (int64_t)mt * nt * S;
-  const unsigned grid = (unsigned)(items < 148 ? items : 148);
-  if (S == 1) {
-    mgemm_bf16x3_kernel<<<grid, THREADS_TC, SMEM_BYTES, st>>>(mA, mB, q.C, m, n, q.scm, q.scn,
-                                                              q.alpha, q.beta, kps, kbt, 0, mt,
-                                                              nt, 1);
-    return (int)cudaGetLastError();
-  }
-  double* P = splitk_buffer((size_t)S * m * n);
-  if (!P) return (int)cudaErrorMemoryAllocation;
-  mgemm_bf16x3_kernel<<<grid, THREADS_TC, SMEM_BYTES, st>>>(mA, mB, P, m, n, 1, m, 1.0, 0.0, kps,
-                                                            kbt, m * n, mt, nt, S);
-  e = (int)cudaGetLastError();
-  if (e) return e;
-  return splitk_reduce(s, m, n, S, P, q.alpha, q.beta, q.C, q.scm, q.scn);
+  TcOut out{q.C, q.scm, q.scn, 0, 0, 0, 0, 0};
+  return launch_tc<NSL>(st, maps, kbt, kbt, m, n, mp, np, q.alpha, q.beta, out, S);
 }
 
 int gemm_mixed(stream_t s, char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha,

@@ -39,6 +39,11 @@ int gemm(stream_t s, char ta, char tb, int64_t m, int64_t n, int64_t k, double a
 // with A(m,k) = A[b*sab + m*sam + k*sak], B(k,n) = B[b*sbb + k*sbk + n*sbn],
 // C(m,n) = C[b*scb + m*scm + n*scn] for batch b.  Batches must not write
 // overlapping C elements.
+// Optional (batch 1 only):
+//   dn > 0    C(m,n) = C[m*scm + (n % dn)*scn + (n / dn)*scn2]  (n splits into
+//             two tensor indices, e.g. (b,c) of a v^3 cube written permuted)
+//   kseg > 0  two K segments: k < kseg reads A, B as above; k >= kseg reads
+//             A1[m*sam + (k-kseg)*sak1] and B1[(k-kseg)*sbk1 + n*sbn].
 struct Gemm {
   int64_t m = 0, n = 0, k = 0, batch = 1;
   double alpha = 1.0, beta = 0.0;
@@ -48,10 +53,48 @@ struct Gemm {
   int64_t sbk = 1, sbn = 0, sbb = 0;
   double* C = nullptr;
   int64_t scm = 1, scn = 0, scb = 0;
+  int64_t dn = 0, scn2 = 0;
+  int64_t kseg = 0;
+  const double* A1 = nullptr;
+  int64_t sak1 = 0;
+  const double* B1 = nullptr;
+  int64_t sbk1 = 0;
 };
 int gemm_strided(stream_t s, const Gemm& g);
-// Split-BF16 tensor-core version of gemm_strided (batch must be 1).
+// Split-BF16 tensor-core version of gemm_strided (batch 1, no dn/kseg).
 int gemm_strided_mixed(stream_t s, const Gemm& g);
+
+// Pre-split operand of the tensor-core GEMM: X(r,k) as `slices` (2 or 3)
+// BF16 slices [slices][rows_p][k_p] (k fastest; rows padded to 128, k to 64,
+// zero filled) and the TMA descriptor over them.  tc_operand_elems() is the
+// BF16 element count of the storage; tc_split() fills it (dst 16-byte
+// aligned) from the FP64 source X(r,k) = src[r*sr + k*sk] and encodes the
+// descriptor.  Three slices reproduce FP32-level products, two slices
+// ~2^-16 relative.
+struct TcOperand {
+  alignas(64) unsigned char map[128];
+  int64_t rows = 0, rows_p = 0, k = 0, k_p = 0;
+  int slices = 0;
+};
+size_t tc_operand_elems(int64_t rows, int64_t k, int slices);
+int tc_split(stream_t s, const double* src, int64_t rows, int64_t k, int64_t sr, int64_t sk,
+             int slices, void* dst, TcOperand* op);
+// C(m,n) = alpha sum_k A(m,k) B(k,n) + beta C(m,n) over pre-split operands
+// (all with the same slice count): A[0]/B[0] give the first K segment,
+// A[1]/B[1] (optional) a second one.  C is FP64, or FP32 when f32, at
+// C[rowoff(m) + coloff(n)] with rowoff(m) = (m % dm)*scm + (m / dm)*scm2
+// (dm = 0: m*scm) and coloff(n) = (n % dn)*scn + (n / dn)*scn2 (dn = 0:
+// n*scn).  Stores are coalesced when scm == 1.
+struct TcGemm {
+  int64_t m = 0, n = 0;
+  double alpha = 1.0, beta = 0.0;
+  const TcOperand* A[2] = {nullptr, nullptr};
+  const TcOperand* B[2] = {nullptr, nullptr};
+  void* C = nullptr;
+  bool f32 = false;
+  int64_t scm = 1, scn = 0, dn = 0, scn2 = 0, dm = 0, scm2 = 0;
+};
+int tc_gemm(stream_t s, const TcGemm& g);
 
 // out = alpha * permute(in) + beta * out.  in has rank nd with dims
 // in_dims (column-major, first fastest); out dimension d is in dimension
@@ -97,23 +140,29 @@ int outer(stream_t s, int64_t na, int64_t ni, int64_t nb, int64_t nj, double alp
 int combine(stream_t s, int64_t n, int m, const double* const* X, const double* coef,
             double* out);
 
-// (T) pieces for one occupied triplet (src/cc/cc_triples.jl:113-136):
+// (T) energy of one occupied triplet (src/cc/cc_triples.jl:113-156) from
+// K[a,b,c] (FP64, or FP32 when k_f32), without storing X:
 //   X[a,b,c] = (4K[abc]-2K[acb]-2K[cba]-2K[bac]+K[cab]+K[bca]) / (eijk-ev[a]-ev[b]-ev[c])
-//   *eout    = sum K*X  (skipped when eout == nullptr)
-int triples_x(stream_t s, int nv, const double* K, double eijk, const double* ev, double* X,
-              double* scratch, double* eout);
-// K[a,b,c] = W0[a,b,c] + W1[b,a,c] + W2[a,c,b] + W3[c,b,a] + W4[b,c,a] + W5[c,a,b]
-// (the six index permutations of W^{ijk}, W^{jik}, W^{ikj}, W^{kji}, W^{jki},
-// W^{kij}); 8^3 cubes staged through shared memory.
-int triples_sumw(stream_t s, int nv, const double* const* W, double* K);
-// Cube-tiled variant of triples_x (same result).
-int triples_x_cube(stream_t s, int nv, const double* K, double eijk, const double* ev, double* X,
-                   double* scratch, double* eout);
-// IntX[:,i] += fac X.M_jk, IntX[:,j] += fac X.M_ik, IntX[:,k] += fac X.M_ij and the same for
-// IntY with N_*; M/N are nv x nv slices.  One block per virtual index, fixed order.
-int triples_int(stream_t s, int nv, const double* X, const double* Mjk, const double* Mik,
-                const double* Mij, const double* Njk, const double* Nik, const double* Nij,
-                double fac, double* IntX, double* IntY, int i, int j, int k);
+//   out[0]   = sum KE*X      (KE = KU when given, else K)
+//   out[1]   = sum X*Y,  Y[a,b,c] = g0[a] M0[b,c] + g1[b] M1[a,c] + g2[c] M2[a,b]
+//                              + f0[a] N0[b,c] + f1[b] N1[a,c] + f2[c] N2[a,b]
+// The 8^3 cubes of K are visited in orbits of the index permutations, so each
+// element of K is read once; partial sums land in `scratch` (at least
+// reduce_scratch_len() doubles) and are summed in a fixed order.  `tri` holds
+// the cube triples A <= B <= C (3 ints each) for nt = ceil(nv/8) cubes per
+// axis: triples_cube_count(nv) of them, written by triples_cube_table().
+// nv <= 1290 (32-bit element offsets).
+struct TriplesTerms {
+  const double* g[3];
+  const double* f[3];
+  const double* M[3];
+  const double* N[3];
+};
+int64_t triples_cube_count(int nv);
+void triples_cube_table(int nv, int* tri);
+int triples_energy(stream_t s, int nv, const void* K, const void* KU, bool k_f32, double eijk,
+                   const double* ev, const TriplesTerms& t, const int* tri, double* scratch,
+                   double* out);
 
 // Split-K GEMM (column-major, device pointers) whose partial products use a
 // fixed file-scope device array instead of allocated memory; m*n must not
@@ -157,6 +206,7 @@ int ladder_unpack(stream_t s, int nv, int no, int a0, int npairs, const int* pai
 
 // Count of kernels launched through this layer in this process.
 int64_t launches();
+void note_launches(int n);  // add n launches made outside dev_cuda.cu
 
 }  // namespace dev
 }  // namespace ecg

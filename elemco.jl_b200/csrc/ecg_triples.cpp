@@ -6,11 +6,22 @@
 //   W^{xyz}[a,b,c] = sum_d T^{xy}_{ad} (bd|cz) - sum_l T^{xl}_{ab} (ly|cz)
 //   K[a,b,c] = W^{ijk}[a,b,c] + W^{jik}[b,a,c] + W^{ikj}[a,c,b]
 //            + W^{kji}[c,b,a] + W^{jki}[b,c,a] + W^{kij}[c,a,b]
-// so each W is two plain GEMMs (M=v N=v^2 K=v and M=v^2 N=v K=o) that read
-// vvvo[b,c,d,k] = <bc|dk> and ovoo in place, and a cube-tiled kernel sums the
-// six permuted W's.  A fused kernel forms X and sum K*X, another accumulates
-// IntX/IntY.  Per-triplet energies are summed on the host in triplet order,
-// so the result is deterministic.
+// The six vvvo GEMMs (M=v, N=v^2, K=v) accumulate straight into K: each
+// epilogue writes W^{xyz}[a',(b',c')] to its permuted position in K.  vvvo is
+// held in two layouts, [b,c,d,k] and [c,b,d,k], chosen per permutation so
+// that the (b',c') pair maps to K through at most one index split.  On the
+// tensor cores, whose epilogue lanes run along the GEMM rows, a GEMM whose
+// a' index is not the unit stride of K is run transposed (rows (b',c')).
+// With T^{xy}_{ab} = T^{yx}_{ba} the six ovoo GEMMs pair up into three GEMMs
+// with a two-segment K of 2o, also accumulated into K.  A fused kernel forms
+// X and both energy sums (sum K X and the singles/Fock term sum X Y,
+// cc_triples.jl:113-156); per-triplet energies are summed on the host in
+// triplet order, so the result is deterministic.
+//
+// Mixed precision: every operand is split into two BF16 slices once per call
+// (vvvo in both layouts, T^{xy} per pair, T2[:,:,x,:] and T2[:,:,:,x] per
+// occupied index, ovoo per pair), the GEMMs run on the tensor cores and K is
+// kept in FP32.
 #include "ecg_triples.h"
 
 #include <cmath>
@@ -20,89 +31,279 @@ namespace ecg {
 
 namespace {
 
-// W^{xyz} for amplitudes T (T2 or covariant U2) into Wout.
-void build_W(Ctx& c, const double* T, const double* V3, const double* On, double* Wout, int x,
-             int y, int z) {
-  const int64_t o = c.no, v = c.nv, v2 = v * v, v3 = v2 * v, o2 = o * o;
-  dev::stream_t s = c.st;
-  dev::Gemm g;
-  // W[a,(b,c)] = sum_d T[a,d,x,y] vvvo[(b,c),d,z]
-  g.m = v; g.n = v2; g.k = v; g.alpha = 1.0; g.beta = 0.0;
-  g.A = T + v2 * (x + o * y); g.sam = 1; g.sak = v;
-  g.B = V3 + v3 * z; g.sbk = v2; g.sbn = 1;
-  g.C = Wout; g.scm = 1; g.scn = v;
-  check(c.mixed_active ? dev::gemm_strided_mixed(s, g) : dev::gemm_strided(s, g), "W vvvo");
-  // W[(a,b),c] -= sum_l T[a,b,x,l] ovoo[l,c,y,z]
-  g = dev::Gemm{};
-  g.m = v2; g.n = v; g.k = o; g.alpha = -1.0; g.beta = 1.0;
-  g.A = T + v2 * x; g.sam = 1; g.sak = v2 * o;
-  g.B = On + o * y + o2 * v * z; g.sbk = 1; g.sbn = o2;
-  g.C = Wout; g.scm = 1; g.scn = v2;
-  check(c.mixed_active ? dev::gemm_strided_mixed(s, g) : dev::gemm_strided(s, g), "W ovoo");
+// BF16 slices of the (T) operands in mixed precision: two slices (products
+// hi*hi + hi*lo + lo*hi, ~2^-16 relative per product) keep the (T) energy
+// within ~1e-8 relative of FP64, since the element errors average out.
+constexpr int kTriplesSlices = 2;
+
+// One W GEMM of K = P[W]: amplitudes T^{xy}, integrals of occupied z in the
+// [b,c,d] (l2 = false) or [c,b,d] (l2 = true) layout, and where W[a',n] lands
+// in K: K[a'*scm + (n % dn)*scn + (n / dn)*scn2] (dn = 0: n*scn).
+struct PermW {
+  int x, y, z;
+  bool l2;
+  int64_t scm, scn, dn, scn2;
+};
+
+// n = b' + v c' in the [b,c,d] layout, n = c' + v b' in the [c,b,d] layout
+void perm_table(int i, int j, int k, int64_t v, PermW* P) {
+  const int64_t v2 = v * v;
+  P[0] = {i, j, k, false, 1, v, 0, 0};    // W^{ijk} -> K[a',b',c'] = a' + v n
+  P[1] = {j, i, k, false, v, 1, v, v2};   // W^{jik} -> K[b',a',c'] = v a' + b' + v^2 c'
+  P[2] = {i, k, j, true, 1, v, 0, 0};     // W^{ikj} -> K[a',c',b'] = a' + v n
+  P[3] = {k, j, i, true, v2, 1, 0, 0};    // W^{kji} -> K[c',b',a'] = v^2 a' + n
+  P[4] = {j, k, i, true, v, 1, v, v2};    // W^{jki} -> K[c',a',b'] = v a' + c' + v^2 b'
+  P[5] = {k, i, j, false, v2, 1, 0, 0};   // W^{kij} -> K[b',c',a'] = v^2 a' + n
 }
 
-// K^{ijk} = P[W] for amplitudes T.
-void build_K(Ctx& c, const double* T, const double* V3, const double* On, double* const* W,
-             double* K, int i, int j, int k) {
-  const int perm[6][3] = {{i, j, k}, {j, i, k}, {i, k, j}, {k, j, i}, {j, k, i}, {k, i, j}};
-  for (int q = 0; q < 6; ++q) build_W(c, T, V3, On, W[q], perm[q][0], perm[q][1], perm[q][2]);
-  check(dev::triples_sumw(c.st, (int)c.nv, W, K), "sum W");
+// BF16 operands of one amplitude tensor (T2 or covariant U2).
+struct SplitAmps {
+  std::vector<dev::TcOperand> pair;  // T^{xy}[a,d]: rows a, k d        (x + o*y)
+  std::vector<dev::TcOperand> G;     // T2[:,:,x,l]: rows (a,b), k l    (x)
+  std::vector<dev::TcOperand> C;     // T2[:,:,l,x]: rows (a,b), k l    (x)
+};
+
+uint16_t* alloc_bf16(Ctx& c, size_t elems, const char* what) {
+  return reinterpret_cast<uint16_t*>(c.alloc((int64_t)((elems + 3) / 4), what));
+}
+
+void split_amps(Ctx& c, const double* T, SplitAmps& S) {
+  const int64_t o = c.no, v = c.nv, v2 = v * v;
+  dev::stream_t s = c.st;
+  S.pair.resize(o * o);
+  S.G.resize(o);
+  S.C.resize(o);
+  const size_t ep = dev::tc_operand_elems(v, v, kTriplesSlices);
+  const size_t eg = dev::tc_operand_elems(v2, o, kTriplesSlices);
+  uint16_t* bp = alloc_bf16(c, ep * o * o, "(T) T^{xy} BF16");
+  uint16_t* bg = alloc_bf16(c, 2 * eg * o, "(T) T2 slices BF16");
+  for (int64_t y = 0; y < o; ++y)
+    for (int64_t x = 0; x < o; ++x)
+      check(dev::tc_split(s, T + v2 * (x + o * y), v, v, 1, v, kTriplesSlices,
+                          bp + ep * (x + o * y), &S.pair[x + o * y]),
+            "split T^{xy}");
+  for (int64_t x = 0; x < o; ++x) {
+    check(dev::tc_split(s, T + v2 * x, v2, o, 1, v2 * o, kTriplesSlices, bg + eg * x, &S.G[x]),
+          "split T2 G");
+    check(dev::tc_split(s, T + v2 * o * x, v2, o, 1, v2, kTriplesSlices, bg + eg * (o + x),
+                        &S.C[x]),
+          "split T2 C");
+  }
+}
+
+// Everything the K builds read: FP64 integrals and amplitudes, or their
+// BF16 splits.
+struct TriplesOps {
+  bool mixed = false;
+  const double* V1 = nullptr;  // [b,c,d,k]
+  const double* V2 = nullptr;  // [c,b,d,k]
+  const double* On = nullptr;  // [l,j,c,k]
+  std::vector<dev::TcOperand> V1s, V2s, Ons;
+};
+
+// K^{ijk} = P[W] for amplitudes T (FP64) / Sp (mixed), into K (FP64 / FP32).
+void build_K(Ctx& c, const TriplesOps& ops, const double* T, const SplitAmps* Sp, void* K, int i,
+             int j, int k) {
+  const int64_t o = c.no, v = c.nv, v2 = v * v, v3 = v2 * v, o2 = o * o;
+  dev::stream_t s = c.st;
+  PermW P[6];
+  perm_table(i, j, k, v, P);
+  for (int q = 0; q < 6; ++q) {
+    const PermW& p = P[q];
+    if (ops.mixed) {
+      dev::TcGemm g;
+      g.alpha = 1.0; g.beta = q ? 1.0 : 0.0; g.C = K; g.f32 = true;
+      const dev::TcOperand* Ta = &Sp->pair[p.x + o * p.y];
+      const dev::TcOperand* Vb = p.l2 ? &ops.V2s[p.z] : &ops.V1s[p.z];
+      if (p.scm == 1) {  // rows a'
+        g.m = v; g.n = v2; g.A[0] = Ta; g.B[0] = Vb;
+        g.scm = 1; g.scn = p.scn; g.dn = p.dn; g.scn2 = p.scn2;
+      } else {           // rows (b',c'), columns a'
+        g.m = v2; g.n = v; g.A[0] = Vb; g.B[0] = Ta;
+        g.scm = p.scn; g.dm = p.dn; g.scm2 = p.scn2; g.scn = p.scm;
+      }
+      check(dev::tc_gemm(s, g), "W vvvo");
+    } else {
+      dev::Gemm g;
+      g.m = v; g.n = v2; g.k = v; g.alpha = 1.0; g.beta = q ? 1.0 : 0.0;
+      g.A = T + v2 * (p.x + o * p.y); g.sam = 1; g.sak = v;
+      g.B = (p.l2 ? ops.V2 : ops.V1) + v3 * p.z; g.sbk = v2; g.sbn = 1;
+      g.C = (double*)K; g.scm = p.scm; g.scn = p.scn; g.dn = p.dn; g.scn2 = p.scn2;
+      check(dev::gemm_strided(s, g), "W vvvo");
+    }
+  }
+  // ovoo terms, pairs of permutations sharing one output index order:
+  //  (1) K[a,b,c] -= sum_l T2[a,b,i,l] On[l,j,c,k] + T2[a,b,l,j] On[l,i,c,k]
+  //  (2) K[a,b,c] -= sum_l T2[a,c,i,l] On[l,k,b,j] + T2[a,c,l,k] On[l,i,b,j]
+  //  (3) K[a,b,c] -= sum_l T2[b,c,l,k] On[l,j,a,i] + T2[b,c,j,l] On[l,k,a,i]
+  auto on = [&](int y, int z) { return ops.On + o * y + o2 * v * z; };
+  if (ops.mixed) {  // rows along the unit stride of K
+    auto op = [&](int y, int z) { return &ops.Ons[y + o * z]; };
+    dev::TcGemm g;
+    g.alpha = -1.0; g.beta = 1.0; g.C = K; g.f32 = true;
+    // (1) rows (a,b), columns c
+    g.m = v2; g.n = v;
+    g.A[0] = &Sp->G[i]; g.A[1] = &Sp->C[j]; g.B[0] = op(j, k); g.B[1] = op(i, k);
+    g.scm = 1; g.scn = v2;
+    check(dev::tc_gemm(s, g), "W ovoo 1");
+    // (2) rows (a,c), columns b
+    g.m = v2; g.n = v;
+    g.A[0] = &Sp->G[i]; g.A[1] = &Sp->C[k]; g.B[0] = op(k, j); g.B[1] = op(i, j);
+    g.scm = 1; g.dm = v; g.scm2 = v2; g.scn = v;
+    check(dev::tc_gemm(s, g), "W ovoo 2");
+    // (3) rows a, columns (b,c)
+    g.m = v; g.n = v2;
+    g.A[0] = op(j, i); g.A[1] = op(k, i); g.B[0] = &Sp->C[k]; g.B[1] = &Sp->G[j];
+    g.scm = 1; g.dm = 0; g.scm2 = 0; g.scn = v;
+    check(dev::tc_gemm(s, g), "W ovoo 3");
+    return;
+  }
+  dev::Gemm g;
+  g.k = 2 * o; g.kseg = o; g.alpha = -1.0; g.beta = 1.0; g.C = (double*)K;
+  // (1) rows (a,b), columns c
+  g.m = v2; g.n = v;
+  g.A = T + v2 * i; g.sam = 1; g.sak = v2 * o; g.A1 = T + v2 * o * j; g.sak1 = v2;
+  g.B = on(j, k); g.sbk = 1; g.sbn = o2; g.B1 = on(i, k); g.sbk1 = 1;
+  g.scm = 1; g.scn = v2; g.dn = 0; g.scn2 = 0;
+  check(dev::gemm_strided(s, g), "W ovoo 1");
+  // (2) rows b, columns (a,c)
+  g.m = v; g.n = v2;
+  g.A = on(k, j); g.sam = o2; g.sak = 1; g.A1 = on(i, j); g.sak1 = 1;
+  g.B = T + v2 * i; g.sbk = v2 * o; g.sbn = 1; g.B1 = T + v2 * o * k; g.sbk1 = v2;
+  g.scm = v; g.scn = 1; g.dn = v; g.scn2 = v2;
+  check(dev::gemm_strided(s, g), "W ovoo 2");
+  // (3) rows (b,c), columns a
+  g.m = v2; g.n = v;
+  g.A = T + v2 * o * k; g.sam = 1; g.sak = v2; g.A1 = T + v2 * j; g.sak1 = v2 * o;
+  g.B = on(j, i); g.sbk = 1; g.sbn = o2; g.B1 = on(k, i); g.sbk1 = 1;
+  g.scm = v; g.scn = 1; g.dn = 0; g.scn2 = 0;
+  check(dev::gemm_strided(s, g), "W ovoo 3");
 }
 
 }  // namespace
 
 void pert_triples(Ctx& c, const double* U1h, const double* U2h, double* et, double* etb) {
-  const int64_t o = c.no, v = c.nv, Q = c.nq, v3 = v * v * v;
+  const int64_t o = c.no, v = c.nv, v2 = v * v, v3 = v2 * v, n = c.n;
   const bool lam = (U1h != nullptr);
+  const bool mixed = c.mixed_active;
   dev::stream_t s = c.st;
-  // integrals, allocated per call (v^3 o + o^3 v doubles) and freed on exit
+  // everything allocated here is freed on exit
   struct Scope {
     Ctx& c;
     size_t n0;
     ~Scope() { c.release_to(n0); }
   } scope{c, c.allocs.size()};
-  double* V3 = c.alloc(v3 * o, "(T) vvvo");
+
+  TriplesOps ops;
+  ops.mixed = mixed;
   double* On = c.alloc(o * o * o * v, "(T) ovoo");
-  double* Wb[6];
-  for (int q = 0; q < 6; ++q) Wb[q] = c.alloc(v3, "(T) W");
-  double* K = c.alloc(v3, "(T) K");
-  double* X = c.alloc(v3, "(T) X");
-  double* KU = lam ? c.alloc(v3, "(T) K(Lambda)") : nullptr;
-  double* U2 = lam ? c.alloc(c.n2(), "(T) U2") : nullptr;
-  double* U2c = lam ? c.alloc(c.n2(), "(T) U2 covariant") : nullptr;
-  double* IntXY = c.alloc(2 * v * o, "(T) IntX/IntY");
-  int64_t ntrip = 0;
-  for (int64_t kk = 0; kk < o; ++kk)
-    for (int64_t jj = 0; jj <= kk; ++jj)
-      for (int64_t ii = 0; ii <= jj; ++ii)
-        if (!(ii == jj && jj == kk)) ++ntrip;
-  double* Et = c.alloc(std::max<int64_t>(ntrip, 1), "(T) energies");
+  ops.On = On;
   Contractor con = c.con();
-  // vvvo[b,c,d,k] = (bd|ck): per k, a GEMM batched over d
-  for (int64_t kk = 0; kk < o; ++kk) {
+  con(1.0, c.Boo, "ljQ", c.Bvo, "ckQ", 0.0, On, "ljck");
+  // vvvo[b,c,d,k] = (bd|ck): per k, a GEMM batched over d; [c,b,d,k] by permutation
+  const int64_t d3[3] = {v, v, v};
+  const int swap01[3] = {1, 0, 2};
+  auto build_v = [&](int64_t kk, double* out) {
     dev::Gemm g;
-    g.m = v; g.n = v; g.k = Q; g.batch = v; g.alpha = 1.0; g.beta = 0.0;
+    g.m = v; g.n = v; g.k = c.nq; g.batch = v; g.alpha = 1.0; g.beta = 0.0;
     g.A = c.Bvv; g.sam = 1; g.sak = v * v; g.sab = v;
     g.B = c.Bvo + v * kk; g.sbk = v * o; g.sbn = 1; g.sbb = 0;
-    g.C = V3 + v3 * kk; g.scm = 1; g.scn = v; g.scb = v * v;
+    g.C = out; g.scm = 1; g.scn = v; g.scb = v * v;
     check(dev::gemm_strided(s, g), "vvvo");
+  };
+  if (!mixed) {
+    double* V1 = c.alloc(v3 * o, "(T) vvvo [b,c,d,k]");
+    double* V2 = c.alloc(v3 * o, "(T) vvvo [c,b,d,k]");
+    for (int64_t kk = 0; kk < o; ++kk) {
+      build_v(kk, V1 + v3 * kk);
+      check(dev::permute(s, 3, d3, swap01, 1.0, V1 + v3 * kk, 0.0, V2 + v3 * kk), "vvvo perm");
+    }
+    ops.V1 = V1;
+    ops.V2 = V2;
+  } else {
+    const size_t evs = dev::tc_operand_elems(v2, v, kTriplesSlices);
+    const size_t eos = dev::tc_operand_elems(v, o, kTriplesSlices);
+    uint16_t* bv = alloc_bf16(c, 2 * evs * o, "(T) vvvo BF16");
+    uint16_t* bo = alloc_bf16(c, eos * o * o, "(T) ovoo BF16");
+    const size_t mark = c.allocs.size();
+    double* Vt = c.alloc(v3, "(T) vvvo slab");
+    double* Vt2 = c.alloc(v3, "(T) vvvo slab");
+    ops.V1s.resize(o);
+    ops.V2s.resize(o);
+    ops.Ons.resize(o * o);
+    for (int64_t kk = 0; kk < o; ++kk) {
+      build_v(kk, Vt);
+      check(dev::tc_split(s, Vt, v2, v, 1, v2, kTriplesSlices, bv + evs * kk, &ops.V1s[kk]),
+            "split vvvo");
+      check(dev::permute(s, 3, d3, swap01, 1.0, Vt, 0.0, Vt2), "vvvo perm");
+      check(dev::tc_split(s, Vt2, v2, v, 1, v2, kTriplesSlices, bv + evs * (o + kk),
+                          &ops.V2s[kk]),
+            "split vvvo");
+    }
+    for (int64_t z = 0; z < o; ++z)
+      for (int64_t y = 0; y < o; ++y)
+        check(dev::tc_split(s, On + o * y + o * o * v * z, v, o, o * o, 1, kTriplesSlices,
+                            bo + eos * (y + o * z), &ops.Ons[y + o * z]),
+              "split ovoo");
+    check(dev::sync(s), "sync");
+    c.release_to(mark);
   }
-  con(1.0, c.Boo, "ljQ", c.Bvo, "ckQ", 0.0, On, "ljck");
-  check(dev::memset0(IntXY, 2 * v * o * 8, s), "memset");
-  double* IntX = IntXY;
-  double* IntY = IntXY + v * o;
+
+  void* K = mixed ? (void*)c.alloc((v3 + 1) / 2, "(T) K") : (void*)c.alloc(v3, "(T) K");
+  void* KU = nullptr;
+  double* U2c = nullptr;
   if (lam) {
+    KU = mixed ? (void*)c.alloc((v3 + 1) / 2, "(T) K(Lambda)")
+               : (void*)c.alloc(v3, "(T) K(Lambda)");
+    double* U2 = c.alloc(c.n2(), "(T) U2");
+    U2c = c.alloc(c.n2(), "(T) U2 covariant");
     check(dev::h2d(U2, U2h, c.n2() * 8, s), "h2d U2");
     // contra2covariant (cctools.jl:935-938): (2 U2[a,b,i,j] + U2[b,a,i,j]) / 3
     check(dev::axpby(s, c.n2(), 2.0 / 3.0, U2, 0.0, U2c), "U2c");
     con.permute(1.0 / 3.0, U2, "baij", 1.0, U2c, "abij");
   }
+  SplitAmps ST, SU;
+  if (mixed) {
+    split_amps(c, c.T2(), ST);
+    if (lam) split_amps(c, U2c, SU);
+  }
+
+  // singles / Fock vectors: g = T1 (or U1/2), f[a,i] = fock[i, o+a]
+  std::vector<double> gh(v * o), fh(v * o);
+  {
+    std::vector<double> T1h(v * o);
+    if (!lam) {
+      check(dev::d2h(T1h.data(), c.T1(), v * o * 8, s), "d2h");
+      check(dev::sync(s), "sync");
+    }
+    for (int64_t i = 0; i < o; ++i)
+      for (int64_t a = 0; a < v; ++a) {
+        gh[a + v * i] = lam ? 0.5 * U1h[a + v * i] : T1h[a + v * i];
+        fh[a + v * i] = c.fock_host[i + (o + a) * n];
+      }
+  }
+  double* gf = c.alloc(2 * v * o, "(T) singles/Fock vectors");
+  check(dev::h2d(gf, gh.data(), v * o * 8, s), "h2d");
+  check(dev::h2d(gf + v * o, fh.data(), v * o * 8, s), "h2d");
+  const int64_t ncube = dev::triples_cube_count((int)v);
+  std::vector<int> trih(3 * ncube);
+  dev::triples_cube_table((int)v, trih.data());
+  int* tri = reinterpret_cast<int*>(c.alloc((3 * ncube + 1) / 2, "(T) cube table"));
+  check(dev::h2d(tri, trih.data(), 3 * ncube * sizeof(int), s), "h2d");
+
+  int64_t ntrip = 0;
+  for (int64_t kk = 0; kk < o; ++kk)
+    for (int64_t jj = 0; jj <= kk; ++jj)
+      for (int64_t ii = 0; ii <= jj; ++ii)
+        if (!(ii == jj && jj == kk)) ++ntrip;
+  double* Et = c.alloc(std::max<int64_t>(2 * ntrip, 2), "(T) energies");
   std::vector<double> fac;
   fac.reserve(ntrip);
   const double* eps = c.fock_host.data();
-  const int64_t n = c.n;
   const double* ev = c.eps + o;
   const double* Nsrc = lam ? U2c : c.T2();
+  auto M = [&](int x, int y) { return c.Kvvoo + v2 * (x + o * y); };
+  auto N = [&](int x, int y) { return Nsrc + v2 * (x + o * y); };
   int64_t t = 0;
   for (int k = 0; k < o; ++k)
     for (int j = 0; j <= k; ++j) {
@@ -114,51 +315,37 @@ void pert_triples(Ctx& c, const double* U1h, const double* U2h, double* et, doub
           f = 1.0;
         }
         const double eijk = eps[i + i * n] + eps[j + j * n] + eps[k + k * n];
-        build_K(c, c.T2(), V3, On, Wb, K, i, j, k);
-        if (!lam) {
-          check(dev::triples_x_cube(s, (int)v, K, eijk, ev, X, c.red, Et + t), "triples X");
-        } else {
-          check(dev::triples_x_cube(s, (int)v, K, eijk, ev, X, c.red, nullptr), "triples X");
-          build_K(c, U2c, V3, On, Wb, KU, i, j, k);
-          check(dev::dot(s, v3, KU, X, c.red, Et + t), "triples E");
-        }
-        const int64_t v2 = v * v;
-        auto M = [&](int x, int y) { return c.Kvvoo + v2 * (x + o * y); };
-        auto N = [&](int x, int y) { return Nsrc + v2 * (x + o * y); };
-        check(dev::triples_int(s, (int)v, X, M(j, k), M(i, k), M(i, j), N(j, k), N(i, k), N(i, j),
-                               f, IntX, IntY, i, j, k),
-              "triples Int");
+        build_K(c, ops, c.T2(), &ST, K, i, j, k);
+        if (lam) build_K(c, ops, U2c, &SU, KU, i, j, k);
+        dev::TriplesTerms tt;
+        tt.g[0] = gf + v * i; tt.g[1] = gf + v * j; tt.g[2] = gf + v * k;
+        tt.f[0] = gf + v * (o + i); tt.f[1] = gf + v * (o + j); tt.f[2] = gf + v * (o + k);
+        tt.M[0] = M(j, k); tt.M[1] = M(i, k); tt.M[2] = M(i, j);
+        tt.N[0] = N(j, k); tt.N[1] = N(i, k); tt.N[2] = N(i, j);
+        check(dev::triples_energy(s, (int)v, K, KU, mixed, eijk, ev, tt, tri, c.red, Et + 2 * t),
+              "triples energy");
         fac.push_back(f);
         ++t;
       }
     }
-  std::vector<double> Eh(ntrip), IX(2 * v * o);
-  if (ntrip) check(dev::d2h(Eh.data(), Et, ntrip * 8, s), "d2h");
-  check(dev::d2h(IX.data(), IntXY, 2 * v * o * 8, s), "d2h");
-  std::vector<double> T1h(v * o);
-  check(dev::d2h(T1h.data(), c.T1(), v * o * 8, s), "d2h");
+  std::vector<double> Eh(2 * ntrip);
+  if (ntrip) check(dev::d2h(Eh.data(), Et, 2 * ntrip * 8, s), "d2h");
   check(dev::sync(s), "sync");
-  if (c.mixed_active) {
+  if (mixed) {
     int tc = 0;
     check(dev::tc_error(&tc), "tc_error");
     if (tc) throw Error(ECG_ERR_TIMEOUT, "tensor-core GEMM wait timed out in (T)");
   }
-  double Enb3 = 0.0;
-  for (int64_t q = 0; q < ntrip; ++q) Enb3 += fac[q] * Eh[q];
-  // singles and Fock contributions (cc_triples.jl:143-156 / :286-294)
-  double En3 = 0.0;
-  for (int64_t i = 0; i < o; ++i)
-    for (int64_t a = 0; a < v; ++a) {
-      double x = IX[a + v * i], y = IX[v * o + a + v * i];
-      if (!lam) En3 += T1h[a + v * i] * x;
-      else En3 += 0.5 * U1h[a + v * i] * x;
-      En3 += c.fock_host[i + (o + a) * n] * y;
-    }
-  En3 += Enb3;
+  // sum K X, and the singles / Fock term sum X Y (cc_triples.jl:143-156 / :286-294)
+  double Enb3 = 0.0, Esf = 0.0;
+  for (int64_t q = 0; q < ntrip; ++q) {
+    Enb3 += fac[q] * Eh[2 * q];
+    Esf += fac[q] * Eh[2 * q + 1];
+  }
+  const double En3 = Enb3 + Esf;
   if (!std::isfinite(En3)) throw Error(ECG_ERR_NONFINITE, "non-finite (T) energy");
   *et = En3;
   *etb = Enb3;
-  (void)Q;
 }
 
 }  // namespace ecg
