@@ -51,6 +51,14 @@ def parse_args():
     p.add_argument("--cpu-sample", type=int, default=2, help="CPU-baseline iterations")
     p.add_argument("--tts", action="store_true",
                    help="CCSD(T) time-to-solution, FP64 vs mixed, on --workload (one line)")
+    p.add_argument("--gradient", action="store_true",
+                   help="analytic dE/dlambda (Lambda rrule) vs finite differences, FP64 and "
+                        "mixed, on --workload (one line)")
+    p.add_argument("--sweep", action="store_true",
+                   help="DCSD time per iteration and device memory, FP64 vs mixed, over the "
+                        "C6..C10 alkane sizes (one line)")
+    p.add_argument("--occ", type=int, default=0,
+                   help="--tts only: override the occupied count (smaller profiling cases)")
     return p.parse_args()
 
 
@@ -170,7 +178,7 @@ def run_tts(a):
     import ecgpu
     from ecgpu.synthetic import WORKLOADS, make_workload
     no, nv, nq = WORKLOADS[a.workload]
-    B, h1, e0, no = make_workload(a.workload)
+    B, h1, e0, no = make_workload(a.workload, no=a.occ or None)
     ntrip = sum(1 for k in range(no) for j in range(k + 1) for i in range(j + 1)
                 if not (i == j == k))
     ft = ntrip * (12.0 * nv**4 + 12.0 * no * nv**3)
@@ -197,7 +205,8 @@ def run_tts(a):
                          "ccsd_tflops_per_iter": fcc * r["iterations"] / tcc / 1e12,
                          "pert_t_tflops": ft / tt / 1e12}
     f64, mx = out["fp64"], out["mixed"]
-    line = {"metric": "CCSD(T) time-to-solution", "workload": a.workload,
+    line = {"metric": "CCSD(T) time-to-solution",
+            "workload": a.workload + (f" with o={no}" if a.occ else ""),
             "shape": {"o": no, "v": nv, "nQ": nq}, "unit": "s", "fp64": f64, "mixed": mx,
             "speedup": f64["total_s"] / mx["total_s"],
             "dE_uEh": abs((mx["E_ccsd"] + mx["E_T"]) - (f64["E_ccsd"] + f64["E_T"])) * 1e6,
@@ -206,10 +215,116 @@ def run_tts(a):
     print(json.dumps(line), flush=True)
 
 
+def run_gradient(a):
+    """dE/dlambda for h + lambda P through the Lambda-equation rrule, against
+    the fourth-order central difference (step 1e-3) of converged energies,
+    in FP64 and mixed precision (one JSON line).  P: seeded random symmetric
+    MO-basis one-electron operator standing in for a dipole component."""
+    import torch
+    import ecgpu
+    from ecgpu.driver import ECInfo, FDump, rrule_cc_energy
+    from ecgpu.synthetic import make_workload
+    B, h, e0, no = make_workload(a.workload, no=a.occ or None)
+    rng = np.random.default_rng(11)
+    P = rng.standard_normal(h.shape)
+    P = 0.5 * (P + P.T)
+    P /= np.linalg.norm(P, 2)  # unit spectral norm, a field-like strength
+    tight = dict(thr=1e-14, conven=1.0, maxit=200)
+    dc = a.method == "dcsd"
+    out = {}
+    for prec in ("fp64", "mixed"):
+        EC = ECInfo()
+        EC.fd = FDump(h, e0, 2 * no, B=B)
+        EC.set("cc", **tight)
+        EC.set("gpu", precision=prec)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        E, pullback = rrule_cc_energy(EC, a.method)
+        torch.cuda.synchronize()
+        t_an = time.perf_counter() - t0
+        analytic = float(np.sum(pullback(1.0) * P))
+        ctx = EC.context()
+        ctx.set_precision(ecgpu.ECG_PREC_MIXED if prec == "mixed" else ecgpu.ECG_PREC_FP64)
+        d = 1e-3
+        Es = {}
+        for k in (-2, -1, 1, 2):
+            ctx.set_system(B, h + k * d * P, e0, no)
+            _, _, ehf = ctx.fock()
+            _, T1, T2 = ctx.mp2()
+            r = ctx.cc_solve(T1, T2, dc=dc, opts=ctx.opts(**tight))
+            Es[k] = ehf + r["E"]
+        fd = (Es[-2] - 8 * Es[-1] + 8 * Es[1] - Es[2]) / (12 * d)
+        out[prec] = {"E": E, "dE_dlambda": analytic, "fd4": fd, "abs_err": abs(analytic - fd),
+                     "rrule_s": t_an}
+        EC.context().close()
+    line = {"metric": "CC energy gradient via Lambda rrule", "workload": a.workload,
+            "method": a.method, "shape": {"o": no, "v": B.shape[0] - no, "nQ": B.shape[2]},
+            "fp64": out["fp64"], "mixed": out["mixed"],
+            "mixed_vs_fp64_dE_dlambda": abs(out["mixed"]["dE_dlambda"] - out["fp64"]["dE_dlambda"]),
+            "mixed_vs_fp64_E_uEh": abs(out["mixed"]["E"] - out["fp64"]["E"]) * 1e6,
+            "perturbation": "seeded random symmetric MO one-electron operator of unit spectral "
+                            "norm, FD step 1e-3",
+            "data": "synthetic DF factors (see ecgpu/synthetic.py)"}
+    print(json.dumps(line), flush=True)
+
+
+def run_sweep(a):
+    """DCSD time per iteration (CUDA events on the library stream, mean of
+    a.steps after a.warmup) and device memory in use, FP64 vs mixed, for the
+    C6H14..C10H22/cc-pVDZ sizes (one JSON line)."""
+    import torch
+    import ecgpu
+    from ecgpu.synthetic import WORKLOADS, make_workload
+    rows = []
+    for name in ("c6h14_vdz", "c7h16_vdz", "c8h18_vdz", "c9h20_vdz", "c10h22_vdz"):
+        no, nv, nq = WORKLOADS[name]
+        B, h1, e0, no = make_workload(name)
+        row = {"workload": name, "o": no, "v": nv, "nQ": nq}
+        for prec, pname in ((ecgpu.ECG_PREC_FP64, "fp64"), (ecgpu.ECG_PREC_MIXED, "mixed")):
+            torch.cuda.synchronize()
+            free0, _ = torch.cuda.mem_get_info()
+            with ecgpu.Context(0) as ctx:
+                ctx.set_precision(prec)
+                ctx.set_system(B, h1, e0, no)
+                _, T1, T2 = ctx.mp2()
+                stream = torch.cuda.ExternalStream(ctx.stream())
+                ctx.cc_load(T1, T2)
+                for _ in range(a.warmup):
+                    ctx.cc_step(dc=True)
+                ctx.cc_load(T1, T2)
+                torch.cuda.synchronize()
+                e = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+                e[0].record(stream)
+                for _ in range(a.steps):
+                    ctx.cc_step(dc=True)
+                e[1].record(stream)
+                torch.cuda.synchronize()
+                free1, _ = torch.cuda.mem_get_info()
+                row[pname] = {"ms_per_iter": e[0].elapsed_time(e[1]) / a.steps,
+                              "device_mem_gb": (free0 - free1) / 1e9,
+                              "algorithmic_tflops": algorithmic_flops(no, nv, nq, dc=True)
+                              * a.steps
+                              / (e[0].elapsed_time(e[1]) / 1000.0) / 1e12}
+        row["speedup"] = row["fp64"]["ms_per_iter"] / row["mixed"]["ms_per_iter"]
+        rows.append(row)
+    line = {"metric": "DCSD time per iteration, FP64 vs mixed, alkane size sweep",
+            "unit": "ms/iter", "steps": a.steps, "warmup": a.warmup, "rows": rows,
+            "note": "v^3 o intermediates are never formed: the ladder is built per a-block "
+                    "from B^Q_ab",
+            "data": "synthetic DF factors (see ecgpu/synthetic.py)"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse_args()
     if a.tts:
         run_tts(a)
+        return
+    if a.gradient:
+        run_gradient(a)
+        return
+    if a.sweep:
+        run_sweep(a)
         return
     from ecgpu.synthetic import WORKLOADS, make_workload
     wl = WORKLOADS[a.workload]

@@ -17,6 +17,7 @@ struct ecg_ctx : Ctx {};
 
 struct ecg_diis {
   ecg_ctx* ctx;
+  uint64_t generation;  // the context's system generation its buffers belong to
   DiisState st;
   double* v;
   double* r;
@@ -382,6 +383,24 @@ int ecg_one_rdm(ecg_ctx* c, const double* T1, const double* T2, const double* U1
   });
 }
 
+int ecg_energy_gradient(ecg_ctx* c, const double* T1, const double* T2, const double* U1,
+                        const double* U2, double* G) {
+  if (!c) return ECG_ERR_ARG;
+  return guarded(c, [&] {
+    need_system(*c);
+    need_ptr(G, "G");
+    load_T(*c, T1, T2);
+    need_ptr(U1, "U1");
+    need_ptr(U2, "U2");
+    lambda_load_U(*c, U1, U2);
+    // correlation part: the 1RDM with all T1 terms; reference part: the
+    // closed-shell HF density, 2 on the occupied diagonal
+    one_rdm(*c, nullptr, G);
+    const int64_t n = c->n;
+    for (int64_t i = 0; i < c->no; ++i) G[i + n * i] += 2.0;
+  });
+}
+
 int ecg_diis_create(ecg_ctx* c, int32_t maxdiis, double resthr, int64_t len, ecg_diis** out) {
   if (!c || !out) return ECG_ERR_ARG;
   *out = nullptr;
@@ -392,6 +411,7 @@ int ecg_diis_create(ecg_ctx* c, int32_t maxdiis, double resthr, int64_t len, ecg
     need_system(*c);
     if (len <= 0) throw Error(ECG_ERR_ARG, "len must be positive");
     diis_reset(*c, d->st, maxdiis, resthr, len, false);
+    d->generation = c->generation;
     d->v = c->alloc(len, "diis vec");
     d->r = c->alloc(len, "diis res");
   });
@@ -411,6 +431,9 @@ int ecg_diis_perform(ecg_diis* d, double* vec, const double* res) {
     need_ptr(res, "res");
     check_finite(vec, d->st.len, "vec");
     check_finite(res, d->st.len, "res");
+    if (d->generation != c->generation)
+      throw Error(ECG_ERR_STATE, "DIIS object belongs to an earlier system: set_system freed "
+                                 "its buffers; create a new one");
     check(dev::h2d(d->v, vec, d->st.len * 8, c->st), "h2d");
     check(dev::h2d(d->r, res, d->st.len * 8, c->st), "h2d");
     diis_perform(*c, d->st, d->v, d->r);

@@ -63,6 +63,12 @@ void Ctx::free_all() {
   if (hscal) dev::hfree_pinned(hscal);
   hscal = nullptr;
   have_system = false;
+  // buffers allocated on first use must be allocated again for the next system
+  U = RU = vT = D1 = dD1 = nullptr;
+  lambda_ready = false;
+  ws_base = nullptr;
+  ws.init(nullptr, 0);
+  ++generation;
 }
 
 double scal(Ctx& c, int i) { return c.hscal[i]; }

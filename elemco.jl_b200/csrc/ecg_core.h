@@ -29,6 +29,7 @@ struct Ctx {
   std::string err;
   uint64_t memcap = 0, memused = 0;
   std::vector<std::pair<void*, size_t>> allocs;
+  uint64_t generation = 0;  // bumped whenever free_all() releases the system's buffers
   int prec = ECG_PREC_FP64;
   bool mixed_active = false;  // route large GEMMs to the split-BF16 tensor-core GEMM
 

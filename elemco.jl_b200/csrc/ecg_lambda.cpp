@@ -287,7 +287,16 @@ LambdaResult lambda_solve(Ctx& c, bool dc, const ecg_cc_opts& o) {
   const double* ev = c.eps + c.no;
   LambdaResult r;
   double prev = 0.0;
+  // ECG_PREC_MIXED: the Lambda residual's large GEMMs use split-BF16 tensor-core
+  // products until the squared residual is below 100 thr, then FP64
+  // iterations refine; convergence is only declared on an FP64 residual.
+  bool mixed_phase = (c.prec == ECG_PREC_MIXED);
+  struct Restore {
+    Ctx& c;
+    ~Restore() { c.mixed_active = false; }
+  } restore{c};
   for (int it = 1; it <= o.maxit; ++it) {
+    c.mixed_active = mixed_phase;
     lambda_residual(c, dc);
     double* R1 = c.RU;
     double* R2 = c.RU + n1;
@@ -312,6 +321,10 @@ LambdaResult lambda_solve(Ctx& c, bool dc, const ecg_cc_opts& o) {
     prev = norm;
     if (!std::isfinite(norm) || !std::isfinite(r.normR))
       throw Error(ECG_ERR_NONFINITE, "non-finite value in Lambda iteration");
+    if (mixed_phase) {
+      if (r.normR < 100.0 * o.thr) mixed_phase = false;
+      continue;
+    }
     if (r.normR < o.thr && std::fabs(r.dnorm) < thren) {
       r.converged = true;
       break;

@@ -66,6 +66,7 @@ SIGNATURES = {
                                    C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "ecg_lambda_pert_t": (C.c_int, [_P, _D, _D, _D, _D, _D, _D]),
     "ecg_one_rdm": (C.c_int, [_P, _D, _D, _D, _D, _D, _D]),
+    "ecg_energy_gradient": (C.c_int, [_P, _D, _D, _D, _D, _D]),
     "ecg_diis_create": (C.c_int, [_P, C.c_int32, C.c_double, C.c_int64, C.POINTER(_P)]),
     "ecg_diis_perform": (C.c_int, [_P, _D, _D]),
     "ecg_diis_destroy": (C.c_int, [_P]),

@@ -158,6 +158,14 @@ class Context:
                                       dptr(as_f(U2)), dptr(D1), dptr(dD1)))
         return D1, dD1
 
+    def energy_gradient(self, T1, T2, U1, U2):
+        """dE/dh (n x n, MO basis, orbitals fixed) of the converged CC energy:
+        the T1-dressed 1RDM plus the HF density."""
+        G = fvec((self.n, self.n))
+        self._chk(self._L.ecg_energy_gradient(self._h, dptr(as_f(T1)), dptr(as_f(T2)),
+                                              dptr(as_f(U1)), dptr(as_f(U2)), dptr(G)))
+        return G
+
     def cc_step_host(self, T1, T2, dc=False):
         """One iteration with host amplitudes (updated in place)."""
         out = fvec(5)

@@ -329,6 +329,46 @@ def ccdriver(EC, method, fcidump=""):
     return out
 
 
+def rrule_cc_energy(EC, method, h=None, fcidump=""):
+    """Reverse rule of the total closed-shell CCSD/DCSD energy E(h).
+
+    `h` is the MO-basis one-electron matrix (default: that of the integrals);
+    orbitals are held fixed.  Returns (E, pullback) with pullback(dE) = dE * G,
+    G = dE/dh from the Lambda (adjoint) equations: the T1-dressed 1RDM plus the
+    HF density (ecg_energy_gradient).  For a field term h + lambda P (e.g. a
+    dipole operator P) dE/dlambda = sum(G * P).  This is the rule a Julia
+    ChainRules.rrule for the @cc energy returns; the reference itself has no
+    analytic property path (it computes the densities, src/cc/cc_lagrange.jl:786-791).
+    """
+    name, dc, lam, pert = parse_method(method)
+    if pert or name not in ("CCSD", "DCSD"):
+        raise ValueError("energy gradients are available for ccsd, dcsd, λccsd and λdcsd")
+    B, h0, e0, nocc = _system_from(EC, fcidump)
+    h = h0 if h is None else np.asarray(h, dtype=float)
+    ctx = EC.context()
+    o = EC.options
+    ctx.set_precision(ECG_PREC_MIXED if o["gpu"].precision == "mixed" else ECG_PREC_FP64)
+    ctx.set_system(B, h, e0, nocc)
+    _, _, EHF = ctx.fock()
+    _, T1, T2 = ctx.mp2()
+    opts = ctx.opts(thr=o["cc"].thr, conven=o["cc"].conven, maxit=o["cc"].maxit,
+                    shifts=o["cc"].shifts, shiftp=o["cc"].shiftp, maxdiis=o["diis"].maxdiis,
+                    resthr=o["diis"].resthr)
+    r = ctx.cc_solve(T1, T2, dc=dc, opts=opts)
+    if not r["converged"]:
+        raise RuntimeError("CC iterations did not converge")
+    lr = ctx.lambda_solve(r["T1"], r["T2"], dc=dc, opts=opts)
+    if not lr["converged"]:
+        raise RuntimeError("CC-LM iterations did not converge")
+    G = ctx.energy_gradient(r["T1"], r["T2"], lr["U1"], lr["U2"])
+    E = EHF + r["E"]
+
+    def pullback(dE):
+        return dE * G
+
+    return E, pullback
+
+
 def cc(EC, method, fcidump=""):
     """``@cc method`` (src/ElemCo.jl:523-548)."""
     return ccdriver(EC, method, fcidump=fcidump)

@@ -14,6 +14,8 @@ Shapes of the named workloads (active orbitals after freezing O/C 1s):
   (H2O)_3/cc-pVDZ  o=12 v=57  nQ=252
   (H2O)_4/cc-pVDZ  o=16 v=76  nQ=336
   (H2O)_6/cc-pVTZ  o=24 v=318 nQ=846
+  C_nH_2n+2/cc-pVDZ, n=6..10: 14n+5(2n+2) basis functions, o=3n+1 (C 1s
+  frozen), v = nbf-(4n+1), nQ ~ 3.46 nbf (cc-pVDZ-RI)
 """
 import numpy as np
 
@@ -24,6 +26,9 @@ WORKLOADS = {
     "h2o4_vdz": (16, 76, 336),
     "h2o6_vtz": (24, 318, 846),
     "c6h14_vdz": (19, 129, 532),
+    "c7h16_vdz": (22, 149, 616),
+    "c8h18_vdz": (25, 169, 700),
+    "c9h20_vdz": (28, 189, 784),
     "c10h22_vdz": (31, 209, 868),
 }
 
@@ -58,7 +63,9 @@ def make_system(no, nv, nq, seed=1234, emp2_per_occ=-0.05):
     return B, h1, 0.0, eps
 
 
-def make_workload(name, seed=1234):
-    no, nv, nq = WORKLOADS[name]
+def make_workload(name, seed=1234, no=None):
+    """(B, h1, e0, no) of a named workload; `no` overrides its occupied count."""
+    no0, nv, nq = WORKLOADS[name]
+    no = no or no0
     B, h1, e0, eps = make_system(no, nv, nq, seed=seed)
     return B, h1, e0, no

@@ -128,6 +128,17 @@ int ecg_lambda_pert_t(ecg_ctx* ctx, const double* T1, const double* T2,
 int ecg_one_rdm(ecg_ctx* ctx, const double* T1, const double* T2,
                 const double* U1, const double* U2, double* D1, double* dD1);
 
+/* Analytic gradient of the converged CCSD/DCSD energy with respect to the MO
+ * one-electron matrix h (n x n, orbitals held fixed): G = dD1 + the HF
+ * density (2 on the occupied diagonal), dD1 the T1-dressed 1RDM of
+ * calc_1RDM (src/cc/cc_lagrange.jl:786-791) at converged amplitudes T1/T2 and
+ * multipliers U1/U2 (ecg_lambda_solve).  For a one-electron perturbation
+ * h + lambda P, dE/dlambda = sum_pq G[p,q] P[p,q].  The reference stops at
+ * the densities; this contraction is the pullback behind the Julia/Python
+ * rrule of the CC energy. */
+int ecg_energy_gradient(ecg_ctx* ctx, const double* T1, const double* T2,
+                        const double* U1, const double* U2, double* G);
+
 /* Stand-alone DIIS on device vectors of length len (src/solvers/diis.jl:34-305,
  * plain dot).  Vectors are host arrays; the history stays on the device. */
 typedef struct ecg_diis ecg_diis;
