@@ -118,6 +118,34 @@ __device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
       : "d"(a), "d"(b));
 }
 
+// m16n8kK FP64 MMA (K = 4, 8, 16; sm_90+ shapes).  Fragments, with g = lane/4
+// and t = lane%4: A (16 x K) a[2j] = A(g, t+4j), a[2j+1] = A(g+8, t+4j);
+// B (K x 8) b[j] = B(t+4j, g); C (16 x 8) c0,c1 = C(g, 2t..2t+1),
+// c2,c3 = C(g+8, 2t..2t+1).
+template <int K>
+__device__ __forceinline__ void dmma16(double (&d)[4], const double* a, const double* b) {
+  if constexpr (K == 4) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
+        "{%0,%1,%2,%3};\n"
+        : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+        : "d"(a[0]), "d"(a[1]), "d"(b[0]));
+  } else if constexpr (K == 8) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+        "{%8,%9}, {%0,%1,%2,%3};\n"
+        : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+  } else {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, "
+        "{%4,%5,%6,%7,%8,%9,%10,%11}, {%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
+        : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]),
+          "d"(a[7]), "d"(b[0]), "d"(b[1]), "d"(b[2]), "d"(b[3]));
+  }
+}
+
 template <int BM, int BN, int BK, int WM, int WN, int STAGES, int MINB = 1>
 struct GemmCfg {
   static constexpr int WARPS_M = BM / WM;
@@ -130,12 +158,19 @@ struct GemmCfg {
   static constexpr size_t SMEM = (size_t)STAGES * (A_STAGE + B_STAGE) * sizeof(double);
 };
 
-template <int BM, int BN, int BK, int WM, int WN, int STAGES, int MINB>
+// KMMA = 0: mma.m8n8k4 (8-row fragments); KMMA = 4, 8, 16: mma.m16n8kKMMA.
+// FLAGS: bit 0 = two K segments (kseg/A1/B1), bit 1 = split column index (dn);
+// plain GEMMs instantiate neither, so their loader and epilogue stay minimal.
+constexpr int GF_SEG = 1, GF_DN = 2;
+template <int BM, int BN, int BK, int WM, int WN, int STAGES, int MINB, int KMMA, int FLAGS>
 __global__ void __launch_bounds__(GemmCfg<BM, BN, BK, WM, WN, STAGES>::THREADS, MINB)
     dgemm_kernel(GemmArgs g) {
   using Cfg = GemmCfg<BM, BN, BK, WM, WN, STAGES>;
   constexpr int NT = Cfg::THREADS;
-  constexpr int MT = WM / 8, NTL = WN / 8;
+  constexpr int RH = (KMMA == 0) ? 8 : 16;  // rows of one MMA fragment
+  constexpr int NACC = (KMMA == 0) ? 2 : 4;  // accumulators per fragment and thread
+  constexpr int MT = WM / RH, NTL = WN / 8;
+  static_assert(KMMA == 0 || BK % KMMA == 0, "BK must be a multiple of the MMA depth");
   extern __shared__ double smem[];
   double* As = smem;
   double* Bs = smem + STAGES * Cfg::A_STAGE;
@@ -167,9 +202,13 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, BK, WM, WN, STAGES>::THREADS, 
         int64_t gm = m0 + mm, gk = k0 + kk;
         bool ok = gm < g.m && gk < kdep;
         const double* src = A;
-        if (ok)
-          src = (g.kseg > 0 && gk >= g.kseg) ? g.A1 + gm * g.sam + (gk - g.kseg) * g.sak1
-                                              : A + gm * g.sam + gk * g.sak;
+        if constexpr ((FLAGS & GF_SEG) != 0) {
+          if (ok)
+            src = (gk >= g.kseg) ? g.A1 + gm * g.sam + (gk - g.kseg) * g.sak1
+                                 : A + gm * g.sam + gk * g.sak;
+        } else {
+          if (ok) src = A + gm * g.sam + gk * g.sak;
+        }
         cp_async8(as + kk * Cfg::LDA_S + mm, src, ok);
       }
     }
@@ -182,19 +221,25 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, BK, WM, WN, STAGES>::THREADS, 
         int64_t gn = n0 + nn, gk = k0 + kk;
         bool ok = gn < g.n && gk < kdep;
         const double* src = B;
-        if (ok)
-          src = (g.kseg > 0 && gk >= g.kseg) ? g.B1 + (gk - g.kseg) * g.sbk1 + gn * g.sbn
-                                              : B + gk * g.sbk + gn * g.sbn;
+        if constexpr ((FLAGS & GF_SEG) != 0) {
+          if (ok)
+            src = (gk >= g.kseg) ? g.B1 + (gk - g.kseg) * g.sbk1 + gn * g.sbn
+                                 : B + gk * g.sbk + gn * g.sbn;
+        } else {
+          if (ok) src = B + gk * g.sbk + gn * g.sbn;
+        }
         cp_async8(bs + kk * Cfg::LDB_S + nn, src, ok);
       }
     }
   };
 
-  double acc[MT][NTL][2];
+  double acc[MT][NTL][NACC];
 #pragma unroll
   for (int i = 0; i < MT; ++i)
 #pragma unroll
-    for (int j = 0; j < NTL; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    for (int j = 0; j < NTL; ++j)
+#pragma unroll
+      for (int c = 0; c < NACC; ++c) acc[i][j][c] = 0.0;
 
 #pragma unroll
   for (int s = 0; s < STAGES - 1; ++s) {
@@ -209,17 +254,52 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, BK, WM, WN, STAGES>::THREADS, 
     cp_async_commit();
     const double* as = As + (kt % STAGES) * Cfg::A_STAGE;
     const double* bs = Bs + (kt % STAGES) * Cfg::B_STAGE;
+    if constexpr (KMMA == 0) {
 #pragma unroll
-    for (int kk = 0; kk < BK; kk += 4) {
-      double af[MT], bf[NTL];
+      for (int kk = 0; kk < BK; kk += 4) {
+        double af[MT], bf[NTL];
 #pragma unroll
-      for (int i = 0; i < MT; ++i) af[i] = as[(kk + tq) * Cfg::LDA_S + wm0 + i * 8 + gq];
+        for (int i = 0; i < MT; ++i) af[i] = as[(kk + tq) * Cfg::LDA_S + wm0 + i * 8 + gq];
 #pragma unroll
-      for (int j = 0; j < NTL; ++j) bf[j] = bs[(kk + tq) * Cfg::LDB_S + wn0 + j * 8 + gq];
+        for (int j = 0; j < NTL; ++j) bf[j] = bs[(kk + tq) * Cfg::LDB_S + wn0 + j * 8 + gq];
 #pragma unroll
-      for (int i = 0; i < MT; ++i)
+        for (int i = 0; i < MT; ++i)
 #pragma unroll
-        for (int j = 0; j < NTL; ++j) dmma884(acc[i][j], af[i], bf[j]);
+          for (int j = 0; j < NTL; ++j) {
+            double d2[2] = {acc[i][j][0], acc[i][j][1]};
+            dmma884(d2, af[i], bf[j]);
+            acc[i][j][0] = d2[0];
+            acc[i][j][1] = d2[1];
+          }
+      }
+    } else {
+      constexpr int KQ = KMMA / 4;
+#pragma unroll
+      for (int kk = 0; kk < BK; kk += KMMA) {
+        double af[MT][2 * KQ], bf[NTL][KQ];
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+          for (int q = 0; q < KQ; ++q) {
+            const double* ap = as + (kk + tq + 4 * q) * Cfg::LDA_S + wm0 + i * 16 + gq;
+            af[i][2 * q] = ap[0];
+            af[i][2 * q + 1] = ap[8];
+          }
+#pragma unroll
+        for (int j = 0; j < NTL; ++j)
+#pragma unroll
+          for (int q = 0; q < KQ; ++q)
+            bf[j][q] = bs[(kk + tq + 4 * q) * Cfg::LDB_S + wn0 + j * 8 + gq];
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+          for (int j = 0; j < NTL; ++j) {
+            double d4[4] = {acc[i][j][0], acc[i][j][1], acc[i][j][2], acc[i][j][3]};
+            dmma16<KMMA>(d4, af[i], bf[j]);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) acc[i][j][c] = d4[c];
+          }
+      }
     }
   }
   cp_async_wait<0>();
@@ -230,41 +310,48 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, BK, WM, WN, STAGES>::THREADS, 
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const int64_t col = n0 + wn0 + j * 8 + 2 * tq + h;
-      coff[j][h] = g.dn > 0 ? (col % g.dn) * g.scn + (col / g.dn) * g.scn2 : col * g.scn;
+      if constexpr ((FLAGS & GF_DN) != 0)
+        coff[j][h] = (col % g.dn) * g.scn + (col / g.dn) * g.scn2;
+      else
+        coff[j][h] = col * g.scn;
     }
 #pragma unroll
-  for (int i = 0; i < MT; ++i) {
-    int64_t row = m0 + wm0 + i * 8 + gq;
-    if (row >= g.m) continue;
+  for (int i = 0; i < MT; ++i)
 #pragma unroll
-    for (int j = 0; j < NTL; ++j) {
+    for (int rr = 0; rr < NACC / 2; ++rr) {
+      const int64_t row = m0 + wm0 + i * RH + 8 * rr + gq;
+      if (row >= g.m) continue;
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        int64_t col = n0 + wn0 + j * 8 + 2 * tq + h;
-        if (col < g.n) {
-          double* cp = C + row * g.scm + coff[j][h];
-          double v = g.alpha * acc[i][j][h];
-          if (g.beta != 0.0) v += g.beta * *cp;
-          *cp = v;
+      for (int j = 0; j < NTL; ++j) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          int64_t col = n0 + wn0 + j * 8 + 2 * tq + h;
+          if (col < g.n) {
+            double* cp = C + row * g.scm + coff[j][h];
+            double v = g.alpha * acc[i][j][2 * rr + h];
+            if (g.beta != 0.0) v += g.beta * *cp;
+            *cp = v;
+          }
         }
       }
     }
-  }
 }
 
-template <int BM, int BN, int BK, int WM, int WN, int STAGES, int MINB = 1>
+template <int BM, int BN, int BK, int WM, int WN, int STAGES, int MINB = 1, int KMMA = 0,
+          int FLAGS = 0>
 static int launch_gemm(const GemmArgs& g, int64_t batch, cudaStream_t st) {
   using Cfg = GemmCfg<BM, BN, BK, WM, WN, STAGES>;
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(dgemm_kernel<BM, BN, BK, WM, WN, STAGES, MINB>,
+    cudaFuncSetAttribute(dgemm_kernel<BM, BN, BK, WM, WN, STAGES, MINB, KMMA, FLAGS>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
     attr = true;
   }
   int64_t gx = (g.m + BM - 1) / BM, gy = (g.n + BN - 1) / BN;
   if (gy > 65535 || batch > 65535) return (int)cudaErrorInvalidConfiguration;
   dim3 grid((unsigned)gx, (unsigned)gy, (unsigned)batch);
-  dgemm_kernel<BM, BN, BK, WM, WN, STAGES, MINB><<<grid, Cfg::THREADS, Cfg::SMEM, st>>>(g);
+  dgemm_kernel<BM, BN, BK, WM, WN, STAGES, MINB, KMMA, FLAGS>
+      <<<grid, Cfg::THREADS, Cfg::SMEM, st>>>(g);
   return launched();
 }
 
@@ -446,7 +533,10 @@ static int gemm_launch(stream_t s, const Gemm& q) {
     g.sak1 = q.sak1;
     g.B1 = q.B1;
     g.sbk1 = q.sbk1;
-    return launch_gemm<64, 64, 16, 32, 32, 3, 3>(g, 1, st);
+    if (q.kseg > 0 && q.dn > 0)
+      return launch_gemm<64, 64, 16, 32, 32, 3, 3, 0, GF_SEG | GF_DN>(g, 1, st);
+    if (q.kseg > 0) return launch_gemm<64, 64, 16, 32, 32, 3, 3, 0, GF_SEG>(g, 1, st);
+    return launch_gemm<64, 64, 16, 32, 32, 3, 3, 0, GF_DN>(g, 1, st);
   }
   // Split-K for GEMMs whose output covers too few tiles to fill the SMs:
   // each z-slice writes a partial product, a fixed-order reduction sums them.
@@ -477,9 +567,9 @@ static int gemm_launch(stream_t s, const Gemm& q) {
                                                           q.C, q.scm, q.scn);
     return launched();
   }
-  // 64x64 tiles, 4 warps of 32x32, 3 CTAs per SM: the best of the measured
-  // configurations on both the small (o^3 v^3 at o=16, v=76) and the large
-  // (8192^3, 7632^3) shapes on B200.
+  // 64x64 tiles, 4 warps of 32x32, mma.m8n8k4, 3 CTAs per SM: the best or
+  // within 2% of the best measured configuration (tile sizes, m16n8k{4,8,16})
+  // on every CCSD/(T) shape on B200 (elemco.jl_b200/gemm_configs_bench.cu).
   return launch_gemm<64, 64, 16, 32, 32, 3, 3>(g, q.batch, st);
 }
 
