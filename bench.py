@@ -192,15 +192,18 @@ def run_tts(a):
             ctx.set_precision(prec)
             ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
             torch.cuda.synchronize()
+            clocks = Clocks(0)
+            clocks.start()
             ev[0].record(stream)
             r = ctx.cc_solve(T1, T2)
             ev[1].record(stream)
             et, etb = ctx.pert_t(r["T1"], r["T2"])
             ev[2].record(stream)
             torch.cuda.synchronize()
+            clk = clocks.stop()
             tcc = ev[0].elapsed_time(ev[1]) / 1000.0
             tt = ev[1].elapsed_time(ev[2]) / 1000.0
-            out[name] = {"ccsd_s": tcc, "pert_t_s": tt, "total_s": tcc + tt,
+            out[name] = {"ccsd_s": tcc, "pert_t_s": tt, "total_s": tcc + tt, "clocks": clk,
                          "iterations": r["iterations"], "E_ccsd": r["E"], "E_T": et,
                          "ccsd_tflops_per_iter": fcc * r["iterations"] / tcc / 1e12,
                          "pert_t_tflops": ft / tt / 1e12}

@@ -1066,28 +1066,42 @@ __device__ __forceinline__ int pick3(int i, int s0, int s1, int s2) {
   return i == 0 ? s0 : (i == 1 ? s1 : s2);
 }
 
-// One block per orbit of cube triples A <= B <= C.  The six cubes K[S_s0 +
-// x, S_s1 + y, S_s2 + z] (s a permutation, S = 8*(A,B,C)) are staged in
-// shared memory with the M/N blocks and the vectors they need.  Thread
-// (x,y,z) then owns the element e0 = S + (x,y,z) and its six orderings: it
-// reads K at each ordering (one value per cube), forms their six X values
-// with one reciprocal of the common denominator, and adds
-// sum_e K_e X_e and sum_e X_e Y_e over the orderings.  Every ordered element
-// of the orbit is reached |stabiliser| times (1, 2 or 6 when two or three of
-// A, B, C coincide), which the weight undoes.
+template <int BYTES>
+__device__ __forceinline__ void cp_async_n(void* smem, const void* gmem, bool pred) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const int sz = pred ? BYTES : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(s), "l"(gmem), "n"(BYTES),
+               "r"(sz));
+}
+
+// One block per orbit of cube triples A <= B <= C at a time.  The six cubes
+// K[S_s0 + x, S_s1 + y, S_s2 + z] (s a permutation, S = 8*(A,B,C)) are staged
+// in shared memory, in K's own precision, with the M/N blocks and vectors
+// they need; the loads of the next orbit (cp.async, double-buffered) run while
+// the current one is evaluated.  Thread (x,y,z) owns the element
+// e0 = S + (x,y,z) and its six orderings: it reads K at each ordering (one
+// value per cube), forms their six X values with one reciprocal of the common
+// denominator, and adds sum_e K_e X_e and sum_e X_e Y_e over the orderings.
+// Every ordered element of the orbit is reached |stabiliser| times (1, 2 or 6
+// when two or three of A, B, C coincide), which the weight undoes.
 template <typename T, bool HAS_U>
-__global__ void __launch_bounds__(512, 2) triples_energy_kernel(int nv, const T* __restrict__ K,
+struct EnergySmem {
+  static constexpr int CUBES = 6 * TCUBE_ELEMS;
+  static constexpr int CUBE_BYTES = ((HAS_U ? 2 : 1) * CUBES * (int)sizeof(T) + 15) / 16 * 16;
+  static constexpr int BUF = CUBE_BYTES + TS_STAGE * 8;
+  static constexpr int BYTES = 2 * BUF;
+};
+
+template <typename T, bool HAS_U>
+__global__ void __launch_bounds__(512, 1) triples_energy_kernel(int nv, const T* __restrict__ K,
                                                                 const T* __restrict__ KU,
                                                                 double eijk,
                                                                 const double* __restrict__ ev,
                                                                 TriplesTerms tt,
                                                                 const int* __restrict__ tri,
                                                                 int ntri, double* part) {
-  extern __shared__ double tsm[];
-  double* cubeK = tsm;                                   // [6][648]
-  double* cubeU = cubeK + 6 * TCUBE_ELEMS;               // [6][648] (HAS_U)
-  double* pmat = cubeU + (HAS_U ? 6 * TCUBE_ELEMS : 0);  // [w][pair][64]
-  double* pvec = pmat + TS_MAT;                          // [w][pos][8]
+  using L = EnergySmem<T, HAS_U>;
+  extern __shared__ __align__(16) unsigned char tsm_raw[];
   __shared__ double sh[32];
   const int v = nv, tid = threadIdx.x;
   const int l[3] = {tid & 7, (tid >> 3) & 7, tid >> 6};
@@ -1098,58 +1112,68 @@ __global__ void __launch_bounds__(512, 2) triples_energy_kernel(int nv, const T*
   for (int q = 0; q < 6; ++q)
     koff[q] = q * TCUBE_ELEMS + l[perm3(q, 0)] + TPITCH * (l[perm3(q, 1)] + TPITCH * l[perm3(q, 2)]);
   constexpr int NSTAGE = (TS_STAGE + 511) / 512;
-  const double XW[6] = {4.0, -2.0, -2.0, -2.0, 1.0, 1.0};
-  double eK = 0.0, eY = 0.0;
-  for (int t = blockIdx.x; t < ntri; t += gridDim.x) {
+
+  // cp.async of orbit t into buffer b (one commit group per call)
+  auto issue = [&](int t, int b) {
+    unsigned char* base = tsm_raw + b * L::BUF;
+    T* cK = reinterpret_cast<T*>(base);
+    T* cU = cK + L::CUBES;
+    double* pm = reinterpret_cast<double*>(base + L::CUBE_BYTES);
     const int S0 = tri[3 * t] * TCUBE, S1 = tri[3 * t + 1] * TCUBE, S2 = tri[3 * t + 2] * TCUBE;
-    // global loads of the orbit, then the shared-memory stores
-    double kv[6], uv[HAS_U ? 6 : 1], sv[NSTAGE];
 #pragma unroll
     for (int q = 0; q < 6; ++q) {
       const int x = pick3(perm3(q, 0), S0, S1, S2) + l[0];
       const int y = pick3(perm3(q, 1), S0, S1, S2) + l[1];
       const int z = pick3(perm3(q, 2), S0, S1, S2) + l[2];
       const bool ok = x < v && y < v && z < v;
-      const int idx = x + v * (y + v * z);
-      kv[q] = ok ? (double)K[idx] : 0.0;
-      if (HAS_U) uv[HAS_U ? q : 0] = ok ? (double)KU[idx] : 0.0;
+      const int idx = ok ? x + v * (y + v * z) : 0;
+      cp_async_n<(int)sizeof(T)>(cK + q * TCUBE_ELEMS + lme, K + idx, ok);
+      if (HAS_U) cp_async_n<(int)sizeof(T)>(cU + q * TCUBE_ELEMS + lme, KU + idx, ok);
     }
 #pragma unroll
     for (int u = 0; u < NSTAGE; ++u) {
       const int e = tid + 512 * u;
-      double val = 0.0;
       if (e < TS_MAT) {
         const int w = e / 384, pr = (e >> 6) % 6, i = e & 7, j = (e >> 3) & 7;
         const int px = pr >> 1, py0 = pr & 1, py = py0 < px ? py0 : py0 + 1;
         const int r0 = pick3(px, S0, S1, S2) + i, c0 = pick3(py, S0, S1, S2) + j;
         const double* src = w == 0 ? tt.M[0] : w == 1 ? tt.M[1] : w == 2 ? tt.M[2]
                           : w == 3 ? tt.N[0] : w == 4 ? tt.N[1] : tt.N[2];
-        if (r0 < v && c0 < v) val = src[r0 + v * c0];
+        const bool ok = r0 < v && c0 < v;
+        cp_async_n<8>(pm + e, ok ? src + r0 + v * c0 : src, ok);
       } else if (e < TS_STAGE) {
         const int f = e - TS_MAT, w = f / 24, pos = (f >> 3) % 3, i = f & 7;
         const int x = pick3(pos, S0, S1, S2) + i;
         const double* src = w == 0 ? tt.g[0] : w == 1 ? tt.g[1] : w == 2 ? tt.g[2]
                           : w == 3 ? tt.f[0] : w == 4 ? tt.f[1] : w == 5 ? tt.f[2] : ev;
-        if (x < v) val = src[x];
+        const bool ok = x < v;
+        cp_async_n<8>(pm + e, ok ? src + x : src, ok);
       }
-      sv[u] = val;
     }
-#pragma unroll
-    for (int q = 0; q < 6; ++q) {
-      cubeK[q * TCUBE_ELEMS + lme] = kv[q];
-      if (HAS_U) cubeU[q * TCUBE_ELEMS + lme] = uv[HAS_U ? q : 0];
-    }
-#pragma unroll
-    for (int u = 0; u < NSTAGE; ++u) {
-      const int e = tid + 512 * u;
-      if (e < TS_STAGE) pmat[e] = sv[u];
-    }
-    __syncthreads();
+    cp_async_commit();
+  };
+
+  const double XW[6] = {4.0, -2.0, -2.0, -2.0, 1.0, 1.0};
+  double eK = 0.0, eY = 0.0;
+  int b = 0;
+  if (blockIdx.x < ntri) issue(blockIdx.x, 0);
+  for (int t = blockIdx.x; t < ntri; t += gridDim.x, b ^= 1) {
+    const int tn = t + gridDim.x;
+    if (tn < ntri) issue(tn, b ^ 1);
+    else cp_async_commit();  // an empty group keeps the group count in step
+    cp_async_wait<1>();      // this orbit's copies have landed ...
+    __syncthreads();         // ... for every thread
+    const unsigned char* base = tsm_raw + b * L::BUF;
+    const T* cK = reinterpret_cast<const T*>(base);
+    const T* cU = cK + L::CUBES;
+    const double* pmat = reinterpret_cast<const double*>(base + L::CUBE_BYTES);
+    const double* pvec = pmat + TS_MAT;
+    const int S0 = tri[3 * t] * TCUBE, S1 = tri[3 * t + 1] * TCUBE, S2 = tri[3 * t + 2] * TCUBE;
     const int a0 = S0 + l[0], b0 = S1 + l[1], c0 = S2 + l[2];
     if (a0 < v && b0 < v && c0 < v) {
       double k[6];
 #pragma unroll
-      for (int q = 0; q < 6; ++q) k[q] = cubeK[koff[q]];
+      for (int q = 0; q < 6; ++q) k[q] = (double)cK[koff[q]];
       const double dinv =
           __drcp_rn(eijk - pvec[144 + l[0]] - pvec[152 + l[1]] - pvec[160 + l[2]]);
       double X[6];
@@ -1176,7 +1200,7 @@ __global__ void __launch_bounds__(512, 2) triples_energy_kernel(int nv, const T*
         const double y = vg[0][p0] * mat(0, p1, p2) + vg[1][p1] * mat(1, p0, p2) +
                          vg[2][p2] * mat(2, p0, p1) + vg[3][p0] * mat(3, p1, p2) +
                          vg[4][p1] * mat(4, p0, p2) + vg[5][p2] * mat(5, p0, p1);
-        ek += (HAS_U ? cubeU[koff[q]] : k[q]) * X[q];
+        ek += (HAS_U ? (double)cU[koff[q]] : k[q]) * X[q];
         ey += X[q] * y;
       }
       const bool ab = (S0 == S1), bc = (S1 == S2);
@@ -1184,8 +1208,9 @@ __global__ void __launch_bounds__(512, 2) triples_energy_kernel(int nv, const T*
       eK += wgt * ek;
       eY += wgt * ey;
     }
-    __syncthreads();
+    __syncthreads();  // buffer b is refilled by the next iteration's issue
   }
+  cp_async_wait<0>();
   const double r0 = block_sum(eK, sh);
   const double r1 = block_sum(eY, sh);
   if (threadIdx.x == 0) {
@@ -1199,29 +1224,40 @@ int triples_energy(stream_t s, int nv, const void* K, const void* KU, bool k_f32
                    double* out) {
   cudaStream_t st = (cudaStream_t)s;
   const int64_t ntri = triples_cube_count(nv);
-  const int g = (int)(ntri < RED_BLOCKS ? ntri : RED_BLOCKS);
   if (nv > 1290) return (int)cudaErrorInvalidValue;  // 32-bit element offsets
-  const size_t smem = ((KU ? 12 : 6) * TCUBE_ELEMS + TS_STAGE) * sizeof(double);
+  // one resident block per SM: 128 registers a thread keep the evaluation free
+  // of spills; the double-buffered loads overlap it with the next orbit
+  const int g = (int)(ntri < 148 ? ntri : 148);
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(triples_energy_kernel<double, false>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 1024);
+                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         EnergySmem<double, false>::BYTES);
     cudaFuncSetAttribute(triples_energy_kernel<float, false>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 1024);
+                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         EnergySmem<float, false>::BYTES);
     cudaFuncSetAttribute(triples_energy_kernel<double, true>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 1024);
+                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         EnergySmem<double, true>::BYTES);
     cudaFuncSetAttribute(triples_energy_kernel<float, true>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 1024);
+                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         EnergySmem<float, true>::BYTES);
     attr = true;
   }
   if (k_f32) {
-    auto k = KU ? triples_energy_kernel<float, true> : triples_energy_kernel<float, false>;
-    k<<<g, 512, smem, st>>>(nv, (const float*)K, (const float*)KU, eijk, ev, t, tri, (int)ntri,
-                            scratch);
+    if (KU)
+      triples_energy_kernel<float, true><<<g, 512, EnergySmem<float, true>::BYTES, st>>>(
+          nv, (const float*)K, (const float*)KU, eijk, ev, t, tri, (int)ntri, scratch);
+    else
+      triples_energy_kernel<float, false><<<g, 512, EnergySmem<float, false>::BYTES, st>>>(
+          nv, (const float*)K, nullptr, eijk, ev, t, tri, (int)ntri, scratch);
   } else {
-    auto k = KU ? triples_energy_kernel<double, true> : triples_energy_kernel<double, false>;
-    k<<<g, 512, smem, st>>>(nv, (const double*)K, (const double*)KU, eijk, ev, t, tri,
-                            (int)ntri, scratch);
+    if (KU)
+      triples_energy_kernel<double, true><<<g, 512, EnergySmem<double, true>::BYTES, st>>>(
+          nv, (const double*)K, (const double*)KU, eijk, ev, t, tri, (int)ntri, scratch);
+    else
+      triples_energy_kernel<double, false><<<g, 512, EnergySmem<double, false>::BYTES, st>>>(
+          nv, (const double*)K, nullptr, eijk, ev, t, tri, (int)ntri, scratch);
   }
   int e = launched();
   if (e) return e;

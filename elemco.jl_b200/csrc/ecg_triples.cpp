@@ -9,7 +9,9 @@
 // The six vvvo GEMMs (M=v, N=v^2, K=v) accumulate straight into K: each
 // epilogue writes W^{xyz}[a',(b',c')] to its permuted position in K.  vvvo is
 // held in two layouts, [b,c,d,k] and [c,b,d,k], chosen per permutation so
-// that the (b',c') pair maps to K through at most one index split.  On the
+// that the (b',c') pair maps to K through at most one index split; with that
+// choice the permutations pair up into three GEMMs of K depth 2v whose two
+// halves write the same K positions.  On the
 // tensor cores, whose epilogue lanes run along the GEMM rows, a GEMM whose
 // a' index is not the unit stride of K is run transposed (rows (b',c')).
 // With T^{xy}_{ab} = T^{yx}_{ba} the six ovoo GEMMs pair up into three GEMMs
@@ -106,30 +108,42 @@ void build_K(Ctx& c, const TriplesOps& ops, const double* T, const SplitAmps* Sp
              int j, int k) {
   const int64_t o = c.no, v = c.nv, v2 = v * v, v3 = v2 * v, o2 = o * o;
   dev::stream_t s = c.st;
+  // vvvo terms: the six W GEMMs pair into three that write the same K
+  // positions (perm_table: ijk+ikj, jik+jki, kji+kij); on the tensor cores
+  // each pair is one GEMM with a two-segment K of 2v (one K pass instead of
+  // two).
   PermW P[6];
   perm_table(i, j, k, v, P);
-  for (int q = 0; q < 6; ++q) {
-    const PermW& p = P[q];
+  const int pairs[3][2] = {{0, 2}, {1, 4}, {3, 5}};
+  for (int q = 0; q < 3; ++q) {
+    const PermW& p0 = P[pairs[q][0]];
+    const PermW& p1 = P[pairs[q][1]];
     if (ops.mixed) {
       dev::TcGemm g;
       g.alpha = 1.0; g.beta = q ? 1.0 : 0.0; g.C = K; g.f32 = true;
-      const dev::TcOperand* Ta = &Sp->pair[p.x + o * p.y];
-      const dev::TcOperand* Vb = p.l2 ? &ops.V2s[p.z] : &ops.V1s[p.z];
-      if (p.scm == 1) {  // rows a'
-        g.m = v; g.n = v2; g.A[0] = Ta; g.B[0] = Vb;
-        g.scm = 1; g.scn = p.scn; g.dn = p.dn; g.scn2 = p.scn2;
-      } else {           // rows (b',c'), columns a'
-        g.m = v2; g.n = v; g.A[0] = Vb; g.B[0] = Ta;
-        g.scm = p.scn; g.dm = p.dn; g.scm2 = p.scn2; g.scn = p.scm;
+      auto Ta = [&](const PermW& p) { return &Sp->pair[p.x + o * p.y]; };
+      auto Vb = [&](const PermW& p) { return p.l2 ? &ops.V2s[p.z] : &ops.V1s[p.z]; };
+      if (p0.scm == 1) {  // rows a'
+        g.m = v; g.n = v2;
+        g.A[0] = Ta(p0); g.A[1] = Ta(p1); g.B[0] = Vb(p0); g.B[1] = Vb(p1);
+        g.scm = 1; g.scn = p0.scn; g.dn = p0.dn; g.scn2 = p0.scn2;
+      } else {            // rows (b',c'), columns a'
+        g.m = v2; g.n = v;
+        g.A[0] = Vb(p0); g.A[1] = Vb(p1); g.B[0] = Ta(p0); g.B[1] = Ta(p1);
+        g.scm = p0.scn; g.dm = p0.dn; g.scm2 = p0.scn2; g.scn = p0.scm;
       }
       check(dev::tc_gemm(s, g), "W vvvo");
     } else {
-      dev::Gemm g;
-      g.m = v; g.n = v2; g.k = v; g.alpha = 1.0; g.beta = q ? 1.0 : 0.0;
-      g.A = T + v2 * (p.x + o * p.y); g.sam = 1; g.sak = v;
-      g.B = (p.l2 ? ops.V2 : ops.V1) + v3 * p.z; g.sbk = v2; g.sbn = 1;
-      g.C = (double*)K; g.scm = p.scm; g.scn = p.scn; g.dn = p.dn; g.scn2 = p.scn2;
-      check(dev::gemm_strided(s, g), "W vvvo");
+      // FP64 is bound by the MMA pipe, not by the K traffic: two plain GEMMs
+      // keep the lean single-segment loader
+      for (const PermW* p : {&p0, &p1}) {
+        dev::Gemm g;
+        g.m = v; g.n = v2; g.k = v; g.alpha = 1.0; g.beta = (q || p == &p1) ? 1.0 : 0.0;
+        g.A = T + v2 * (p->x + o * p->y); g.sam = 1; g.sak = v;
+        g.B = (p->l2 ? ops.V2 : ops.V1) + v3 * p->z; g.sbk = v2; g.sbn = 1;
+        g.C = (double*)K; g.scm = p->scm; g.scn = p->scn; g.dn = p->dn; g.scn2 = p->scn2;
+        check(dev::gemm_strided(s, g), "W vvvo");
+      }
     }
   }
   // ovoo terms, pairs of permutations sharing one output index order:
