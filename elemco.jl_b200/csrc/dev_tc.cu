@@ -37,6 +37,9 @@ constexpr int TM = 128, TN = 128, TK = 64;
 constexpr int TILE_BYTES_A = TM * TK * 2;  // 16 KiB per slice
 constexpr int TILE_BYTES_B = TN * TK * 2;
 constexpr int RING_BYTES = 192 * 1024;
+// longest K (in 64-wide k-blocks) one FP32 tensor-memory accumulator sums
+// before its partial product is handed to an FP64 reduction
+constexpr int KB_ACC = 16;
 constexpr unsigned long long WAIT_NS = 1000000000ull;  // 1 s bound on every mbarrier wait
 
 template <int NSL>
@@ -643,9 +646,12 @@ int gemm_strided_mixed(stream_t s, const Gemm& q) {
   maps.b1 = maps.b0;
   const int kbt = (int)(kp / TK);
   const int64_t tiles = (mp / TM) * (np / TN);
-  // split K when the output has fewer tiles than SMs (at least 4 k-blocks per slice)
+  // split K when the output has fewer tiles than SMs (at least 4 k-blocks per
+  // slice), and so that no FP32 accumulator sums more than KB_ACC k-blocks:
+  // the slices' partial products are added in FP64
   int S = 1;
   if (tiles < 148 && kbt >= 8) S = (int)std::min<int64_t>((148 + tiles - 1) / tiles, kbt / 4);
+  S = std::max(S, (kbt + KB_ACC - 1) / KB_ACC);
   TcOut out{q.C, q.scm, q.scn, 0, 0, 0, 0, 0};
   return launch_tc<NSL>(st, maps, kbt, kbt, m, n, mp, np, q.alpha, q.beta, out, S);
 }
