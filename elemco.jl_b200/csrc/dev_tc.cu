@@ -504,10 +504,13 @@ __nv_bfloat16* split_buffer(size_t n) {
   return g_split;
 }
 
-int make_map(EncodeFn enc, CUtensorMap* m, const void* base, int64_t rows_p, int64_t k_p,
-             int nsl) {
-  cuuint64_t dims[3] = {(cuuint64_t)k_p, (cuuint64_t)rows_p, (cuuint64_t)nsl};
-  cuuint64_t strides[2] = {(cuuint64_t)(k_p * 2), (cuuint64_t)(rows_p * k_p * 2)};
+// rows: extent of the map (rows past it read as zero); slice_stride in BF16
+// elements (default: rows * k_p, a dense [slice][row][k] block)
+int make_map(EncodeFn enc, CUtensorMap* m, const void* base, int64_t rows, int64_t k_p, int nsl,
+             int64_t slice_stride = 0) {
+  if (slice_stride == 0) slice_stride = rows * k_p;
+  cuuint64_t dims[3] = {(cuuint64_t)k_p, (cuuint64_t)rows, (cuuint64_t)nsl};
+  cuuint64_t strides[2] = {(cuuint64_t)(k_p * 2), (cuuint64_t)(slice_stride * 2)};
   cuuint32_t box[3] = {(cuuint32_t)TK, (cuuint32_t)TM, 1};
   cuuint32_t es[3] = {1, 1, 1};
   CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(base), dims, strides,
@@ -525,6 +528,16 @@ void launch_split(cudaStream_t st, const double* src, int64_t R, int64_t K, int6
   const unsigned g = (unsigned)(tiles < 148 * 16 ? tiles : 148 * 16);
   split_kernel<<<g, dim3(32, 8), 0, st>>>(src, R, K, sr, sk, Rp, Kp, nsl, dst);
   note_launches(1);
+}
+
+// K slices of a GEMM with `tiles` output tiles and kbt k-blocks: enough to
+// fill the SMs when the output has fewer tiles than SMs (at least 4 k-blocks
+// per slice), and so that no FP32 accumulator sums more than KB_ACC k-blocks
+// (the slices' partial products are added in FP64).
+int split_count(int64_t tiles, int kbt) {
+  int S = 1;
+  if (tiles < 148 && kbt >= 8) S = (int)std::min<int64_t>((148 + tiles - 1) / tiles, kbt / 4);
+  return std::max(S, (kbt + KB_ACC - 1) / KB_ACC);
 }
 
 // Launch over pre-split operands; S > 1 splits the combined k-blocks into S
@@ -582,12 +595,28 @@ int tc_split(stream_t s, const double* src, int64_t rows, int64_t k, int64_t sr,
   op->rows_p = pad_rows(rows);
   op->k_p = pad_k(k);
   op->slices = slices;
+  op->base = dst;
+  op->slice_stride = op->rows_p * op->k_p;
   launch_split((cudaStream_t)s, src, rows, k, sr, sk, op->rows_p, op->k_p, slices,
                (__nv_bfloat16*)dst);
   e = (int)cudaGetLastError();
   if (e) return e;
   return make_map(enc, reinterpret_cast<CUtensorMap*>(op->map), dst, op->rows_p, op->k_p,
                   slices);
+}
+
+int tc_view(const TcOperand& parent, int64_t row0, int64_t rows, TcOperand* out) {
+  if (!out || !parent.base || row0 < 0 || rows <= 0 || row0 + rows > parent.rows_p)
+    return (int)cudaErrorInvalidValue;
+  EncodeFn enc = nullptr;
+  int e = encode_fn(&enc);
+  if (e) return e;
+  *out = parent;
+  out->rows = rows;
+  out->rows_p = pad_rows(rows);
+  out->base = (__nv_bfloat16*)parent.base + row0 * parent.k_p;
+  return make_map(enc, reinterpret_cast<CUtensorMap*>(out->map), out->base, rows, parent.k_p,
+                  parent.slices, parent.slice_stride);
 }
 
 int tc_gemm(stream_t s, const TcGemm& g) {
@@ -611,11 +640,13 @@ int tc_gemm(stream_t s, const TcGemm& g) {
   const int kb0 = (int)(A0->k_p / TK);
   const int kbt = kb0 + (A1 ? (int)(A1->k_p / TK) : 0);
   TcOut out{g.C, g.scm, g.scn, g.dn, g.scn2, g.dm, g.scm2, g.f32 ? 1 : 0};
+  const int64_t mp = pad_rows(g.m), np = pad_rows(g.n);
+  int S = 1;
+  if (!g.f32 && g.dn == 0 && g.dm == 0) S = split_count(mp / TM * (np / TN), kbt);
   if (A0->slices == 3)
-    return launch_tc<3>((cudaStream_t)s, maps, kb0, kbt, g.m, g.n, A0->rows_p, B0->rows_p,
-                        g.alpha, g.beta, out, 1);
-  return launch_tc<2>((cudaStream_t)s, maps, kb0, kbt, g.m, g.n, A0->rows_p, B0->rows_p, g.alpha,
-                      g.beta, out, 1);
+    return launch_tc<3>((cudaStream_t)s, maps, kb0, kbt, g.m, g.n, mp, np, g.alpha, g.beta, out,
+                        S);
+  return launch_tc<2>((cudaStream_t)s, maps, kb0, kbt, g.m, g.n, mp, np, g.alpha, g.beta, out, S);
 }
 
 // C(m,n) = alpha sum_k A(m,k) B(k,n) + beta C(m,n) with the strided operands of
@@ -645,13 +676,7 @@ int gemm_strided_mixed(stream_t s, const Gemm& q) {
   maps.a1 = maps.a0;
   maps.b1 = maps.b0;
   const int kbt = (int)(kp / TK);
-  const int64_t tiles = (mp / TM) * (np / TN);
-  // split K when the output has fewer tiles than SMs (at least 4 k-blocks per
-  // slice), and so that no FP32 accumulator sums more than KB_ACC k-blocks:
-  // the slices' partial products are added in FP64
-  int S = 1;
-  if (tiles < 148 && kbt >= 8) S = (int)std::min<int64_t>((148 + tiles - 1) / tiles, kbt / 4);
-  S = std::max(S, (kbt + KB_ACC - 1) / KB_ACC);
+  const int S = split_count((mp / TM) * (np / TN), kbt);
   TcOut out{q.C, q.scm, q.scn, 0, 0, 0, 0, 0};
   return launch_tc<NSL>(st, maps, kbt, kbt, m, n, mp, np, q.alpha, q.beta, out, S);
 }

@@ -55,6 +55,23 @@ void Ctx::ensure_ws(int64_t nd) {
   ws.init(ws_base, nd);
 }
 
+void* Ctx::ensure_tc(size_t bytes) {
+  if (tc_bytes >= bytes) return tc_base;
+  if (st) dev::sync(st);
+  for (size_t q = 0; q < allocs.size(); ++q)
+    if (allocs[q].first == tc_base) {
+      dev::dfree(allocs[q].first);
+      memused -= allocs[q].second;
+      allocs.erase(allocs.begin() + q);
+      break;
+    }
+  tc_base = nullptr;
+  tc_bytes = 0;
+  tc_base = alloc((int64_t)((bytes + 7) / 8), "split-operand storage");
+  tc_bytes = bytes;
+  return tc_base;
+}
+
 void Ctx::free_all() {
   if (st) dev::sync(st);
   for (auto& a : allocs) dev::dfree(a.first);
@@ -66,6 +83,8 @@ void Ctx::free_all() {
   // buffers allocated on first use must be allocated again for the next system
   U = RU = vT = D1 = dD1 = nullptr;
   lambda_ready = false;
+  tc_base = nullptr;
+  tc_bytes = 0;
   ws_base = nullptr;
   ws.init(nullptr, 0);
   ++generation;
@@ -326,21 +345,75 @@ void ladder(Ctx& c, const double* Bf, const double* BfT, const double* T2, doubl
   double* Vm = c.ws.get(std::max<int64_t>(ncdm * maxpp, 1));
   double* Lp = c.ws.get(maxpp * nijp);
   double* Lm = c.ws.get(std::max<int64_t>(maxpp * nijm, 1));
+  // Mixed precision: the operands shared by every a-block (BfT for the V
+  // build, the packed T2 for the contractions) are split into BF16 slices once
+  // per call, each block reads row ranges of them; the per-block V+/- are
+  // split per block.  Which GEMMs go to the tensor cores follows gemm_prec's
+  // size rule.
+  const double big = 67108864.0;
+  const bool mv = c.mixed_active && (double)(v * c.lblocks[0].na) * (double)(v * v) * Q >= big;
+  const bool mp = c.mixed_active && (double)maxpp * nijp * ncdp >= big;
+  const bool mm = c.mixed_active && nijm > 0 && (double)maxpp * nijm * ncdm >= big;
+  constexpr int NSL = 3;
+  dev::TcOperand oB, oTs, oTa, oVp, oVm;
+  uint16_t *pB = nullptr, *pTs = nullptr, *pTa = nullptr, *pVp = nullptr, *pVm = nullptr;
+  if (mv || mp || mm) {
+    const size_t eB = mv ? dev::tc_operand_elems(v * v, Q, NSL) : 0;
+    const size_t eTs = mp ? dev::tc_operand_elems(nijp, ncdp, NSL) : 0;
+    const size_t eVp = mp ? dev::tc_operand_elems(maxpp, ncdp, NSL) : 0;
+    const size_t eTa = mm ? dev::tc_operand_elems(nijm, ncdm, NSL) : 0;
+    const size_t eVm = mm ? dev::tc_operand_elems(maxpp, ncdm, NSL) : 0;
+    uint16_t* base = (uint16_t*)c.ensure_tc(2 * (eB + eTs + eVp + eTa + eVm));
+    pB = base;
+    pTs = pB + eB;
+    pVp = pTs + eTs;
+    pTa = pVp + eVp;
+    pVm = pTa + eTa;
+    if (mv) check(dev::tc_split(s, BfT, v * v, Q, 1, v * v, NSL, pB, &oB), "split BfT");
+    if (mp) check(dev::tc_split(s, Ts, nijp, ncdp, ncdp, 1, NSL, pTs, &oTs), "split T+");
+    if (mm) check(dev::tc_split(s, Ta, nijm, ncdm, ncdm, 1, NSL, pTa, &oTa), "split T-");
+  }
   for (auto& b : c.lblocks) {
     const int64_t nb = v - b.a0;
     // V[c,a',d,b''] = sum_Q BfT[c,a0+a',Q] BfT[d,a0+b'',Q]
-    check(gemm_prec(c.mixed_active, s, 'N', 'T', v * b.na, v * nb, Q, 1.0, BfT + v * b.a0, v * v,
-                    BfT + v * b.a0, v * v, 0.0, V, v * b.na),
-          "gemm ladder V");
+    if (mv) {
+      dev::TcOperand a, bb;
+      check(dev::tc_view(oB, v * b.a0, v * b.na, &a), "view BfT");
+      check(dev::tc_view(oB, v * b.a0, v * nb, &bb), "view BfT");
+      dev::TcGemm g;
+      g.m = v * b.na; g.n = v * nb; g.A[0] = &a; g.B[0] = &bb;
+      g.C = V; g.scm = 1; g.scn = v * b.na;
+      check(dev::tc_gemm(s, g), "gemm ladder V");
+    } else {
+      check(dev::gemm(s, 'N', 'T', v * b.na, v * nb, Q, 1.0, BfT + v * b.a0, v * v,
+                      BfT + v * b.a0, v * v, 0.0, V, v * b.na),
+            "gemm ladder V");
+    }
     const int* pairs = c.pairs + 2 * b.poff;
     check(dev::ladder_pack_v(s, (int)v, b.a0, b.na, b.npp, pairs, c.cdp, V, Vp, Vm), "pack V");
-    check(gemm_prec(c.mixed_active, s, 'T', 'N', b.npp, nijp, ncdp, 1.0, Vp, ncdp, Ts, ncdp, 0.0,
-                    Lp, b.npp),
-          "gemm ladder +");
-    if (b.npm > 0 && nijm > 0)
-      check(gemm_prec(c.mixed_active, s, 'T', 'N', b.npm, nijm, ncdm, 1.0, Vm, ncdm, Ta, ncdm,
-                      0.0, Lm, b.npm),
-            "gemm ladder -");
+    if (mp) {
+      check(dev::tc_split(s, Vp, b.npp, ncdp, ncdp, 1, NSL, pVp, &oVp), "split V+");
+      dev::TcGemm g;
+      g.m = b.npp; g.n = nijp; g.A[0] = &oVp; g.B[0] = &oTs;
+      g.C = Lp; g.scm = 1; g.scn = b.npp;
+      check(dev::tc_gemm(s, g), "gemm ladder +");
+    } else {
+      check(dev::gemm(s, 'T', 'N', b.npp, nijp, ncdp, 1.0, Vp, ncdp, Ts, ncdp, 0.0, Lp, b.npp),
+            "gemm ladder +");
+    }
+    if (b.npm > 0 && nijm > 0) {
+      if (mm) {
+        check(dev::tc_split(s, Vm, b.npm, ncdm, ncdm, 1, NSL, pVm, &oVm), "split V-");
+        dev::TcGemm g;
+        g.m = b.npm; g.n = nijm; g.A[0] = &oVm; g.B[0] = &oTa;
+        g.C = Lm; g.scm = 1; g.scn = b.npm;
+        check(dev::tc_gemm(s, g), "gemm ladder -");
+      } else {
+        check(dev::gemm(s, 'T', 'N', b.npm, nijm, ncdm, 1.0, Vm, ncdm, Ta, ncdm, 0.0, Lm,
+                        b.npm),
+              "gemm ladder -");
+      }
+    }
     check(dev::ladder_unpack(s, (int)v, (int)o, b.a0, b.npp, pairs, c.ijp, Lp, Lm, R2),
           "ladder unpack");
   }

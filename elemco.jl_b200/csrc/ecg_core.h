@@ -64,6 +64,9 @@ struct Ctx {
 
   Arena ws;
   double* ws_base = nullptr;
+  // storage for BF16-split operands kept across GEMMs (mixed precision)
+  void* tc_base = nullptr;
+  size_t tc_bytes = 0;
 
   // ladder pair tables (device int pairs) and a-blocks
   int *cdp = nullptr, *ijp = nullptr, *pairs = nullptr;
@@ -91,6 +94,7 @@ struct Ctx {
   double* alloc(int64_t ndoubles, const char* what);
   void release_to(size_t nallocs);  // free allocations made after the first nallocs
   void ensure_ws(int64_t ndoubles);  // grow the workspace arena (outside any capture)
+  void* ensure_tc(size_t bytes);     // grow the split-operand storage (contents are lost)
   void free_all();
   Contractor con() { return Contractor(st, &ws, &ext, mixed_active); }
 };

@@ -75,13 +75,20 @@ struct TcOperand {
   alignas(64) unsigned char map[128];
   int64_t rows = 0, rows_p = 0, k = 0, k_p = 0;
   int slices = 0;
+  void* base = nullptr;        // first BF16 element of row 0, slice 0
+  int64_t slice_stride = 0;    // BF16 elements between slices
 };
 size_t tc_operand_elems(int64_t rows, int64_t k, int slices);
 int tc_split(stream_t s, const double* src, int64_t rows, int64_t k, int64_t sr, int64_t sk,
              int slices, void* dst, TcOperand* op);
+// Rows [row0, row0 + rows) of a split operand as an operand of their own (no
+// copy: a descriptor over the same storage; rows past the view read as zero).
+int tc_view(const TcOperand& parent, int64_t row0, int64_t rows, TcOperand* out);
 // C(m,n) = alpha sum_k A(m,k) B(k,n) + beta C(m,n) over pre-split operands
 // (all with the same slice count): A[0]/B[0] give the first K segment,
-// A[1]/B[1] (optional) a second one.  C is FP64, or FP32 when f32, at
+// A[1]/B[1] (optional) a second one.  A plain FP64 C (no index maps) may be
+// computed in K slices summed in FP64 (to fill the GPU and to bound the FP32
+// accumulation length).  C is FP64, or FP32 when f32, at
 // C[rowoff(m) + coloff(n)] with rowoff(m) = (m % dm)*scm + (m / dm)*scm2
 // (dm = 0: m*scm) and coloff(n) = (n % dn)*scn + (n / dn)*scn2 (dn = 0:
 // n*scn).  Stores are coalesced when scm == 1.
