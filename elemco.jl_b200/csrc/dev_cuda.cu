@@ -69,6 +69,40 @@ int d2d(void* dst, const void* src, size_t bytes, stream_t s) {
   if (!bytes) return 0;
   return (int)cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, (cudaStream_t)s);
 }
+int graph_capture_begin(stream_t s) {
+  return (int)cudaStreamBeginCapture((cudaStream_t)s, cudaStreamCaptureModeThreadLocal);
+}
+
+int graph_capture_run(stream_t s, int64_t* nodes) {
+  cudaStream_t st = (cudaStream_t)s;
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(st, &g);
+  if (e != cudaSuccess) return (int)e;
+  size_t n = 0;
+  cudaGraphGetNodes(g, nullptr, &n);
+  if (nodes) *nodes = (int64_t)n;
+  cudaGraphExec_t x = nullptr;
+  e = cudaGraphInstantiate(&x, g, 0);
+  if (e == cudaSuccess) {
+    e = cudaGraphLaunch(x, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaGraphExecDestroy(x);
+  }
+  cudaGraphDestroy(g);
+  return (int)e;
+}
+
+void graph_capture_abort(stream_t s) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing((cudaStream_t)s, &cs) == cudaSuccess &&
+      cs != cudaStreamCaptureStatusNone) {
+    cudaGraph_t g = nullptr;
+    cudaStreamEndCapture((cudaStream_t)s, &g);
+    if (g) cudaGraphDestroy(g);
+  }
+  cudaGetLastError();
+}
+
 int memset0(void* dst, size_t bytes, stream_t s) {
   if (!bytes) return 0;
   return (int)cudaMemsetAsync(dst, 0, bytes, (cudaStream_t)s);
@@ -98,6 +132,7 @@ struct GemmArgs {
   int64_t sak1 = 0;
   const double* B1 = nullptr;
   int64_t sbk1 = 0;
+  const int64_t* ptab = nullptr;  // GF_PTAB: offsets of A, B, C, A1, B1 per batch item
 };
 
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool pred) {
@@ -159,9 +194,10 @@ struct GemmCfg {
 };
 
 // KMMA = 0: mma.m8n8k4 (8-row fragments); KMMA = 4, 8, 16: mma.m16n8kKMMA.
-// FLAGS: bit 0 = two K segments (kseg/A1/B1), bit 1 = split column index (dn);
-// plain GEMMs instantiate neither, so their loader and epilogue stay minimal.
-constexpr int GF_SEG = 1, GF_DN = 2;
+// FLAGS: bit 0 = two K segments (kseg/A1/B1), bit 1 = split column index (dn),
+// bit 2 = batch items placed by an offset table (ptab) instead of strides;
+// plain GEMMs instantiate none, so their loader and epilogue stay minimal.
+constexpr int GF_SEG = 1, GF_DN = 2, GF_PTAB = 4;
 template <int BM, int BN, int BK, int WM, int WN, int STAGES, int MINB, int KMMA, int FLAGS>
 __global__ void __launch_bounds__(GemmCfg<BM, BN, BK, WM, WN, STAGES>::THREADS, MINB)
     dgemm_kernel(GemmArgs g) {
@@ -176,9 +212,25 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, BK, WM, WN, STAGES>::THREADS, 
   double* Bs = smem + STAGES * Cfg::A_STAGE;
 
   const int64_t bz = blockIdx.z;
-  const double* A = g.A + bz * g.sab;
-  const double* B = g.B + bz * g.sbb;
-  double* C = g.C + bz * g.scb;
+  const double* A;
+  const double* B;
+  double* C;
+  const double* A1 = g.A1;
+  const double* B1 = g.B1;
+  if constexpr ((FLAGS & GF_PTAB) != 0) {
+    const int64_t* pt = g.ptab + 5 * bz;
+    A = g.A + pt[0];
+    B = g.B + pt[1];
+    C = g.C + pt[2];
+    if constexpr ((FLAGS & GF_SEG) != 0) {
+      A1 = g.A1 + pt[3];
+      B1 = g.B1 + pt[4];
+    }
+  } else {
+    A = g.A + bz * g.sab;
+    B = g.B + bz * g.sbb;
+    C = g.C + bz * g.scb;
+  }
   const int64_t m0 = (int64_t)blockIdx.x * BM;
   const int64_t n0 = (int64_t)blockIdx.y * BN;
   const int tid = threadIdx.x;
@@ -204,7 +256,7 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, BK, WM, WN, STAGES>::THREADS, 
         const double* src = A;
         if constexpr ((FLAGS & GF_SEG) != 0) {
           if (ok)
-            src = (gk >= g.kseg) ? g.A1 + gm * g.sam + (gk - g.kseg) * g.sak1
+            src = (gk >= g.kseg) ? A1 + gm * g.sam + (gk - g.kseg) * g.sak1
                                  : A + gm * g.sam + gk * g.sak;
         } else {
           if (ok) src = A + gm * g.sam + gk * g.sak;
@@ -223,7 +275,7 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, BK, WM, WN, STAGES>::THREADS, 
         const double* src = B;
         if constexpr ((FLAGS & GF_SEG) != 0) {
           if (ok)
-            src = (gk >= g.kseg) ? g.B1 + (gk - g.kseg) * g.sbk1 + gn * g.sbn
+            src = (gk >= g.kseg) ? B1 + (gk - g.kseg) * g.sbk1 + gn * g.sbn
                                  : B + gk * g.sbk + gn * g.sbn;
         } else {
           if (ok) src = B + gk * g.sbk + gn * g.sbn;
@@ -523,8 +575,9 @@ static int gemm_launch(stream_t s, const Gemm& q) {
   GemmArgs g{q.A, q.B, q.C, q.m, q.n, q.k, q.sam, q.sak, q.sab, q.sbk, q.sbn, q.sbb,
              q.scm, q.scn, q.scb, q.alpha, q.beta, (q.sam != 1 && q.sak == 1) ? 1 : 0,
              (q.sbk != 1 && q.sbn == 1) ? 1 : 0, 0};
-  if (q.dn > 0 || q.kseg > 0) {
-    if (q.batch != 1 || (q.kseg > 0 && (q.kseg >= q.k || !q.A1 || !q.B1)))
+  const int flags = (q.kseg > 0 ? GF_SEG : 0) | (q.dn > 0 ? GF_DN : 0) | (q.ptab ? GF_PTAB : 0);
+  if (flags) {
+    if ((!q.ptab && q.batch != 1) || (q.kseg > 0 && (q.kseg >= q.k || !q.A1 || !q.B1)))
       return (int)cudaErrorInvalidValue;
     g.dn = q.dn;
     g.scn2 = q.scn2;
@@ -533,10 +586,21 @@ static int gemm_launch(stream_t s, const Gemm& q) {
     g.sak1 = q.sak1;
     g.B1 = q.B1;
     g.sbk1 = q.sbk1;
-    if (q.kseg > 0 && q.dn > 0)
-      return launch_gemm<64, 64, 16, 32, 32, 3, 3, 0, GF_SEG | GF_DN>(g, 1, st);
-    if (q.kseg > 0) return launch_gemm<64, 64, 16, 32, 32, 3, 3, 0, GF_SEG>(g, 1, st);
-    return launch_gemm<64, 64, 16, 32, 32, 3, 3, 0, GF_DN>(g, 1, st);
+    g.ptab = q.ptab;
+    const int64_t nb = q.batch;
+    switch (flags) {
+      case GF_SEG: return launch_gemm<64, 64, 16, 32, 32, 3, 3, 0, GF_SEG>(g, nb, st);
+      case GF_DN: return launch_gemm<64, 64, 16, 32, 32, 3, 3, 0, GF_DN>(g, nb, st);
+      case GF_SEG | GF_DN:
+        return launch_gemm<64, 64, 16, 32, 32, 3, 3, 0, GF_SEG | GF_DN>(g, nb, st);
+      case GF_PTAB: return launch_gemm<64, 64, 16, 32, 32, 3, 3, 0, GF_PTAB>(g, nb, st);
+      case GF_PTAB | GF_SEG:
+        return launch_gemm<64, 64, 16, 32, 32, 3, 3, 0, GF_PTAB | GF_SEG>(g, nb, st);
+      case GF_PTAB | GF_DN:
+        return launch_gemm<64, 64, 16, 32, 32, 3, 3, 0, GF_PTAB | GF_DN>(g, nb, st);
+      default:
+        return launch_gemm<64, 64, 16, 32, 32, 3, 3, 0, GF_PTAB | GF_SEG | GF_DN>(g, nb, st);
+    }
   }
   // Split-K for GEMMs whose output covers too few tiles to fill the SMs:
   // each z-slice writes a partial product, a fixed-order reduction sums them.
@@ -1092,15 +1156,21 @@ struct EnergySmem {
   static constexpr int BYTES = 2 * BUF;
 };
 
+// Batch item y = blockIdx.y reads K + y*kstride (and KU), its denominator
+// shift and terms from eijk_tab / tt_tab when given (else eijk0 / tt0), and
+// leaves its partial sums at part[(2y + c) * gridDim.x + blockIdx.x].
 template <typename T, bool HAS_U>
-__global__ void __launch_bounds__(512, 1) triples_energy_kernel(int nv, const T* __restrict__ K,
-                                                                const T* __restrict__ KU,
-                                                                double eijk,
-                                                                const double* __restrict__ ev,
-                                                                TriplesTerms tt,
-                                                                const int* __restrict__ tri,
-                                                                int ntri, double* part) {
+__global__ void __launch_bounds__(512, 1) triples_energy_kernel(
+    int nv, const T* __restrict__ K, const T* __restrict__ KU, int64_t kstride, double eijk0,
+    const double* __restrict__ eijk_tab, const double* __restrict__ ev, TriplesTerms tt0,
+    const TriplesTerms* __restrict__ tt_tab, const int* __restrict__ tri, int ntri,
+    double* part) {
   using L = EnergySmem<T, HAS_U>;
+  const int y = blockIdx.y;
+  K += (int64_t)y * kstride;
+  if (HAS_U) KU += (int64_t)y * kstride;
+  const TriplesTerms tt = tt_tab ? tt_tab[y] : tt0;
+  const double eijk = eijk_tab ? eijk_tab[y] : eijk0;
   extern __shared__ __align__(16) unsigned char tsm_raw[];
   __shared__ double sh[32];
   const int v = nv, tid = threadIdx.x;
@@ -1214,20 +1284,37 @@ __global__ void __launch_bounds__(512, 1) triples_energy_kernel(int nv, const T*
   const double r0 = block_sum(eK, sh);
   const double r1 = block_sum(eY, sh);
   if (threadIdx.x == 0) {
-    part[blockIdx.x] = r0;
-    part[RED_BLOCKS + blockIdx.x] = r1;
+    part[(2 * y) * gridDim.x + blockIdx.x] = r0;
+    part[(2 * y + 1) * gridDim.x + blockIdx.x] = r1;
   }
 }
 
-int triples_energy(stream_t s, int nv, const void* K, const void* KU, bool k_f32, double eijk,
-                   const double* ev, const TriplesTerms& t, const int* tri, double* scratch,
-                   double* out) {
-  cudaStream_t st = (cudaStream_t)s;
-  const int64_t ntri = triples_cube_count(nv);
-  if (nv > 1290) return (int)cudaErrorInvalidValue;  // 32-bit element offsets
+// out[2y + c] = sum_i part[(2y + c) * nparts + i], one block per (y, c), fixed order
+__global__ void final_sum_pairs_kernel(int nparts, const double* part, double* out) {
+  __shared__ double sh[32];
+  const int q = blockIdx.x;
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x) acc += part[(int64_t)q * nparts + i];
+  const double r = block_sum(acc, sh);
+  if (threadIdx.x == 0) out[q] = r;
+}
+
+static int64_t energy_grid(int nv) {
   // one resident block per SM: 128 registers a thread keep the evaluation free
   // of spills; the double-buffered loads overlap it with the next orbit
-  const int g = (int)(ntri < 148 ? ntri : 148);
+  const int64_t ntri = triples_cube_count(nv);
+  return ntri < 148 ? ntri : 148;
+}
+
+int64_t triples_energy_scratch_len(int nv, int nitems) { return 2 * energy_grid(nv) * nitems; }
+
+static int launch_energy(cudaStream_t st, int nv, int nitems, const void* K, const void* KU,
+                         int64_t kstride, bool k_f32, double eijk0, const double* eijk_tab,
+                         const double* ev, const TriplesTerms& tt0, const TriplesTerms* tt_tab,
+                         const int* tri, double* scratch, double* out) {
+  const int64_t ntri = triples_cube_count(nv);
+  if (nv > 1290 || nitems <= 0 || nitems > 65535) return (int)cudaErrorInvalidValue;
+  const int g = (int)energy_grid(nv);
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(triples_energy_kernel<double, false>,
@@ -1244,25 +1331,46 @@ int triples_energy(stream_t s, int nv, const void* K, const void* KU, bool k_f32
                          EnergySmem<float, true>::BYTES);
     attr = true;
   }
+  const dim3 grid((unsigned)g, (unsigned)nitems);
   if (k_f32) {
     if (KU)
-      triples_energy_kernel<float, true><<<g, 512, EnergySmem<float, true>::BYTES, st>>>(
-          nv, (const float*)K, (const float*)KU, eijk, ev, t, tri, (int)ntri, scratch);
+      triples_energy_kernel<float, true><<<grid, 512, EnergySmem<float, true>::BYTES, st>>>(
+          nv, (const float*)K, (const float*)KU, kstride, eijk0, eijk_tab, ev, tt0, tt_tab, tri,
+          (int)ntri, scratch);
     else
-      triples_energy_kernel<float, false><<<g, 512, EnergySmem<float, false>::BYTES, st>>>(
-          nv, (const float*)K, nullptr, eijk, ev, t, tri, (int)ntri, scratch);
+      triples_energy_kernel<float, false><<<grid, 512, EnergySmem<float, false>::BYTES, st>>>(
+          nv, (const float*)K, nullptr, kstride, eijk0, eijk_tab, ev, tt0, tt_tab, tri,
+          (int)ntri, scratch);
   } else {
     if (KU)
-      triples_energy_kernel<double, true><<<g, 512, EnergySmem<double, true>::BYTES, st>>>(
-          nv, (const double*)K, (const double*)KU, eijk, ev, t, tri, (int)ntri, scratch);
+      triples_energy_kernel<double, true><<<grid, 512, EnergySmem<double, true>::BYTES, st>>>(
+          nv, (const double*)K, (const double*)KU, kstride, eijk0, eijk_tab, ev, tt0, tt_tab,
+          tri, (int)ntri, scratch);
     else
-      triples_energy_kernel<double, false><<<g, 512, EnergySmem<double, false>::BYTES, st>>>(
-          nv, (const double*)K, nullptr, eijk, ev, t, tri, (int)ntri, scratch);
+      triples_energy_kernel<double, false><<<grid, 512, EnergySmem<double, false>::BYTES, st>>>(
+          nv, (const double*)K, nullptr, kstride, eijk0, eijk_tab, ev, tt0, tt_tab, tri,
+          (int)ntri, scratch);
   }
   int e = launched();
   if (e) return e;
-  final_sum_kernel<<<1, 256, 0, st>>>(g, 2, scratch, out);
+  final_sum_pairs_kernel<<<2 * nitems, 256, 0, st>>>(g, scratch, out);
   return launched();
+}
+
+int triples_energy(stream_t s, int nv, const void* K, const void* KU, bool k_f32, double eijk,
+                   const double* ev, const TriplesTerms& t, const int* tri, double* scratch,
+                   double* out) {
+  return launch_energy((cudaStream_t)s, nv, 1, K, KU, 0, k_f32, eijk, nullptr, ev, t, nullptr,
+                       tri, scratch, out);
+}
+
+int triples_energy_batched(stream_t s, int nv, int nitems, const void* K, const void* KU,
+                           int64_t kstride, bool k_f32, const double* eijk_tab, const double* ev,
+                           const TriplesTerms* tt_tab, const int* tri, double* scratch,
+                           double* out) {
+  TriplesTerms none{};
+  return launch_energy((cudaStream_t)s, nv, nitems, K, KU, kstride, k_f32, 0.0, eijk_tab, ev,
+                       none, tt_tab, tri, scratch, out);
 }
 
 }  // namespace dev

@@ -225,7 +225,8 @@ template <int NSL>
 __global__ void __launch_bounds__(THREADS_TC, 1)
     mgemm_bf16_kernel(const __grid_constant__ TcMaps maps, TcOut out, int64_t M, int64_t N,
                       double alpha, double beta, int kb_seg0, int kb_per_split, int kblocks_total,
-                      int64_t split_stride, int mtiles, int ntiles, int nsplit) {
+                      int64_t split_stride, int mtiles, int ntiles, int nsplit,
+                      const TcMaps* __restrict__ mtab) {
   using Cfg = TcCfg<NSL>;
   constexpr int STAGES = Cfg::STAGES, STAGE_BYTES = Cfg::STAGE_BYTES;
   extern __shared__ uint8_t smem_raw[];
@@ -278,7 +279,11 @@ __global__ void __launch_bounds__(THREADS_TC, 1)
     }
     z = (int)(it / ((int64_t)mtiles * ntiles));
   };
-  auto item_kblocks = [&](int z) { return min(kb_per_split, kblocks_total - z * kb_per_split); };
+  // z is a K slice (mtab == nullptr) or a batch item with its own operand maps
+  // (mtab[z]), each covering all k-blocks
+  auto item_kblocks = [&](int z) {
+    return mtab ? kblocks_total : min(kb_per_split, kblocks_total - z * kb_per_split);
+  };
 
   if (warp == 0) {
     if (lane == 0) {
@@ -286,7 +291,8 @@ __global__ void __launch_bounds__(THREADS_TC, 1)
       for (int64_t it = blockIdx.x; it < items && !*(volatile int*)abort_flag; it += gridDim.x) {
         int mt, nt, z;
         item_coords(it, mt, nt, z);
-        const int nk = item_kblocks(z), kb0 = z * kb_per_split;
+        const int nk = item_kblocks(z), kb0 = mtab ? 0 : z * kb_per_split;
+        const TcMaps* mp = mtab ? mtab + z : &maps;
         for (int kb = 0; kb < nk; ++kb, ++g) {
           const int s = (int)(g % STAGES);
           const int64_t u = g / STAGES;
@@ -298,8 +304,8 @@ __global__ void __launch_bounds__(THREADS_TC, 1)
           uint8_t* st = tiles + s * STAGE_BYTES;
           const int kg = kb0 + kb;
           const bool s1 = kg >= kb_seg0;
-          const CUtensorMap* ma = s1 ? &maps.a1 : &maps.a0;
-          const CUtensorMap* mb = s1 ? &maps.b1 : &maps.b0;
+          const CUtensorMap* ma = s1 ? &mp->a1 : &mp->a0;
+          const CUtensorMap* mb = s1 ? &mp->b1 : &mp->b0;
           const int kx = (s1 ? kg - kb_seg0 : kg) * TK;
           mbar_expect_tx(&full[s], STAGE_BYTES);
           for (int t = 0; t < NSL; ++t) {
@@ -559,7 +565,7 @@ int launch_tc(cudaStream_t st, const TcMaps& maps, int kb0, int kbt, int64_t m, 
   const unsigned grid = (unsigned)(items < 148 ? items : 148);
   if (S == 1) {
     mgemm_bf16_kernel<NSL><<<grid, THREADS_TC, Cfg::SMEM_BYTES, st>>>(
-        maps, out, m, n, alpha, beta, kb0, kps, kbt, 0, mt, nt, 1);
+        maps, out, m, n, alpha, beta, kb0, kps, kbt, 0, mt, nt, 1, nullptr);
     note_launches(1);
     return (int)cudaGetLastError();
   }
@@ -568,7 +574,7 @@ int launch_tc(cudaStream_t st, const TcMaps& maps, int kb0, int kbt, int64_t m, 
   if (!P) return (int)cudaErrorMemoryAllocation;
   TcOut po{P, 1, m, 0, 0, 0, 0, 0};
   mgemm_bf16_kernel<NSL><<<grid, THREADS_TC, Cfg::SMEM_BYTES, st>>>(
-      maps, po, m, n, 1.0, 0.0, kb0, kps, kbt, m * n, mt, nt, S);
+      maps, po, m, n, 1.0, 0.0, kb0, kps, kbt, m * n, mt, nt, S, nullptr);
   note_launches(1);
   int e = (int)cudaGetLastError();
   if (e) return e;
@@ -647,6 +653,63 @@ int tc_gemm(stream_t s, const TcGemm& g) {
     return launch_tc<3>((cudaStream_t)s, maps, kb0, kbt, g.m, g.n, mp, np, g.alpha, g.beta, out,
                         S);
   return launch_tc<2>((cudaStream_t)s, maps, kb0, kbt, g.m, g.n, mp, np, g.alpha, g.beta, out, S);
+}
+
+size_t tc_maps_bytes() { return sizeof(TcMaps); }
+
+int tc_maps_fill(const TcOperand* A0, const TcOperand* B0, const TcOperand* A1,
+                 const TcOperand* B1, void* dst) {
+  if (!A0 || !B0 || !dst || (A1 == nullptr) != (B1 == nullptr)) return (int)cudaErrorInvalidValue;
+  TcMaps* m = reinterpret_cast<TcMaps*>(dst);
+  std::memcpy(&m->a0, A0->map, sizeof(CUtensorMap));
+  std::memcpy(&m->b0, B0->map, sizeof(CUtensorMap));
+  std::memcpy(&m->a1, (A1 ? A1 : A0)->map, sizeof(CUtensorMap));
+  std::memcpy(&m->b1, (B1 ? B1 : B0)->map, sizeof(CUtensorMap));
+  return 0;
+}
+
+int tc_gemm_batched(stream_t s, const TcGemm& g, int batch, const void* mtab, int64_t c_stride) {
+  if (g.m <= 0 || g.n <= 0 || batch <= 0) return 0;
+  const TcOperand* A0 = g.A[0];
+  const TcOperand* B0 = g.B[0];
+  if (!A0 || !B0 || !mtab || ((uintptr_t)mtab & 63) != 0 || A0->slices != B0->slices)
+    return (int)cudaErrorInvalidValue;
+  const TcOperand* A1 = g.A[1];
+  const int kb0 = (int)(A0->k_p / TK);
+  const int kbt = kb0 + (A1 ? (int)(A1->k_p / TK) : 0);
+  const int64_t mp = pad_rows(g.m), np = pad_rows(g.n);
+  const int mt = (int)(mp / TM), nt = (int)(np / TN);
+  const int64_t items = (int64_t)mt * nt * batch;
+  const unsigned grid = (unsigned)(items < 148 ? items : 148);
+  TcOut out{g.C, g.scm, g.scn, g.dn, g.scn2, g.dm, g.scm2, g.f32 ? 1 : 0};
+  TcMaps dummy;
+  std::memset(&dummy, 0, sizeof(dummy));
+  cudaStream_t st = (cudaStream_t)s;
+  if (A0->slices == 3) {
+    using Cfg = TcCfg<3>;
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(mgemm_bf16_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           Cfg::SMEM_BYTES);
+      attr = true;
+    }
+    mgemm_bf16_kernel<3><<<grid, THREADS_TC, Cfg::SMEM_BYTES, st>>>(
+        dummy, out, g.m, g.n, g.alpha, g.beta, kb0, kbt, kbt, c_stride, mt, nt, batch,
+        (const TcMaps*)mtab);
+  } else {
+    using Cfg = TcCfg<2>;
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(mgemm_bf16_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           Cfg::SMEM_BYTES);
+      attr = true;
+    }
+    mgemm_bf16_kernel<2><<<grid, THREADS_TC, Cfg::SMEM_BYTES, st>>>(
+        dummy, out, g.m, g.n, g.alpha, g.beta, kb0, kbt, kbt, c_stride, mt, nt, batch,
+        (const TcMaps*)mtab);
+  }
+  note_launches(1);
+  return (int)cudaGetLastError();
 }
 
 // C(m,n) = alpha sum_k A(m,k) B(k,n) + beta C(m,n) with the strided operands of

@@ -27,6 +27,12 @@ int h2d(void* dst, const void* src, size_t bytes, stream_t s);
 int d2h(void* dst, const void* src, size_t bytes, stream_t s);
 int d2d(void* dst, const void* src, size_t bytes, stream_t s);
 int memset0(void* dst, size_t bytes, stream_t s);
+// Record the launches issued on s after graph_capture_begin into a CUDA graph;
+// graph_capture_run ends the capture, runs the graph once, waits for it and
+// frees it (*nodes: the number of graph nodes).
+int graph_capture_begin(stream_t s);
+int graph_capture_run(stream_t s, int64_t* nodes);
+void graph_capture_abort(stream_t s);  // end a capture in progress, discarding it
 
 // C(m,n) = alpha * sum_k opA(A)(m,k) opB(B)(k,n) + beta * C(m,n), column-major;
 // ta/tb = 'N' or 'T'.  batch > 1 uses strides sa/sb/sc between instances.
@@ -44,6 +50,8 @@ int gemm(stream_t s, char ta, char tb, int64_t m, int64_t n, int64_t k, double a
 //             two tensor indices, e.g. (b,c) of a v^3 cube written permuted)
 //   kseg > 0  two K segments: k < kseg reads A, B as above; k >= kseg reads
 //             A1[m*sam + (k-kseg)*sak1] and B1[(k-kseg)*sbk1 + n*sbn].
+//   ptab      device table of 5 offsets (elements) per batch item b, for A, B,
+//             C, A1, B1, used in place of b*sab, b*sbb, b*scb (batch >= 1).
 struct Gemm {
   int64_t m = 0, n = 0, k = 0, batch = 1;
   double alpha = 1.0, beta = 0.0;
@@ -59,6 +67,7 @@ struct Gemm {
   int64_t sak1 = 0;
   const double* B1 = nullptr;
   int64_t sbk1 = 0;
+  const int64_t* ptab = nullptr;
 };
 int gemm_strided(stream_t s, const Gemm& g);
 // Split-BF16 tensor-core version of gemm_strided (batch 1, no dn/kseg).
@@ -102,6 +111,14 @@ struct TcGemm {
   int64_t scm = 1, scn = 0, dn = 0, scn2 = 0, dm = 0, scm2 = 0;
 };
 int tc_gemm(stream_t s, const TcGemm& g);
+// Batched form: `batch` GEMMs of the shape of g (g.A/g.B give the operand
+// shapes), item b reading the operand descriptors mtab[b] (device memory,
+// 64-byte aligned, tc_maps_bytes() each, written by tc_maps_fill on the host)
+// and writing C + b*c_stride through g's index map.  One launch.
+size_t tc_maps_bytes();
+int tc_maps_fill(const TcOperand* A0, const TcOperand* B0, const TcOperand* A1,
+                 const TcOperand* B1, void* host_dst);
+int tc_gemm_batched(stream_t s, const TcGemm& g, int batch, const void* mtab, int64_t c_stride);
 
 // out = alpha * permute(in) + beta * out.  in has rank nd with dims
 // in_dims (column-major, first fastest); out dimension d is in dimension
@@ -155,7 +172,7 @@ int combine(stream_t s, int64_t n, int m, const double* const* X, const double* 
 //                              + f0[a] N0[b,c] + f1[b] N1[a,c] + f2[c] N2[a,b]
 // The 8^3 cubes of K are visited in orbits of the index permutations, so each
 // element of K is read once; partial sums land in `scratch` (at least
-// reduce_scratch_len() doubles) and are summed in a fixed order.  `tri` holds
+// triples_energy_scratch_len(nv, 1) doubles) and are summed in a fixed order.  `tri` holds
 // the cube triples A <= B <= C (3 ints each) for nt = ceil(nv/8) cubes per
 // axis: triples_cube_count(nv) of them, written by triples_cube_table().
 // nv <= 1290 (32-bit element offsets).
@@ -170,6 +187,15 @@ void triples_cube_table(int nv, int* tri);
 int triples_energy(stream_t s, int nv, const void* K, const void* KU, bool k_f32, double eijk,
                    const double* ev, const TriplesTerms& t, const int* tri, double* scratch,
                    double* out);
+// Batched form: item b reads K + b*kstride (KU likewise), eijk_tab[b] and
+// tt_tab[b] (device tables) and writes out[2b], out[2b+1]; `scratch` holds at
+// least triples_energy_scratch_len(nv, nitems) doubles.  One launch (plus one
+// fixed-order reduction launch).
+int64_t triples_energy_scratch_len(int nv, int nitems);
+int triples_energy_batched(stream_t s, int nv, int nitems, const void* K, const void* KU,
+                           int64_t kstride, bool k_f32, const double* eijk_tab, const double* ev,
+                           const TriplesTerms* tt_tab, const int* tri, double* scratch,
+                           double* out);
 
 // Split-K GEMM (column-major, device pointers) whose partial products use a
 // fixed file-scope device array instead of allocated memory; m*n must not

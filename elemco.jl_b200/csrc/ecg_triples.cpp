@@ -26,6 +26,7 @@
 // kept in FP32.
 #include "ecg_triples.h"
 
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -103,95 +104,162 @@ struct TriplesOps {
   std::vector<dev::TcOperand> V1s, V2s, Ons;
 };
 
-// K^{ijk} = P[W] for amplitudes T (FP64) / Sp (mixed), into K (FP64 / FP32).
-void build_K(Ctx& c, const TriplesOps& ops, const double* T, const SplitAmps* Sp, void* K, int i,
-             int j, int k) {
+// One occupied triplet of the sweep: indices, weight (cc_triples.jl:62-72) and
+// the denominator shift e_i + e_j + e_k.
+struct Trip {
+  int i, j, k;
+  double f, eijk;
+};
+
+// Host-built tables of one amplitude tensor's K builds for the whole sweep,
+// uploaded once: FP64 offset tables [9 GEMMs][triplet][A, B, C, A1, B1] or
+// tensor-core descriptor tables [6 GEMMs][triplet][maps].  The C offset is the
+// triplet's slot in its batch.
+struct KTables {
+  std::vector<int64_t> ptab;
+  std::vector<unsigned char> mtab;
+  int64_t* ptab_d = nullptr;
+  unsigned char* mtab_d = nullptr;
+};
+
+constexpr int kGemmsFP64 = 9, kGemmsMixed = 6;
+
+void fill_tables(Ctx& c, const TriplesOps& ops, const SplitAmps* Sp, const std::vector<Trip>& tr,
+                 int NB, int64_t kstride, KTables& kt) {
   const int64_t o = c.no, v = c.nv, v2 = v * v, v3 = v2 * v, o2 = o * o;
+  const int64_t nt = (int64_t)tr.size();
+  auto on = [&](int y, int z) { return o * y + o2 * v * z; };
+  if (!ops.mixed) {
+    kt.ptab.assign(kGemmsFP64 * nt * 5, 0);
+    for (int64_t t = 0; t < nt; ++t) {
+      const int i = tr[t].i, j = tr[t].j, k = tr[t].k;
+      const int64_t offC = (t % NB) * kstride;
+      PermW P[6];
+      perm_table(i, j, k, v, P);
+      auto put = [&](int q, int64_t a, int64_t b, int64_t a1, int64_t b1) {
+        int64_t* e = kt.ptab.data() + (q * nt + t) * 5;
+        e[0] = a; e[1] = b; e[2] = offC; e[3] = a1; e[4] = b1;
+      };
+      for (int q = 0; q < 6; ++q) put(q, v2 * (P[q].x + o * P[q].y), v3 * P[q].z, 0, 0);
+      put(6, v2 * i, on(j, k), v2 * o * j, on(i, k));
+      put(7, on(k, j), v2 * i, on(i, j), v2 * o * k);
+      put(8, v2 * o * k, on(j, i), v2 * j, on(k, i));
+    }
+    return;
+  }
+  const size_t mb = dev::tc_maps_bytes();
+  kt.mtab.assign(kGemmsMixed * nt * mb, 0);
+  auto op = [&](int y, int z) { return &ops.Ons[y + o * z]; };
+  for (int64_t t = 0; t < nt; ++t) {
+    const int i = tr[t].i, j = tr[t].j, k = tr[t].k;
+    PermW P[6];
+    perm_table(i, j, k, v, P);
+    auto put = [&](int q, const dev::TcOperand* a0, const dev::TcOperand* a1,
+                   const dev::TcOperand* b0, const dev::TcOperand* b1) {
+      check(dev::tc_maps_fill(a0, b0, a1, b1, kt.mtab.data() + (q * nt + t) * mb), "maps");
+    };
+    const int pairs[3][2] = {{0, 2}, {1, 4}, {3, 5}};
+    for (int q = 0; q < 3; ++q) {
+      const PermW& p0 = P[pairs[q][0]];
+      const PermW& p1 = P[pairs[q][1]];
+      const dev::TcOperand* T0 = &Sp->pair[p0.x + o * p0.y];
+      const dev::TcOperand* T1 = &Sp->pair[p1.x + o * p1.y];
+      const dev::TcOperand* V0 = p0.l2 ? &ops.V2s[p0.z] : &ops.V1s[p0.z];
+      const dev::TcOperand* V1 = p1.l2 ? &ops.V2s[p1.z] : &ops.V1s[p1.z];
+      if (p0.scm == 1) put(q, T0, T1, V0, V1);
+      else put(q, V0, V1, T0, T1);
+    }
+    put(3, &Sp->G[i], &Sp->C[j], op(j, k), op(i, k));
+    put(4, &Sp->G[i], &Sp->C[k], op(k, j), op(i, j));
+    put(5, op(j, i), op(k, i), &Sp->C[k], &Sp->G[j]);
+  }
+}
+
+void upload_tables(Ctx& c, KTables& kt) {
   dev::stream_t s = c.st;
-  // vvvo terms: the six W GEMMs pair into three that write the same K
-  // positions (perm_table: ijk+ikj, jik+jki, kji+kij); on the tensor cores
-  // each pair is one GEMM with a two-segment K of 2v (one K pass instead of
-  // two).
+  if (!kt.ptab.empty()) {
+    kt.ptab_d = reinterpret_cast<int64_t*>(c.alloc((int64_t)kt.ptab.size(), "(T) offset table"));
+    check(dev::h2d(kt.ptab_d, kt.ptab.data(), kt.ptab.size() * 8, s), "h2d");
+  }
+  if (!kt.mtab.empty()) {
+    kt.mtab_d = reinterpret_cast<unsigned char*>(
+        c.alloc((int64_t)((kt.mtab.size() + 7) / 8), "(T) descriptor table"));
+    check(dev::h2d(kt.mtab_d, kt.mtab.data(), kt.mtab.size(), s), "h2d");
+  }
+}
+
+// K^{ijk} = P[W] for triplets t0 .. t0+nb-1 into K slots 0 .. nb-1 (FP64 or
+// FP32), one launch per GEMM kind.
+void build_K_batch(Ctx& c, const TriplesOps& ops, const double* T, const SplitAmps* Sp,
+                   const KTables& kt, int64_t nt, int64_t t0, int nb, void* K, int64_t kstride) {
+  const int64_t o = c.no, v = c.nv, v2 = v * v, o2 = o * o;
+  dev::stream_t s = c.st;
   PermW P[6];
-  perm_table(i, j, k, v, P);
+  perm_table(0, 0, 0, v, P);  // output maps and layouts do not depend on i, j, k
+  if (!ops.mixed) {
+    auto tab = [&](int q) { return kt.ptab_d + (q * nt + t0) * 5; };
+    for (int q = 0; q < 6; ++q) {
+      dev::Gemm g;
+      g.m = v; g.n = v2; g.k = v; g.batch = nb; g.alpha = 1.0; g.beta = q ? 1.0 : 0.0;
+      g.A = T; g.sam = 1; g.sak = v;
+      g.B = P[q].l2 ? ops.V2 : ops.V1; g.sbk = v2; g.sbn = 1;
+      g.C = (double*)K; g.scm = P[q].scm; g.scn = P[q].scn; g.dn = P[q].dn; g.scn2 = P[q].scn2;
+      g.ptab = tab(q);
+      check(dev::gemm_strided(s, g), "W vvvo");
+    }
+    dev::Gemm g;
+    g.k = 2 * o; g.kseg = o; g.alpha = -1.0; g.beta = 1.0; g.C = (double*)K; g.batch = nb;
+    // (1) rows (a,b), columns c
+    g.m = v2; g.n = v; g.A = T; g.sam = 1; g.sak = v2 * o; g.A1 = T; g.sak1 = v2;
+    g.B = ops.On; g.sbk = 1; g.sbn = o2; g.B1 = ops.On; g.sbk1 = 1;
+    g.scm = 1; g.scn = v2; g.dn = 0; g.scn2 = 0; g.ptab = tab(6);
+    check(dev::gemm_strided(s, g), "W ovoo 1");
+    // (2) rows b, columns (a,c)
+    g.m = v; g.n = v2; g.A = ops.On; g.sam = o2; g.sak = 1; g.A1 = ops.On; g.sak1 = 1;
+    g.B = T; g.sbk = v2 * o; g.sbn = 1; g.B1 = T; g.sbk1 = v2;
+    g.scm = v; g.scn = 1; g.dn = v; g.scn2 = v2; g.ptab = tab(7);
+    check(dev::gemm_strided(s, g), "W ovoo 2");
+    // (3) rows (b,c), columns a
+    g.m = v2; g.n = v; g.A = T; g.sam = 1; g.sak = v2; g.A1 = T; g.sak1 = v2 * o;
+    g.B = ops.On; g.sbk = 1; g.sbn = o2; g.B1 = ops.On; g.sbk1 = 1;
+    g.scm = v; g.scn = 1; g.dn = 0; g.scn2 = 0; g.ptab = tab(8);
+    check(dev::gemm_strided(s, g), "W ovoo 3");
+    return;
+  }
+  const size_t mb = dev::tc_maps_bytes();
+  auto tab = [&](int q) { return kt.mtab_d + (q * nt + t0) * mb; };
+  // shape representatives (every triplet's operands have the same shapes)
+  const dev::TcOperand* Tp = &Sp->pair[0];
+  const dev::TcOperand* Vp = &ops.V1s[0];
+  const dev::TcOperand* Op = &ops.Ons[0];
+  const dev::TcOperand* Gp = &Sp->G[0];
   const int pairs[3][2] = {{0, 2}, {1, 4}, {3, 5}};
   for (int q = 0; q < 3; ++q) {
     const PermW& p0 = P[pairs[q][0]];
-    const PermW& p1 = P[pairs[q][1]];
-    if (ops.mixed) {
-      dev::TcGemm g;
-      g.alpha = 1.0; g.beta = q ? 1.0 : 0.0; g.C = K; g.f32 = true;
-      auto Ta = [&](const PermW& p) { return &Sp->pair[p.x + o * p.y]; };
-      auto Vb = [&](const PermW& p) { return p.l2 ? &ops.V2s[p.z] : &ops.V1s[p.z]; };
-      if (p0.scm == 1) {  // rows a'
-        g.m = v; g.n = v2;
-        g.A[0] = Ta(p0); g.A[1] = Ta(p1); g.B[0] = Vb(p0); g.B[1] = Vb(p1);
-        g.scm = 1; g.scn = p0.scn; g.dn = p0.dn; g.scn2 = p0.scn2;
-      } else {            // rows (b',c'), columns a'
-        g.m = v2; g.n = v;
-        g.A[0] = Vb(p0); g.A[1] = Vb(p1); g.B[0] = Ta(p0); g.B[1] = Ta(p1);
-        g.scm = p0.scn; g.dm = p0.dn; g.scm2 = p0.scn2; g.scn = p0.scm;
-      }
-      check(dev::tc_gemm(s, g), "W vvvo");
-    } else {
-      // FP64 is bound by the MMA pipe, not by the K traffic: two plain GEMMs
-      // keep the lean single-segment loader
-      for (const PermW* p : {&p0, &p1}) {
-        dev::Gemm g;
-        g.m = v; g.n = v2; g.k = v; g.alpha = 1.0; g.beta = (q || p == &p1) ? 1.0 : 0.0;
-        g.A = T + v2 * (p->x + o * p->y); g.sam = 1; g.sak = v;
-        g.B = (p->l2 ? ops.V2 : ops.V1) + v3 * p->z; g.sbk = v2; g.sbn = 1;
-        g.C = (double*)K; g.scm = p->scm; g.scn = p->scn; g.dn = p->dn; g.scn2 = p->scn2;
-        check(dev::gemm_strided(s, g), "W vvvo");
-      }
-    }
-  }
-  // ovoo terms, pairs of permutations sharing one output index order:
-  //  (1) K[a,b,c] -= sum_l T2[a,b,i,l] On[l,j,c,k] + T2[a,b,l,j] On[l,i,c,k]
-  //  (2) K[a,b,c] -= sum_l T2[a,c,i,l] On[l,k,b,j] + T2[a,c,l,k] On[l,i,b,j]
-  //  (3) K[a,b,c] -= sum_l T2[b,c,l,k] On[l,j,a,i] + T2[b,c,j,l] On[l,k,a,i]
-  auto on = [&](int y, int z) { return ops.On + o * y + o2 * v * z; };
-  if (ops.mixed) {  // rows along the unit stride of K
-    auto op = [&](int y, int z) { return &ops.Ons[y + o * z]; };
     dev::TcGemm g;
-    g.alpha = -1.0; g.beta = 1.0; g.C = K; g.f32 = true;
-    // (1) rows (a,b), columns c
-    g.m = v2; g.n = v;
-    g.A[0] = &Sp->G[i]; g.A[1] = &Sp->C[j]; g.B[0] = op(j, k); g.B[1] = op(i, k);
-    g.scm = 1; g.scn = v2;
-    check(dev::tc_gemm(s, g), "W ovoo 1");
-    // (2) rows (a,c), columns b
-    g.m = v2; g.n = v;
-    g.A[0] = &Sp->G[i]; g.A[1] = &Sp->C[k]; g.B[0] = op(k, j); g.B[1] = op(i, j);
-    g.scm = 1; g.dm = v; g.scm2 = v2; g.scn = v;
-    check(dev::tc_gemm(s, g), "W ovoo 2");
-    // (3) rows a, columns (b,c)
-    g.m = v; g.n = v2;
-    g.A[0] = op(j, i); g.A[1] = op(k, i); g.B[0] = &Sp->C[k]; g.B[1] = &Sp->G[j];
-    g.scm = 1; g.dm = 0; g.scm2 = 0; g.scn = v;
-    check(dev::tc_gemm(s, g), "W ovoo 3");
-    return;
+    g.alpha = 1.0; g.beta = q ? 1.0 : 0.0; g.C = K; g.f32 = true;
+    if (p0.scm == 1) {  // rows a'
+      g.m = v; g.n = v2; g.A[0] = g.A[1] = Tp; g.B[0] = g.B[1] = Vp;
+      g.scm = 1; g.scn = p0.scn; g.dn = p0.dn; g.scn2 = p0.scn2;
+    } else {            // rows (b',c'), columns a'
+      g.m = v2; g.n = v; g.A[0] = g.A[1] = Vp; g.B[0] = g.B[1] = Tp;
+      g.scm = p0.scn; g.dm = p0.dn; g.scm2 = p0.scn2; g.scn = p0.scm;
+    }
+    check(dev::tc_gemm_batched(s, g, nb, tab(q), kstride), "W vvvo");
   }
-  dev::Gemm g;
-  g.k = 2 * o; g.kseg = o; g.alpha = -1.0; g.beta = 1.0; g.C = (double*)K;
+  dev::TcGemm g;
+  g.alpha = -1.0; g.beta = 1.0; g.C = K; g.f32 = true;
   // (1) rows (a,b), columns c
-  g.m = v2; g.n = v;
-  g.A = T + v2 * i; g.sam = 1; g.sak = v2 * o; g.A1 = T + v2 * o * j; g.sak1 = v2;
-  g.B = on(j, k); g.sbk = 1; g.sbn = o2; g.B1 = on(i, k); g.sbk1 = 1;
-  g.scm = 1; g.scn = v2; g.dn = 0; g.scn2 = 0;
-  check(dev::gemm_strided(s, g), "W ovoo 1");
-  // (2) rows b, columns (a,c)
-  g.m = v; g.n = v2;
-  g.A = on(k, j); g.sam = o2; g.sak = 1; g.A1 = on(i, j); g.sak1 = 1;
-  g.B = T + v2 * i; g.sbk = v2 * o; g.sbn = 1; g.B1 = T + v2 * o * k; g.sbk1 = v2;
-  g.scm = v; g.scn = 1; g.dn = v; g.scn2 = v2;
-  check(dev::gemm_strided(s, g), "W ovoo 2");
-  // (3) rows (b,c), columns a
-  g.m = v2; g.n = v;
-  g.A = T + v2 * o * k; g.sam = 1; g.sak = v2; g.A1 = T + v2 * j; g.sak1 = v2 * o;
-  g.B = on(j, i); g.sbk = 1; g.sbn = o2; g.B1 = on(k, i); g.sbk1 = 1;
-  g.scm = v; g.scn = 1; g.dn = 0; g.scn2 = 0;
-  check(dev::gemm_strided(s, g), "W ovoo 3");
+  g.m = v2; g.n = v; g.A[0] = g.A[1] = Gp; g.B[0] = g.B[1] = Op;
+  g.scm = 1; g.scn = v2;
+  check(dev::tc_gemm_batched(s, g, nb, tab(3), kstride), "W ovoo 1");
+  // (2) rows (a,c), columns b
+  g.scm = 1; g.dm = v; g.scm2 = v2; g.scn = v;
+  check(dev::tc_gemm_batched(s, g, nb, tab(4), kstride), "W ovoo 2");
+  // (3) rows a, columns (b,c)
+  g.m = v; g.n = v2; g.A[0] = g.A[1] = Op; g.B[0] = g.B[1] = Gp;
+  g.scm = 1; g.dm = 0; g.scm2 = 0; g.scn = v;
+  check(dev::tc_gemm_batched(s, g, nb, tab(5), kstride), "W ovoo 3");
 }
 
 }  // namespace
@@ -263,12 +331,8 @@ void pert_triples(Ctx& c, const double* U1h, const double* U2h, double* et, doub
     c.release_to(mark);
   }
 
-  void* K = mixed ? (void*)c.alloc((v3 + 1) / 2, "(T) K") : (void*)c.alloc(v3, "(T) K");
-  void* KU = nullptr;
   double* U2c = nullptr;
   if (lam) {
-    KU = mixed ? (void*)c.alloc((v3 + 1) / 2, "(T) K(Lambda)")
-               : (void*)c.alloc(v3, "(T) K(Lambda)");
     double* U2 = c.alloc(c.n2(), "(T) U2");
     U2c = c.alloc(c.n2(), "(T) U2 covariant");
     check(dev::h2d(U2, U2h, c.n2() * 8, s), "h2d U2");
@@ -282,7 +346,37 @@ void pert_triples(Ctx& c, const double* U1h, const double* U2h, double* et, doub
     if (lam) split_amps(c, U2c, SU);
   }
 
-  // singles / Fock vectors: g = T1 (or U1/2), f[a,i] = fock[i, o+a]
+  // the sweep: triplet order and weights of cc_triples.jl:62-72
+  const double* eps = c.fock_host.data();
+  std::vector<Trip> tr;
+  for (int k = 0; k < o; ++k)
+    for (int j = 0; j <= k; ++j)
+      for (int i = 0; i <= j; ++i) {
+        if (i == j && j == k) continue;
+        const double f = (i == j) ? 1.0 : (j == k ? 1.0 : 2.0);
+        tr.push_back({i, j, k, f, eps[i + i * n] + eps[j + j * n] + eps[k + k * n]});
+      }
+  const int64_t nt = (int64_t)tr.size();
+  if (nt == 0) {
+    *et = *etb = 0.0;
+    return;
+  }
+  // batches of NB triplets, one K slot each, within a 4 GiB budget
+  const int64_t esz = mixed ? 4 : 8;
+  const int64_t kstride = (v3 + 31) / 32 * 32;
+  const int64_t per = kstride * esz * (lam ? 2 : 1);
+  const int NB = (int)std::max<int64_t>(1, std::min<int64_t>({256, nt, ((int64_t)4 << 30) / per}));
+  void* K = c.alloc((NB * kstride * esz + 7) / 8, "(T) K slots");
+  void* KU = lam ? (void*)c.alloc((NB * kstride * esz + 7) / 8, "(T) K(Lambda) slots") : nullptr;
+  KTables KT, KUt;
+  fill_tables(c, ops, &ST, tr, NB, kstride, KT);
+  upload_tables(c, KT);
+  if (lam) {
+    fill_tables(c, ops, &SU, tr, NB, kstride, KUt);
+    upload_tables(c, KUt);
+  }
+
+  // energy terms per triplet: g = T1 (or U1/2), f[a,i] = fock[i, o+a], <ij|ab>, T2 (or U2c)
   std::vector<double> gh(v * o), fh(v * o);
   {
     std::vector<double> T1h(v * o);
@@ -299,51 +393,57 @@ void pert_triples(Ctx& c, const double* U1h, const double* U2h, double* et, doub
   double* gf = c.alloc(2 * v * o, "(T) singles/Fock vectors");
   check(dev::h2d(gf, gh.data(), v * o * 8, s), "h2d");
   check(dev::h2d(gf + v * o, fh.data(), v * o * 8, s), "h2d");
+  const double* Nsrc = lam ? U2c : c.T2();
+  auto M = [&](int x, int y) { return c.Kvvoo + v2 * (x + o * y); };
+  auto N = [&](int x, int y) { return Nsrc + v2 * (x + o * y); };
+  std::vector<dev::TriplesTerms> terms(nt);
+  std::vector<double> eijk(nt);
+  for (int64_t t = 0; t < nt; ++t) {
+    const int i = tr[t].i, j = tr[t].j, k = tr[t].k;
+    dev::TriplesTerms& tt = terms[t];
+    tt.g[0] = gf + v * i; tt.g[1] = gf + v * j; tt.g[2] = gf + v * k;
+    tt.f[0] = gf + v * (o + i); tt.f[1] = gf + v * (o + j); tt.f[2] = gf + v * (o + k);
+    tt.M[0] = M(j, k); tt.M[1] = M(i, k); tt.M[2] = M(i, j);
+    tt.N[0] = N(j, k); tt.N[1] = N(i, k); tt.N[2] = N(i, j);
+    eijk[t] = tr[t].eijk;
+  }
+  auto* terms_d = reinterpret_cast<dev::TriplesTerms*>(
+      c.alloc((int64_t)((nt * sizeof(dev::TriplesTerms) + 7) / 8), "(T) energy terms"));
+  double* eijk_d = c.alloc(nt, "(T) denominators");
+  check(dev::h2d(terms_d, terms.data(), nt * sizeof(dev::TriplesTerms), s), "h2d");
+  check(dev::h2d(eijk_d, eijk.data(), nt * 8, s), "h2d");
   const int64_t ncube = dev::triples_cube_count((int)v);
   std::vector<int> trih(3 * ncube);
   dev::triples_cube_table((int)v, trih.data());
   int* tri = reinterpret_cast<int*>(c.alloc((3 * ncube + 1) / 2, "(T) cube table"));
   check(dev::h2d(tri, trih.data(), 3 * ncube * sizeof(int), s), "h2d");
+  double* part = c.alloc(dev::triples_energy_scratch_len((int)v, NB), "(T) partial sums");
+  double* Et = c.alloc(2 * nt, "(T) energies");
 
-  int64_t ntrip = 0;
-  for (int64_t kk = 0; kk < o; ++kk)
-    for (int64_t jj = 0; jj <= kk; ++jj)
-      for (int64_t ii = 0; ii <= jj; ++ii)
-        if (!(ii == jj && jj == kk)) ++ntrip;
-  double* Et = c.alloc(std::max<int64_t>(2 * ntrip, 2), "(T) energies");
-  std::vector<double> fac;
-  fac.reserve(ntrip);
-  const double* eps = c.fock_host.data();
-  const double* ev = c.eps + o;
-  const double* Nsrc = lam ? U2c : c.T2();
-  auto M = [&](int x, int y) { return c.Kvvoo + v2 * (x + o * y); };
-  auto N = [&](int x, int y) { return Nsrc + v2 * (x + o * y); };
-  int64_t t = 0;
-  for (int k = 0; k < o; ++k)
-    for (int j = 0; j <= k; ++j) {
-      const double prefac = (j == k) ? 1.0 : 2.0;
-      for (int i = 0; i <= j; ++i) {
-        double f = prefac;
-        if (i == j) {
-          if (j == k) continue;
-          f = 1.0;
-        }
-        const double eijk = eps[i + i * n] + eps[j + j * n] + eps[k + k * n];
-        build_K(c, ops, c.T2(), &ST, K, i, j, k);
-        if (lam) build_K(c, ops, U2c, &SU, KU, i, j, k);
-        dev::TriplesTerms tt;
-        tt.g[0] = gf + v * i; tt.g[1] = gf + v * j; tt.g[2] = gf + v * k;
-        tt.f[0] = gf + v * (o + i); tt.f[1] = gf + v * (o + j); tt.f[2] = gf + v * (o + k);
-        tt.M[0] = M(j, k); tt.M[1] = M(i, k); tt.M[2] = M(i, j);
-        tt.N[0] = N(j, k); tt.N[1] = N(i, k); tt.N[2] = N(i, j);
-        check(dev::triples_energy(s, (int)v, K, KU, mixed, eijk, ev, tt, tri, c.red, Et + 2 * t),
-              "triples energy");
-        fac.push_back(f);
-        ++t;
-      }
+  // batch loop: the first batch runs directly (first-use set-up of the
+  // kernels), the others are recorded as one CUDA graph and run once
+  const int64_t nbatch = (nt + NB - 1) / NB;
+  try {
+    for (int64_t bi = 0; bi < nbatch; ++bi) {
+      if (bi == 1) check(dev::graph_capture_begin(s), "graph capture");
+      const int64_t t0 = bi * NB;
+      const int nb = (int)std::min<int64_t>(NB, nt - t0);
+      build_K_batch(c, ops, c.T2(), &ST, KT, nt, t0, nb, K, kstride);
+      if (lam) build_K_batch(c, ops, U2c, &SU, KUt, nt, t0, nb, KU, kstride);
+      check(dev::triples_energy_batched(s, (int)v, nb, K, KU, kstride, mixed, eijk_d + t0,
+                                        c.eps + o, terms_d + t0, tri, part, Et + 2 * t0),
+            "triples energy");
     }
-  std::vector<double> Eh(2 * ntrip);
-  if (ntrip) check(dev::d2h(Eh.data(), Et, 2 * ntrip * 8, s), "d2h");
+    if (nbatch > 1) {
+      int64_t nodes = 0;
+      check(dev::graph_capture_run(s, &nodes), "(T) graph");
+    }
+  } catch (...) {
+    dev::graph_capture_abort(s);
+    throw;
+  }
+  std::vector<double> Eh(2 * nt);
+  check(dev::d2h(Eh.data(), Et, 2 * nt * 8, s), "d2h");
   check(dev::sync(s), "sync");
   if (mixed) {
     int tc = 0;
@@ -352,9 +452,9 @@ void pert_triples(Ctx& c, const double* U1h, const double* U2h, double* et, doub
   }
   // sum K X, and the singles / Fock term sum X Y (cc_triples.jl:143-156 / :286-294)
   double Enb3 = 0.0, Esf = 0.0;
-  for (int64_t q = 0; q < ntrip; ++q) {
-    Enb3 += fac[q] * Eh[2 * q];
-    Esf += fac[q] * Eh[2 * q + 1];
+  for (int64_t q = 0; q < nt; ++q) {
+    Enb3 += tr[q].f * Eh[2 * q];
+    Esf += tr[q].f * Eh[2 * q + 1];
   }
   const double En3 = Enb3 + Esf;
   if (!std::isfinite(En3)) throw Error(ECG_ERR_NONFINITE, "non-finite (T) energy");
