@@ -141,11 +141,32 @@ constexpr int EPI_WARPS = 8;  // two per TMEM lane quarter, 64 columns each
 constexpr int THREADS_TC = 32 * (2 + EPI_WARPS);
 constexpr uint32_t TMEM_COLS_P = 2 * TN;
 
-// TMA descriptors of the two K segments: k-blocks [0, kb_seg0) read (a0, b0),
-// the rest read (a1, b1) from their own k = 0.
+// TMA descriptors of up to TC_MAX_SEG K segments, each read from its own k = 0.
 struct TcMaps {
-  CUtensorMap a0, b0, a1, b1;
+  CUtensorMap a[TC_MAX_SEG], b[TC_MAX_SEG];
 };
+
+// K layout of the segments: segment s covers the k-blocks [kb_end[s-1],
+// kb_end[s]) (kb_end nondecreasing, unused trailing segments repeat the total);
+// its last k-block issues kk_last[s] of the TK/16 MMA steps, the rest of that
+// block being zero padding.
+struct TcSegs {
+  int kb_end[TC_MAX_SEG];
+  int kk_last[TC_MAX_SEG];
+};
+
+// Segment of global k-block kg: index, first k-block, end, MMA steps of its
+// last k-block (selects only, no indexed parameter reads).
+struct SegPos {
+  int s, start, end, kk_last;
+};
+__device__ __forceinline__ SegPos seg_of(const TcSegs& sg, int kg) {
+  SegPos p{0, 0, sg.kb_end[0], sg.kk_last[0]};
+#pragma unroll
+  for (int t = 1; t < TC_MAX_SEG; ++t)
+    if (kg >= sg.kb_end[t - 1]) p = SegPos{t, sg.kb_end[t - 1], sg.kb_end[t], sg.kk_last[t]};
+  return p;
+}
 
 // Output element (m, n) lives at C[rowoff(m) + coloff(n)] (FP64, or FP32 when
 // f32) with rowoff(m) = (m % dm)*scm + (m / dm)*scm2 (dm = 0: m*scm) and
@@ -224,7 +245,8 @@ __device__ __forceinline__ void prefetch_cols(const CT* C, int64_t rowoff, int64
 template <int NSL>
 __global__ void __launch_bounds__(THREADS_TC, 1)
     mgemm_bf16_kernel(const __grid_constant__ TcMaps maps, TcOut out, int64_t M, int64_t N,
-                      double alpha, double beta, int kb_seg0, int kb_per_split, int kblocks_total,
+                      double alpha, double beta, const TcSegs segs, int kb_per_split,
+                      int kblocks_total,
                       int64_t split_stride, int mtiles, int ntiles, int nsplit,
                       const TcMaps* __restrict__ mtab) {
   using Cfg = TcCfg<NSL>;
@@ -303,10 +325,10 @@ __global__ void __launch_bounds__(THREADS_TC, 1)
           }
           uint8_t* st = tiles + s * STAGE_BYTES;
           const int kg = kb0 + kb;
-          const bool s1 = kg >= kb_seg0;
-          const CUtensorMap* ma = s1 ? &mp->a1 : &mp->a0;
-          const CUtensorMap* mb = s1 ? &mp->b1 : &mp->b0;
-          const int kx = (s1 ? kg - kb_seg0 : kg) * TK;
+          const SegPos sp = seg_of(segs, kg);
+          const CUtensorMap* ma = &mp->a[sp.s];
+          const CUtensorMap* mb = &mp->b[sp.s];
+          const int kx = (kg - sp.start) * TK;
           mbar_expect_tx(&full[s], STAGE_BYTES);
           for (int t = 0; t < NSL; ++t) {
             tma_load_3d(st + t * TILE_BYTES_A, ma, &full[s], kx, mt * TM, t);
@@ -327,7 +349,7 @@ __global__ void __launch_bounds__(THREADS_TC, 1)
            it += gridDim.x, ++lt) {
         int mt, nt, z;
         item_coords(it, mt, nt, z);
-        const int nk = item_kblocks(z);
+        const int nk = item_kblocks(z), kb0 = mtab ? 0 : z * kb_per_split;
         const int acc = (int)(lt & 1);
         const int64_t ua = lt >> 1;
         if (ua > 0 && !mbar_wait(&tempty[acc], (uint32_t)((ua - 1) & 1))) {
@@ -350,14 +372,17 @@ __global__ void __launch_bounds__(THREADS_TC, 1)
           const uint8_t* st = tiles + s * STAGE_BYTES;
           const uint8_t* As = st;
           const uint8_t* Bs = st + NSL * TILE_BYTES_A;
+          const SegPos sp = seg_of(segs, kb0 + kb);
+          const int nkk = (kb0 + kb == sp.end - 1) ? sp.kk_last : TK / 16;
 #pragma unroll
           for (int p = 0; p < Cfg::NPAIR; ++p) {
             const uint64_t da = umma_desc(As + pair_a(p) * TILE_BYTES_A);
             const uint64_t db = umma_desc(Bs + pair_b(p) * TILE_BYTES_B);
 #pragma unroll
             for (int kk = 0; kk < TK / 16; ++kk)
-              umma(dcol, da + (uint64_t)(kk * 2), db + (uint64_t)(kk * 2),
-                   (kb > 0 || p > 0 || kk > 0) ? 1u : 0u);
+              if (kk < nkk)
+                umma(dcol, da + (uint64_t)(kk * 2), db + (uint64_t)(kk * 2),
+                     (kb > 0 || p > 0 || kk > 0) ? 1u : 0u);
           }
           umma_commit(&empty[s]);
         }
@@ -528,6 +553,43 @@ int make_map(EncodeFn enc, CUtensorMap* m, const void* base, int64_t rows, int64
 int64_t pad_rows(int64_t r) { return (r + TM - 1) / TM * TM; }
 int64_t pad_k(int64_t k) { return (k + TK - 1) / TK * TK; }
 
+// Segment k-block layout of nseg segments of K depths k[s] (padded to TK).
+TcSegs make_segs(int nseg, const int64_t* k) {
+  TcSegs sg;
+  int end = 0;
+  for (int t = 0; t < TC_MAX_SEG; ++t) {
+    if (t < nseg) {
+      const int64_t kp = pad_k(k[t]);
+      end += (int)(kp / TK);
+      sg.kk_last[t] = (int)((k[t] - (kp - TK) + 15) / 16);
+    } else {
+      sg.kk_last[t] = TK / 16;
+    }
+    sg.kb_end[t] = end;
+  }
+  return sg;
+}
+
+// Checks the segments of g (A[s]/B[s] until the first null A[s]) and returns
+// their number, or 0 if they do not form a valid GEMM of g's shape.
+int gemm_segments(const TcGemm& g, int64_t* k) {
+  int ns = 0;
+  const TcOperand* A0 = g.A[0];
+  const TcOperand* B0 = g.B[0];
+  if (!A0 || !B0) return 0;
+  for (; ns < TC_MAX_SEG && g.A[ns]; ++ns) {
+    const TcOperand* A = g.A[ns];
+    const TcOperand* B = g.B[ns];
+    if (!B || A->k != B->k || A->k <= 0 || A->rows < g.m || B->rows < g.n ||
+        A->slices != A0->slices || B->slices != A0->slices)
+      return 0;
+    k[ns] = A->k;
+  }
+  for (int t = ns; t < TC_MAX_SEG; ++t)
+    if (g.B[t]) return 0;
+  return ns;
+}
+
 void launch_split(cudaStream_t st, const double* src, int64_t R, int64_t K, int64_t sr,
                   int64_t sk, int64_t Rp, int64_t Kp, int nsl, __nv_bfloat16* dst) {
   const int64_t tiles = ((Rp + 31) / 32) * ((Kp + 31) / 32);
@@ -549,8 +611,9 @@ int split_count(int64_t tiles, int kbt) {
 // Launch over pre-split operands; S > 1 splits the combined k-blocks into S
 // slices that write FP64 partial products P[z][n][m] (column-major m x n).
 template <int NSL>
-int launch_tc(cudaStream_t st, const TcMaps& maps, int kb0, int kbt, int64_t m, int64_t n,
-              int64_t mp, int64_t np, double alpha, double beta, const TcOut& out, int S) {
+int launch_tc(cudaStream_t st, const TcMaps& maps, const TcSegs& segs, int kbt, int64_t m,
+              int64_t n, int64_t mp, int64_t np, double alpha, double beta, const TcOut& out,
+              int S) {
   using Cfg = TcCfg<NSL>;
   static bool attr = false;
   if (!attr) {
@@ -565,7 +628,7 @@ int launch_tc(cudaStream_t st, const TcMaps& maps, int kb0, int kbt, int64_t m, 
   const unsigned grid = (unsigned)(items < 148 ? items : 148);
   if (S == 1) {
     mgemm_bf16_kernel<NSL><<<grid, THREADS_TC, Cfg::SMEM_BYTES, st>>>(
-        maps, out, m, n, alpha, beta, kb0, kps, kbt, 0, mt, nt, 1, nullptr);
+        maps, out, m, n, alpha, beta, segs, kps, kbt, 0, mt, nt, 1, nullptr);
     note_launches(1);
     return (int)cudaGetLastError();
   }
@@ -574,7 +637,7 @@ int launch_tc(cudaStream_t st, const TcMaps& maps, int kb0, int kbt, int64_t m, 
   if (!P) return (int)cudaErrorMemoryAllocation;
   TcOut po{P, 1, m, 0, 0, 0, 0, 0};
   mgemm_bf16_kernel<NSL><<<grid, THREADS_TC, Cfg::SMEM_BYTES, st>>>(
-      maps, po, m, n, 1.0, 0.0, kb0, kps, kbt, m * n, mt, nt, S, nullptr);
+      maps, po, m, n, 1.0, 0.0, segs, kps, kbt, m * n, mt, nt, S, nullptr);
   note_launches(1);
   int e = (int)cudaGetLastError();
   if (e) return e;
@@ -627,56 +690,48 @@ int tc_view(const TcOperand& parent, int64_t row0, int64_t rows, TcOperand* out)
 
 int tc_gemm(stream_t s, const TcGemm& g) {
   if (g.m <= 0 || g.n <= 0) return 0;
-  const TcOperand* A0 = g.A[0];
-  const TcOperand* B0 = g.B[0];
-  if (!A0 || !B0 || A0->k != B0->k || A0->rows < g.m || B0->rows < g.n ||
-      A0->slices != B0->slices)
-    return (int)cudaErrorInvalidValue;
-  const TcOperand* A1 = g.A[1];
-  const TcOperand* B1 = g.B[1];
-  if ((A1 == nullptr) != (B1 == nullptr)) return (int)cudaErrorInvalidValue;
-  if (A1 && (A1->k != B1->k || A1->rows < g.m || B1->rows < g.n || A1->rows_p != A0->rows_p ||
-             B1->rows_p != B0->rows_p || A1->slices != A0->slices || B1->slices != A0->slices))
-    return (int)cudaErrorInvalidValue;
+  int64_t k[TC_MAX_SEG];
+  const int ns = gemm_segments(g, k);
+  if (ns == 0) return (int)cudaErrorInvalidValue;
   TcMaps maps;
-  std::memcpy(&maps.a0, A0->map, sizeof(CUtensorMap));
-  std::memcpy(&maps.b0, B0->map, sizeof(CUtensorMap));
-  std::memcpy(&maps.a1, (A1 ? A1 : A0)->map, sizeof(CUtensorMap));
-  std::memcpy(&maps.b1, (B1 ? B1 : B0)->map, sizeof(CUtensorMap));
-  const int kb0 = (int)(A0->k_p / TK);
-  const int kbt = kb0 + (A1 ? (int)(A1->k_p / TK) : 0);
+  for (int t = 0; t < TC_MAX_SEG; ++t) {
+    std::memcpy(&maps.a[t], g.A[t < ns ? t : 0]->map, sizeof(CUtensorMap));
+    std::memcpy(&maps.b[t], g.B[t < ns ? t : 0]->map, sizeof(CUtensorMap));
+  }
+  const TcSegs segs = make_segs(ns, k);
+  const int kbt = segs.kb_end[TC_MAX_SEG - 1];
   TcOut out{g.C, g.scm, g.scn, g.dn, g.scn2, g.dm, g.scm2, g.f32 ? 1 : 0};
   const int64_t mp = pad_rows(g.m), np = pad_rows(g.n);
   int S = 1;
   if (!g.f32 && g.dn == 0 && g.dm == 0) S = split_count(mp / TM * (np / TN), kbt);
-  if (A0->slices == 3)
-    return launch_tc<3>((cudaStream_t)s, maps, kb0, kbt, g.m, g.n, mp, np, g.alpha, g.beta, out,
+  if (g.A[0]->slices == 3)
+    return launch_tc<3>((cudaStream_t)s, maps, segs, kbt, g.m, g.n, mp, np, g.alpha, g.beta, out,
                         S);
-  return launch_tc<2>((cudaStream_t)s, maps, kb0, kbt, g.m, g.n, mp, np, g.alpha, g.beta, out, S);
+  return launch_tc<2>((cudaStream_t)s, maps, segs, kbt, g.m, g.n, mp, np, g.alpha, g.beta, out,
+                      S);
 }
 
 size_t tc_maps_bytes() { return sizeof(TcMaps); }
 
-int tc_maps_fill(const TcOperand* A0, const TcOperand* B0, const TcOperand* A1,
-                 const TcOperand* B1, void* dst) {
-  if (!A0 || !B0 || !dst || (A1 == nullptr) != (B1 == nullptr)) return (int)cudaErrorInvalidValue;
+int tc_maps_fill(int nseg, const TcOperand* const* A, const TcOperand* const* B, void* dst) {
+  if (nseg < 1 || nseg > TC_MAX_SEG || !A || !B || !dst) return (int)cudaErrorInvalidValue;
+  for (int t = 0; t < nseg; ++t)
+    if (!A[t] || !B[t]) return (int)cudaErrorInvalidValue;
   TcMaps* m = reinterpret_cast<TcMaps*>(dst);
-  std::memcpy(&m->a0, A0->map, sizeof(CUtensorMap));
-  std::memcpy(&m->b0, B0->map, sizeof(CUtensorMap));
-  std::memcpy(&m->a1, (A1 ? A1 : A0)->map, sizeof(CUtensorMap));
-  std::memcpy(&m->b1, (B1 ? B1 : B0)->map, sizeof(CUtensorMap));
+  for (int t = 0; t < TC_MAX_SEG; ++t) {
+    std::memcpy(&m->a[t], A[t < nseg ? t : 0]->map, sizeof(CUtensorMap));
+    std::memcpy(&m->b[t], B[t < nseg ? t : 0]->map, sizeof(CUtensorMap));
+  }
   return 0;
 }
 
 int tc_gemm_batched(stream_t s, const TcGemm& g, int batch, const void* mtab, int64_t c_stride) {
   if (g.m <= 0 || g.n <= 0 || batch <= 0) return 0;
-  const TcOperand* A0 = g.A[0];
-  const TcOperand* B0 = g.B[0];
-  if (!A0 || !B0 || !mtab || ((uintptr_t)mtab & 63) != 0 || A0->slices != B0->slices)
-    return (int)cudaErrorInvalidValue;
-  const TcOperand* A1 = g.A[1];
-  const int kb0 = (int)(A0->k_p / TK);
-  const int kbt = kb0 + (A1 ? (int)(A1->k_p / TK) : 0);
+  int64_t k[TC_MAX_SEG];
+  const int ns = gemm_segments(g, k);
+  if (ns == 0 || !mtab || ((uintptr_t)mtab & 63) != 0) return (int)cudaErrorInvalidValue;
+  const TcSegs segs = make_segs(ns, k);
+  const int kbt = segs.kb_end[TC_MAX_SEG - 1];
   const int64_t mp = pad_rows(g.m), np = pad_rows(g.n);
   const int mt = (int)(mp / TM), nt = (int)(np / TN);
   const int64_t items = (int64_t)mt * nt * batch;
@@ -685,7 +740,7 @@ int tc_gemm_batched(stream_t s, const TcGemm& g, int batch, const void* mtab, in
   TcMaps dummy;
   std::memset(&dummy, 0, sizeof(dummy));
   cudaStream_t st = (cudaStream_t)s;
-  if (A0->slices == 3) {
+  if (g.A[0]->slices == 3) {
     using Cfg = TcCfg<3>;
     static bool attr = false;
     if (!attr) {
@@ -694,7 +749,7 @@ int tc_gemm_batched(stream_t s, const TcGemm& g, int batch, const void* mtab, in
       attr = true;
     }
     mgemm_bf16_kernel<3><<<grid, THREADS_TC, Cfg::SMEM_BYTES, st>>>(
-        dummy, out, g.m, g.n, g.alpha, g.beta, kb0, kbt, kbt, c_stride, mt, nt, batch,
+        dummy, out, g.m, g.n, g.alpha, g.beta, segs, kbt, kbt, c_stride, mt, nt, batch,
         (const TcMaps*)mtab);
   } else {
     using Cfg = TcCfg<2>;
@@ -705,7 +760,7 @@ int tc_gemm_batched(stream_t s, const TcGemm& g, int batch, const void* mtab, in
       attr = true;
     }
     mgemm_bf16_kernel<2><<<grid, THREADS_TC, Cfg::SMEM_BYTES, st>>>(
-        dummy, out, g.m, g.n, g.alpha, g.beta, kb0, kbt, kbt, c_stride, mt, nt, batch,
+        dummy, out, g.m, g.n, g.alpha, g.beta, segs, kbt, kbt, c_stride, mt, nt, batch,
         (const TcMaps*)mtab);
   }
   note_launches(1);
@@ -734,14 +789,17 @@ int gemm_strided_mixed(stream_t s, const Gemm& q) {
   launch_split(st, q.A, m, k, q.sam, q.sak, mp, kp, NSL, As);  // A(m,k) = A[m sam + k sak]
   launch_split(st, q.B, n, k, q.sbn, q.sbk, np, kp, NSL, Bs);  // B(k,n) = B[k sbk + n sbn]
   TcMaps maps;
-  if ((e = make_map(enc, &maps.a0, As, mp, kp, NSL))) return e;
-  if ((e = make_map(enc, &maps.b0, Bs, np, kp, NSL))) return e;
-  maps.a1 = maps.a0;
-  maps.b1 = maps.b0;
+  if ((e = make_map(enc, &maps.a[0], As, mp, kp, NSL))) return e;
+  if ((e = make_map(enc, &maps.b[0], Bs, np, kp, NSL))) return e;
+  for (int t = 1; t < TC_MAX_SEG; ++t) {
+    maps.a[t] = maps.a[0];
+    maps.b[t] = maps.b[0];
+  }
+  const TcSegs segs = make_segs(1, &k);
   const int kbt = (int)(kp / TK);
   const int S = split_count((mp / TM) * (np / TN), kbt);
   TcOut out{q.C, q.scm, q.scn, 0, 0, 0, 0, 0};
-  return launch_tc<NSL>(st, maps, kbt, kbt, m, n, mp, np, q.alpha, q.beta, out, S);
+  return launch_tc<NSL>(st, maps, segs, kbt, m, n, mp, np, q.alpha, q.beta, out, S);
 }
 
 int gemm_mixed(stream_t s, char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha,

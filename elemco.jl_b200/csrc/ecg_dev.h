@@ -94,30 +94,32 @@ int tc_split(stream_t s, const double* src, int64_t rows, int64_t k, int64_t sr,
 // copy: a descriptor over the same storage; rows past the view read as zero).
 int tc_view(const TcOperand& parent, int64_t row0, int64_t rows, TcOperand* out);
 // C(m,n) = alpha sum_k A(m,k) B(k,n) + beta C(m,n) over pre-split operands
-// (all with the same slice count): A[0]/B[0] give the first K segment,
-// A[1]/B[1] (optional) a second one.  A plain FP64 C (no index maps) may be
+// (all with the same slice count): the K sum runs over up to TC_MAX_SEG
+// segments A[s]/B[s], s = 0, 1, ... (the first null A[s] ends the list), each
+// with its own K depth and operands.  A plain FP64 C (no index maps) may be
 // computed in K slices summed in FP64 (to fill the GPU and to bound the FP32
 // accumulation length).  C is FP64, or FP32 when f32, at
 // C[rowoff(m) + coloff(n)] with rowoff(m) = (m % dm)*scm + (m / dm)*scm2
 // (dm = 0: m*scm) and coloff(n) = (n % dn)*scn + (n / dn)*scn2 (dn = 0:
 // n*scn).  Stores are coalesced when scm == 1.
+constexpr int TC_MAX_SEG = 4;
 struct TcGemm {
   int64_t m = 0, n = 0;
   double alpha = 1.0, beta = 0.0;
-  const TcOperand* A[2] = {nullptr, nullptr};
-  const TcOperand* B[2] = {nullptr, nullptr};
+  const TcOperand* A[TC_MAX_SEG] = {nullptr, nullptr, nullptr, nullptr};
+  const TcOperand* B[TC_MAX_SEG] = {nullptr, nullptr, nullptr, nullptr};
   void* C = nullptr;
   bool f32 = false;
   int64_t scm = 1, scn = 0, dn = 0, scn2 = 0, dm = 0, scm2 = 0;
 };
 int tc_gemm(stream_t s, const TcGemm& g);
-// Batched form: `batch` GEMMs of the shape of g (g.A/g.B give the operand
-// shapes), item b reading the operand descriptors mtab[b] (device memory,
-// 64-byte aligned, tc_maps_bytes() each, written by tc_maps_fill on the host)
-// and writing C + b*c_stride through g's index map.  One launch.
+// Batched form: `batch` GEMMs of the shape of g (g.A/g.B give the segments
+// and operand shapes), item b reading the operand descriptors mtab[b] (device
+// memory, 64-byte aligned, tc_maps_bytes() each, written by tc_maps_fill on
+// the host from nseg segments A[s]/B[s]) and writing C + b*c_stride through
+// g's index map.  One launch.
 size_t tc_maps_bytes();
-int tc_maps_fill(const TcOperand* A0, const TcOperand* B0, const TcOperand* A1,
-                 const TcOperand* B1, void* host_dst);
+int tc_maps_fill(int nseg, const TcOperand* const* A, const TcOperand* const* B, void* host_dst);
 int tc_gemm_batched(stream_t s, const TcGemm& g, int batch, const void* mtab, int64_t c_stride);
 
 // out = alpha * permute(in) + beta * out.  in has rank nd with dims

@@ -22,8 +22,11 @@
 //
 // Mixed precision: every operand is split into two BF16 slices once per call
 // (vvvo in both layouts, T^{xy} per pair, T2[:,:,x,:] and T2[:,:,:,x] per
-// occupied index, ovoo per pair), the GEMMs run on the tensor cores and K is
-// kept in FP32.
+// occupied index, -ovoo per pair), the GEMMs run on the tensor cores and K is
+// kept in FP32.  Each ovoo pair writes K through the same index map, and with
+// the same rows and columns, as one vvvo pair, so every K orientation is one
+// tensor-core GEMM of four K segments (v, v, o, o): three launches per batch,
+// each with a single pass over K.
 #include "ecg_triples.h"
 
 #include <algorithm>
@@ -113,7 +116,7 @@ struct Trip {
 
 // Host-built tables of one amplitude tensor's K builds for the whole sweep,
 // uploaded once: FP64 offset tables [9 GEMMs][triplet][A, B, C, A1, B1] or
-// tensor-core descriptor tables [6 GEMMs][triplet][maps].  The C offset is the
+// tensor-core descriptor tables [3 GEMMs][triplet][maps of 4 segments].  The C offset is the
 // triplet's slot in its batch.
 struct KTables {
   std::vector<int64_t> ptab;
@@ -122,7 +125,7 @@ struct KTables {
   unsigned char* mtab_d = nullptr;
 };
 
-constexpr int kGemmsFP64 = 9, kGemmsMixed = 6;
+constexpr int kGemmsFP64 = 9, kGemmsMixed = 3;
 
 void fill_tables(Ctx& c, const TriplesOps& ops, const SplitAmps* Sp, const std::vector<Trip>& tr,
                  int NB, int64_t kstride, KTables& kt) {
@@ -154,10 +157,12 @@ void fill_tables(Ctx& c, const TriplesOps& ops, const SplitAmps* Sp, const std::
     const int i = tr[t].i, j = tr[t].j, k = tr[t].k;
     PermW P[6];
     perm_table(i, j, k, v, P);
-    auto put = [&](int q, const dev::TcOperand* a0, const dev::TcOperand* a1,
-                   const dev::TcOperand* b0, const dev::TcOperand* b1) {
-      check(dev::tc_maps_fill(a0, b0, a1, b1, kt.mtab.data() + (q * nt + t) * mb), "maps");
-    };
+    // ovoo pairs (A of both segments, B of both segments) in the order of
+    // the vvvo pairs they share K's index map with
+    const dev::TcOperand* ovoo[3][4] = {
+        {op(j, i), op(k, i), &Sp->C[k], &Sp->G[j]},   // rows a, columns (b,c)
+        {&Sp->G[i], &Sp->C[k], op(k, j), op(i, j)},   // rows (a,c), columns b
+        {&Sp->G[i], &Sp->C[j], op(j, k), op(i, k)}};  // rows (a,b), columns c
     const int pairs[3][2] = {{0, 2}, {1, 4}, {3, 5}};
     for (int q = 0; q < 3; ++q) {
       const PermW& p0 = P[pairs[q][0]];
@@ -166,12 +171,11 @@ void fill_tables(Ctx& c, const TriplesOps& ops, const SplitAmps* Sp, const std::
       const dev::TcOperand* T1 = &Sp->pair[p1.x + o * p1.y];
       const dev::TcOperand* V0 = p0.l2 ? &ops.V2s[p0.z] : &ops.V1s[p0.z];
       const dev::TcOperand* V1 = p1.l2 ? &ops.V2s[p1.z] : &ops.V1s[p1.z];
-      if (p0.scm == 1) put(q, T0, T1, V0, V1);
-      else put(q, V0, V1, T0, T1);
+      const bool rows_a = p0.scm == 1;
+      const dev::TcOperand* A[4] = {rows_a ? T0 : V0, rows_a ? T1 : V1, ovoo[q][0], ovoo[q][1]};
+      const dev::TcOperand* B[4] = {rows_a ? V0 : T0, rows_a ? V1 : T1, ovoo[q][2], ovoo[q][3]};
+      check(dev::tc_maps_fill(4, A, B, kt.mtab.data() + (q * nt + t) * mb), "maps");
     }
-    put(3, &Sp->G[i], &Sp->C[j], op(j, k), op(i, k));
-    put(4, &Sp->G[i], &Sp->C[k], op(k, j), op(i, j));
-    put(5, op(j, i), op(k, i), &Sp->C[k], &Sp->G[j]);
   }
 }
 
@@ -238,28 +242,17 @@ void build_K_batch(Ctx& c, const TriplesOps& ops, const double* T, const SplitAm
     const PermW& p0 = P[pairs[q][0]];
     dev::TcGemm g;
     g.alpha = 1.0; g.beta = q ? 1.0 : 0.0; g.C = K; g.f32 = true;
-    if (p0.scm == 1) {  // rows a'
-      g.m = v; g.n = v2; g.A[0] = g.A[1] = Tp; g.B[0] = g.B[1] = Vp;
+    if (p0.scm == 1) {  // rows a', columns (b',c'); ovoo rows a
+      g.m = v; g.n = v2;
+      g.A[0] = g.A[1] = Tp; g.B[0] = g.B[1] = Vp; g.A[2] = g.A[3] = Op; g.B[2] = g.B[3] = Gp;
       g.scm = 1; g.scn = p0.scn; g.dn = p0.dn; g.scn2 = p0.scn2;
-    } else {            // rows (b',c'), columns a'
-      g.m = v2; g.n = v; g.A[0] = g.A[1] = Vp; g.B[0] = g.B[1] = Tp;
+    } else {            // rows (b',c'), columns a'; ovoo rows (a,b) or (a,c)
+      g.m = v2; g.n = v;
+      g.A[0] = g.A[1] = Vp; g.B[0] = g.B[1] = Tp; g.A[2] = g.A[3] = Gp; g.B[2] = g.B[3] = Op;
       g.scm = p0.scn; g.dm = p0.dn; g.scm2 = p0.scn2; g.scn = p0.scm;
     }
-    check(dev::tc_gemm_batched(s, g, nb, tab(q), kstride), "W vvvo");
+    check(dev::tc_gemm_batched(s, g, nb, tab(q), kstride), "W");
   }
-  dev::TcGemm g;
-  g.alpha = -1.0; g.beta = 1.0; g.C = K; g.f32 = true;
-  // (1) rows (a,b), columns c
-  g.m = v2; g.n = v; g.A[0] = g.A[1] = Gp; g.B[0] = g.B[1] = Op;
-  g.scm = 1; g.scn = v2;
-  check(dev::tc_gemm_batched(s, g, nb, tab(3), kstride), "W ovoo 1");
-  // (2) rows (a,c), columns b
-  g.scm = 1; g.dm = v; g.scm2 = v2; g.scn = v;
-  check(dev::tc_gemm_batched(s, g, nb, tab(4), kstride), "W ovoo 2");
-  // (3) rows a, columns (b,c)
-  g.m = v; g.n = v2; g.A[0] = g.A[1] = Op; g.B[0] = g.B[1] = Gp;
-  g.scm = 1; g.dm = 0; g.scm2 = 0; g.scn = v;
-  check(dev::tc_gemm_batched(s, g, nb, tab(5), kstride), "W ovoo 3");
 }
 
 }  // namespace
@@ -322,6 +315,9 @@ void pert_triples(Ctx& c, const double* U1h, const double* U2h, double* et, doub
                           &ops.V2s[kk]),
             "split vvvo");
     }
+    // -ovoo: the ovoo segments share the vvvo GEMMs' alpha = 1 (the BF16
+    // split of -x is the negated split of x)
+    check(dev::axpby(s, o * o * o * v, -1.0, On, 0.0, On), "-ovoo");
     for (int64_t z = 0; z < o; ++z)
       for (int64_t y = 0; y < o; ++y)
         check(dev::tc_split(s, On + o * y + o * o * v * z, v, o, o * o, 1, kTriplesSlices,
