@@ -775,6 +775,18 @@ static unsigned grid_for(int64_t n, int threads, int64_t cap) {
   return (unsigned)b;
 }
 
+__global__ void to_f32_kernel(int64_t n, const double* __restrict__ x, float* __restrict__ y) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = (float)x[i];
+}
+
+int to_f32(stream_t s, int64_t n, const double* x, float* y) {
+  if (n <= 0) return 0;
+  to_f32_kernel<<<grid_for(n, 256, 148 * 16), 256, 0, (cudaStream_t)s>>>(n, x, y);
+  return launched();
+}
+
 int axpby(stream_t s, int64_t n, double alpha, const double* x, double beta, double* y) {
   if (n <= 0) return 0;
   axpby_kernel<<<grid_for(n), 256, 0, (cudaStream_t)s>>>(n, alpha, x, beta, y);
@@ -1098,15 +1110,38 @@ __host__ __device__ constexpr int xp(int r, int d) {
 __host__ __device__ constexpr int xcomp(int q, int r) {
   return perm3_index(perm3(q, xp(r, 0)), perm3(q, xp(r, 1)));
 }
+// Parity of ordering q: (012)(120)(201) even, (021)(102)(210) odd.  For an
+// element in ordering q the transposed orderings (weight -2) are the three of
+// the other parity and the cyclic ones (weight 1) the two others of its own,
+// so X_q = 3 k_q + (sum of k over q's parity) - 2 (sum over the other).
+__host__ __device__ constexpr int perm3_parity(int q) {
+  return ((perm3(q, 0) > perm3(q, 1)) + (perm3(q, 0) > perm3(q, 2)) + (perm3(q, 1) > perm3(q, 2))) & 1;
+}
+constexpr bool x_parity_rule() {
+  for (int q = 0; q < 6; ++q) {
+    if (xcomp(q, 0) != q) return false;
+    for (int r = 1; r < 6; ++r) {
+      const int p = xcomp(q, r);
+      if (p == q || (r <= 3) == (perm3_parity(p) == perm3_parity(q))) return false;
+    }
+  }
+  return true;
+}
+static_assert(x_parity_rule(), "X term orderings follow the parity rule");
 // Index of the ordered position pair (x, y), x != y, in [0, 6).
 __host__ __device__ constexpr int pair_index(int x, int y) { return 2 * x + (y > x ? y - 1 : y); }
 
 constexpr int TCUBE = 8;
 constexpr int TPITCH = 9;                             // padded row pitch of a staged cube
 constexpr int TCUBE_ELEMS = TCUBE * TPITCH * TPITCH;  // 648
-constexpr int TS_MAT = 6 * 6 * 64;  // M0 M1 M2 N0 N1 N2 over the 6 ordered block pairs
-constexpr int TS_VEC = 7 * 3 * 8;   // g0 g1 g2 f0 f1 f2 ev over the 3 blocks
-constexpr int TS_STAGE = TS_MAT + TS_VEC;
+// Staged M/N blocks, in K's precision: for each ordered position pair (x, y)
+// (pair_index) and matrix w (M0 M1 M2 N0 N1 N2) the 8x8 block
+// [S_x + l_x, S_y + l_y] at (l_lo, l_hi) = (l[min(x,y)], l[max(x,y)]), l_lo
+// fastest: within a warp l0 varies fastest, then l1, so the reads are free of
+// bank conflicts.
+constexpr int TS_MAT = 6 * 6 * 64;
+// Staged vectors g0 g1 g2 f0 f1 f2, in K's precision: [w][position][l].
+constexpr int TS_VEC = 6 * 3 * 8;
 
 int64_t triples_cube_count(int nv) {
   const int64_t nt = (nv + TCUBE - 1) / TCUBE;
@@ -1140,20 +1175,28 @@ __device__ __forceinline__ void cp_async_n(void* smem, const void* gmem, bool pr
 
 // One block per orbit of cube triples A <= B <= C at a time.  The six cubes
 // K[S_s0 + x, S_s1 + y, S_s2 + z] (s a permutation, S = 8*(A,B,C)) are staged
-// in shared memory, in K's own precision, with the M/N blocks and vectors
-// they need; the loads of the next orbit (cp.async, double-buffered) run while
-// the current one is evaluated.  Thread (x,y,z) owns the element
-// e0 = S + (x,y,z) and its six orderings: it reads K at each ordering (one
-// value per cube), forms their six X values with one reciprocal of the common
-// denominator, and adds sum_e K_e X_e and sum_e X_e Y_e over the orderings.
-// Every ordered element of the orbit is reached |stabiliser| times (1, 2 or 6
-// when two or three of A, B, C coincide), which the weight undoes.
+// in shared memory with the M/N blocks and vectors they need (all in K's
+// precision; orbital energies in FP64); the loads of the next NBUF-1 orbits
+// (cp.async, NBUF buffers) are in flight while the current one is evaluated,
+// and the cube triple of the orbit after those is read one iteration ahead.
+// Thread (x,y,z) owns the element e0 = S + (x,y,z) and its six orderings: it
+// reads K at each ordering (one value per cube), forms their six X values
+// with one reciprocal of the common denominator, and adds sum_e K_e X_e and
+// sum_e X_e Y_e over the orderings.  Every ordered element of the orbit is
+// reached |stabiliser| times (1, 2 or 6 when two or three of A, B, C
+// coincide), which the weight undoes.
 template <typename T, bool HAS_U>
 struct EnergySmem {
   static constexpr int CUBES = 6 * TCUBE_ELEMS;
-  static constexpr int CUBE_BYTES = ((HAS_U ? 2 : 1) * CUBES * (int)sizeof(T) + 15) / 16 * 16;
-  static constexpr int BUF = CUBE_BYTES + TS_STAGE * 8;
-  static constexpr int BYTES = 2 * BUF;
+  static constexpr int r16(int b) { return (b + 15) / 16 * 16; }
+  static constexpr int MAT_OFF = r16((HAS_U ? 2 : 1) * CUBES * (int)sizeof(T));
+  static constexpr int VEC_OFF = MAT_OFF + r16(TS_MAT * (int)sizeof(T));
+  static constexpr int EV_OFF = VEC_OFF + r16(TS_VEC * (int)sizeof(T));  // 24 doubles
+  static constexpr int S_OFF = EV_OFF + 24 * 8;                          // cube origins
+  static constexpr int BUF = S_OFF + 16;
+  static constexpr int NBUF = (220 * 1024) / BUF < 4 ? (220 * 1024) / BUF : 4;
+  static constexpr int BYTES = NBUF * BUF;
+  static_assert(NBUF >= 2, "two staging buffers at least");
 };
 
 // Batch item y = blockIdx.y reads K + y*kstride (and KU), its denominator
@@ -1166,6 +1209,7 @@ __global__ void __launch_bounds__(512, 1) triples_energy_kernel(
     const TriplesTerms* __restrict__ tt_tab, const int* __restrict__ tri, int ntri,
     double* part) {
   using L = EnergySmem<T, HAS_U>;
+  constexpr int NB = L::NBUF;
   const int y = blockIdx.y;
   K += (int64_t)y * kstride;
   if (HAS_U) KU += (int64_t)y * kstride;
@@ -1181,97 +1225,149 @@ __global__ void __launch_bounds__(512, 1) triples_energy_kernel(
 #pragma unroll
   for (int q = 0; q < 6; ++q)
     koff[q] = q * TCUBE_ELEMS + l[perm3(q, 0)] + TPITCH * (l[perm3(q, 1)] + TPITCH * l[perm3(q, 2)]);
-  constexpr int NSTAGE = (TS_STAGE + 511) / 512;
 
-  // cp.async of orbit t into buffer b (one commit group per call)
-  auto issue = [&](int t, int b) {
+  // Staging roles, fixed per thread.  Threads 0..383 stage element (i, j) =
+  // (l0, l1) of position pair pr = l2 of all six matrices (source row
+  // S_px + i, column S_py + j); threads 384..511 stage the vectors, the
+  // orbital energies and the cube origins.
+  const int pr = l[2], spx = pr >> 1, spy0 = pr & 1, spy = spy0 < spx ? spy0 : spy0 + 1;
+  const int mdst = pr * 6 * 64 + (spx < spy ? l[0] + 8 * l[1] : l[1] + 8 * l[0]);
+  const T* msrc[6] = {(const T*)tt.M[0], (const T*)tt.M[1], (const T*)tt.M[2],
+                      (const T*)tt.N[0], (const T*)tt.N[1], (const T*)tt.N[2]};
+  auto vsrc = [&](int w) {
+    return (const T*)(w == 0 ? tt.g[0] : w == 1 ? tt.g[1] : w == 2 ? tt.g[2] : w == 3 ? tt.f[0]
+                      : w == 4 ? tt.f[1] : tt.f[2]);
+  };
+  const int f0 = tid - 384;
+
+  // cp.async of orbit t (cube origins S) into buffer b (one commit group)
+  auto issue = [&](int b, const int (&S)[3]) {
     unsigned char* base = tsm_raw + b * L::BUF;
     T* cK = reinterpret_cast<T*>(base);
     T* cU = cK + L::CUBES;
-    double* pm = reinterpret_cast<double*>(base + L::CUBE_BYTES);
-    const int S0 = tri[3 * t] * TCUBE, S1 = tri[3 * t + 1] * TCUBE, S2 = tri[3 * t + 2] * TCUBE;
 #pragma unroll
     for (int q = 0; q < 6; ++q) {
-      const int x = pick3(perm3(q, 0), S0, S1, S2) + l[0];
-      const int y = pick3(perm3(q, 1), S0, S1, S2) + l[1];
-      const int z = pick3(perm3(q, 2), S0, S1, S2) + l[2];
+      const int x = S[perm3(q, 0)] + l[0];
+      const int y = S[perm3(q, 1)] + l[1];
+      const int z = S[perm3(q, 2)] + l[2];
       const bool ok = x < v && y < v && z < v;
       const int idx = ok ? x + v * (y + v * z) : 0;
       cp_async_n<(int)sizeof(T)>(cK + q * TCUBE_ELEMS + lme, K + idx, ok);
       if (HAS_U) cp_async_n<(int)sizeof(T)>(cU + q * TCUBE_ELEMS + lme, KU + idx, ok);
     }
+    if (pr < 6) {
+      T* pm = reinterpret_cast<T*>(base + L::MAT_OFF);
+      const int r0 = pick3(spx, S[0], S[1], S[2]) + l[0];
+      const int c0 = pick3(spy, S[0], S[1], S[2]) + l[1];
+      const bool ok = r0 < v && c0 < v;
+      const int64_t off = ok ? r0 + (int64_t)v * c0 : 0;
 #pragma unroll
-    for (int u = 0; u < NSTAGE; ++u) {
-      const int e = tid + 512 * u;
-      if (e < TS_MAT) {
-        const int w = e / 384, pr = (e >> 6) % 6, i = e & 7, j = (e >> 3) & 7;
-        const int px = pr >> 1, py0 = pr & 1, py = py0 < px ? py0 : py0 + 1;
-        const int r0 = pick3(px, S0, S1, S2) + i, c0 = pick3(py, S0, S1, S2) + j;
-        const double* src = w == 0 ? tt.M[0] : w == 1 ? tt.M[1] : w == 2 ? tt.M[2]
-                          : w == 3 ? tt.N[0] : w == 4 ? tt.N[1] : tt.N[2];
-        const bool ok = r0 < v && c0 < v;
-        cp_async_n<8>(pm + e, ok ? src + r0 + v * c0 : src, ok);
-      } else if (e < TS_STAGE) {
-        const int f = e - TS_MAT, w = f / 24, pos = (f >> 3) % 3, i = f & 7;
-        const int x = pick3(pos, S0, S1, S2) + i;
-        const double* src = w == 0 ? tt.g[0] : w == 1 ? tt.g[1] : w == 2 ? tt.g[2]
-                          : w == 3 ? tt.f[0] : w == 4 ? tt.f[1] : w == 5 ? tt.f[2] : ev;
+      for (int w = 0; w < 6; ++w) cp_async_n<(int)sizeof(T)>(pm + mdst + w * 64, msrc[w] + off, ok);
+    } else {
+      T* pv = reinterpret_cast<T*>(base + L::VEC_OFF);
+      // vector entries f = w*24 + pos*8 + i, f < 144
+      for (int f = f0; f < TS_VEC; f += 128) {
+        const int w = f / 24, pos = (f >> 3) % 3, i = f & 7;
+        const int x = pick3(pos, S[0], S[1], S[2]) + i;
         const bool ok = x < v;
-        cp_async_n<8>(pm + e, ok ? src + x : src, ok);
+        cp_async_n<(int)sizeof(T)>(pv + f, vsrc(w) + (ok ? x : 0), ok);
+      }
+      if (f0 >= 16 && f0 < 40) {  // orbital energies: entry e = pos*8 + i
+        double* pe = reinterpret_cast<double*>(base + L::EV_OFF);
+        const int e = f0 - 16, pos = e >> 3, i = e & 7;
+        const int x = pick3(pos, S[0], S[1], S[2]) + i;
+        const bool ok = x < v;
+        cp_async_n<8>(pe + e, ev + (ok ? x : 0), ok);
+      } else if (f0 >= 40 && f0 < 43) {
+        reinterpret_cast<int*>(base + L::S_OFF)[f0 - 40] = pick3(f0 - 40, S[0], S[1], S[2]);
       }
     }
     cp_async_commit();
   };
+  // cube origins of orbit t (read ahead of their use)
+  auto origins = [&](int t, int (&S)[3]) {
+    if (t < ntri) {
+      S[0] = tri[3 * t] * TCUBE;
+      S[1] = tri[3 * t + 1] * TCUBE;
+      S[2] = tri[3 * t + 2] * TCUBE;
+    }
+  };
 
-  const double XW[6] = {4.0, -2.0, -2.0, -2.0, 1.0, 1.0};
   double eK = 0.0, eY = 0.0;
+  // prologue: orbits u = 0 .. NB-2 of this block into buffers u (an empty
+  // group for a missing orbit keeps the group count in step)
+  int ti = blockIdx.x;  // next orbit to issue
+  int nS[3] = {0, 0, 0};
+  origins(ti, nS);
+#pragma unroll 1
+  for (int u = 0; u < NB - 1; ++u, ti += gridDim.x) {
+    const int S[3] = {nS[0], nS[1], nS[2]};
+    origins(ti + gridDim.x, nS);
+    if (ti < ntri) issue(u, S);
+    else cp_async_commit();
+  }
   int b = 0;
-  if (blockIdx.x < ntri) issue(blockIdx.x, 0);
-  for (int t = blockIdx.x; t < ntri; t += gridDim.x, b ^= 1) {
-    const int tn = t + gridDim.x;
-    if (tn < ntri) issue(tn, b ^ 1);
-    else cp_async_commit();  // an empty group keeps the group count in step
-    cp_async_wait<1>();      // this orbit's copies have landed ...
-    __syncthreads();         // ... for every thread
+  for (int t = blockIdx.x; t < ntri; t += gridDim.x, ti += gridDim.x,
+           b = (b + 1 == NB) ? 0 : b + 1) {
+    {
+      // into the buffer evaluated last iteration (released by its trailing barrier)
+      const int S[3] = {nS[0], nS[1], nS[2]};
+      origins(ti + gridDim.x, nS);
+      if (ti < ntri) issue(b == 0 ? NB - 1 : b - 1, S);
+      else cp_async_commit();
+    }
+    cp_async_wait<NB - 1>();  // this orbit's copies have landed ...
+    __syncthreads();          // ... for every thread
     const unsigned char* base = tsm_raw + b * L::BUF;
     const T* cK = reinterpret_cast<const T*>(base);
     const T* cU = cK + L::CUBES;
-    const double* pmat = reinterpret_cast<const double*>(base + L::CUBE_BYTES);
-    const double* pvec = pmat + TS_MAT;
-    const int S0 = tri[3 * t] * TCUBE, S1 = tri[3 * t + 1] * TCUBE, S2 = tri[3 * t + 2] * TCUBE;
-    const int a0 = S0 + l[0], b0 = S1 + l[1], c0 = S2 + l[2];
-    if (a0 < v && b0 < v && c0 < v) {
+    const T* pm = reinterpret_cast<const T*>(base + L::MAT_OFF);
+    const T* pv = reinterpret_cast<const T*>(base + L::VEC_OFF);
+    const double* pe = reinterpret_cast<const double*>(base + L::EV_OFF);
+    const int* sS = reinterpret_cast<const int*>(base + L::S_OFF);
+    const int S0 = sS[0], S1 = sS[1], S2 = sS[2];
+    if (S0 + l[0] < v && S1 + l[1] < v && S2 + l[2] < v) {
       double k[6];
 #pragma unroll
       for (int q = 0; q < 6; ++q) k[q] = (double)cK[koff[q]];
-      const double dinv =
-          __drcp_rn(eijk - pvec[144 + l[0]] - pvec[152 + l[1]] - pvec[160 + l[2]]);
-      double X[6];
+      const double dinv = __drcp_rn(eijk - pe[l[0]] - pe[8 + l[1]] - pe[16 + l[2]]);
+      double se = 0.0, so = 0.0;
 #pragma unroll
       for (int q = 0; q < 6; ++q) {
-        double x = 0.0;
-#pragma unroll
-        for (int r = 0; r < 6; ++r) x += XW[r] * k[xcomp(q, r)];
-        X[q] = x * dinv;
+        if (perm3_parity(q)) so += k[q];
+        else se += k[q];
       }
-      // vectors at the three positions: vg[w][pos]
-      double vg[6][3];
+      const double ce = se - 2.0 * so, co = so - 2.0 * se;
+      double X[6];
 #pragma unroll
-      for (int w = 0; w < 6; ++w)
+      for (int q = 0; q < 6; ++q) X[q] = (3.0 * k[q] + (perm3_parity(q) ? co : ce)) * dinv;
+      // Y of ordering q = (p0,p1,p2): g0[p0] M0[p1,p2] + g1[p1] M1[p0,p2]
+      // + g2[p2] M2[p0,p1] + (f, N likewise).  Each ordered pair (x, y) with
+      // third position z serves three orderings: (z,x,y) through M0/N0,
+      // (x,z,y) through M1/N1 and (x,y,z) through M2/N2.
+      double vg[3][6];  // vectors at the three positions: vg[pos][w]
 #pragma unroll
-        for (int pos = 0; pos < 3; ++pos) vg[w][pos] = pvec[w * 24 + pos * 8 + l[pos]];
+      for (int pos = 0; pos < 3; ++pos)
+#pragma unroll
+        for (int w = 0; w < 6; ++w) vg[pos][w] = (double)pv[(w * 3 + pos) * 8 + l[pos]];
+      double yq[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+      for (int x = 0; x < 3; ++x)
+#pragma unroll
+        for (int yy = 0; yy < 3; ++yy) {
+          if (x == yy) continue;
+          const int z = 3 - x - yy;
+          const int lo = x < yy ? l[x] : l[yy], hi = x < yy ? l[yy] : l[x];
+          const T* mb = pm + pair_index(x, yy) * 6 * 64 + lo + 8 * hi;
+          yq[perm3_index(z, x)] += vg[z][0] * (double)mb[0] + vg[z][3] * (double)mb[3 * 64];
+          yq[perm3_index(x, z)] += vg[z][1] * (double)mb[64] + vg[z][4] * (double)mb[4 * 64];
+          yq[perm3_index(x, yy)] += vg[z][2] * (double)mb[2 * 64] + vg[z][5] * (double)mb[5 * 64];
+        }
       double ek = 0.0, ey = 0.0;
 #pragma unroll
       for (int q = 0; q < 6; ++q) {
-        const int p0 = perm3(q, 0), p1 = perm3(q, 1), p2 = perm3(q, 2);
-        auto mat = [&](int w, int x, int y) {
-          return pmat[(w * 6 + pair_index(x, y)) * 64 + l[x] + 8 * l[y]];
-        };
-        const double y = vg[0][p0] * mat(0, p1, p2) + vg[1][p1] * mat(1, p0, p2) +
-                         vg[2][p2] * mat(2, p0, p1) + vg[3][p0] * mat(3, p1, p2) +
-                         vg[4][p1] * mat(4, p0, p2) + vg[5][p2] * mat(5, p0, p1);
         ek += (HAS_U ? (double)cU[koff[q]] : k[q]) * X[q];
-        ey += X[q] * y;
+        ey += X[q] * yq[q];
       }
       const bool ab = (S0 == S1), bc = (S1 == S2);
       const double wgt = (ab && bc) ? (1.0 / 6.0) : (ab || bc) ? 0.5 : 1.0;
@@ -1355,13 +1451,6 @@ static int launch_energy(cudaStream_t st, int nv, int nitems, const void* K, con
   if (e) return e;
   final_sum_pairs_kernel<<<2 * nitems, 256, 0, st>>>(g, scratch, out);
   return launched();
-}
-
-int triples_energy(stream_t s, int nv, const void* K, const void* KU, bool k_f32, double eijk,
-                   const double* ev, const TriplesTerms& t, const int* tri, double* scratch,
-                   double* out) {
-  return launch_energy((cudaStream_t)s, nv, 1, K, KU, 0, k_f32, eijk, nullptr, ev, t, nullptr,
-                       tri, scratch, out);
 }
 
 int triples_energy_batched(stream_t s, int nv, int nitems, const void* K, const void* KU,

@@ -166,33 +166,33 @@ int outer(stream_t s, int64_t na, int64_t ni, int64_t nb, int64_t nj, double alp
 int combine(stream_t s, int64_t n, int m, const double* const* X, const double* coef,
             double* out);
 
-// (T) energy of one occupied triplet (src/cc/cc_triples.jl:113-156) from
+// y[i] = (float)x[i]
+int to_f32(stream_t s, int64_t n, const double* x, float* y);
+
+// (T) energies of occupied triplets (src/cc/cc_triples.jl:113-156) from
 // K[a,b,c] (FP64, or FP32 when k_f32), without storing X:
 //   X[a,b,c] = (4K[abc]-2K[acb]-2K[cba]-2K[bac]+K[cab]+K[bca]) / (eijk-ev[a]-ev[b]-ev[c])
 //   out[0]   = sum KE*X      (KE = KU when given, else K)
 //   out[1]   = sum X*Y,  Y[a,b,c] = g0[a] M0[b,c] + g1[b] M1[a,c] + g2[c] M2[a,b]
 //                              + f0[a] N0[b,c] + f1[b] N1[a,c] + f2[c] N2[a,b]
 // The 8^3 cubes of K are visited in orbits of the index permutations, so each
-// element of K is read once; partial sums land in `scratch` (at least
-// triples_energy_scratch_len(nv, 1) doubles) and are summed in a fixed order.  `tri` holds
-// the cube triples A <= B <= C (3 ints each) for nt = ceil(nv/8) cubes per
-// axis: triples_cube_count(nv) of them, written by triples_cube_table().
+// element of K is read once.  `tri` holds the cube triples A <= B <= C (3
+// ints each) for nt = ceil(nv/8) cubes per axis: triples_cube_count(nv) of
+// them, written by triples_cube_table().  g, f (length nv) and M, N (nv x nv)
+// hold elements of K's precision; ev (FP64) the virtual orbital energies.
 // nv <= 1290 (32-bit element offsets).
 struct TriplesTerms {
-  const double* g[3];
-  const double* f[3];
-  const double* M[3];
-  const double* N[3];
+  const void* g[3];
+  const void* f[3];
+  const void* M[3];
+  const void* N[3];
 };
 int64_t triples_cube_count(int nv);
 void triples_cube_table(int nv, int* tri);
-int triples_energy(stream_t s, int nv, const void* K, const void* KU, bool k_f32, double eijk,
-                   const double* ev, const TriplesTerms& t, const int* tri, double* scratch,
-                   double* out);
-// Batched form: item b reads K + b*kstride (KU likewise), eijk_tab[b] and
-// tt_tab[b] (device tables) and writes out[2b], out[2b+1]; `scratch` holds at
-// least triples_energy_scratch_len(nv, nitems) doubles.  One launch (plus one
-// fixed-order reduction launch).
+// Item b reads K + b*kstride (KU likewise), eijk_tab[b] and tt_tab[b] (device
+// tables) and writes out[2b], out[2b+1]; partial sums land in `scratch` (at
+// least triples_energy_scratch_len(nv, nitems) doubles) and are summed in a
+// fixed order.  One launch (plus one fixed-order reduction launch).
 int64_t triples_energy_scratch_len(int nv, int nitems);
 int triples_energy_batched(stream_t s, int nv, int nitems, const void* K, const void* KU,
                            int64_t kstride, bool k_f32, const double* eijk_tab, const double* ev,

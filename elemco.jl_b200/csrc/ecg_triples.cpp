@@ -390,15 +390,33 @@ void pert_triples(Ctx& c, const double* U1h, const double* U2h, double* et, doub
   check(dev::h2d(gf, gh.data(), v * o * 8, s), "h2d");
   check(dev::h2d(gf + v * o, fh.data(), v * o * 8, s), "h2d");
   const double* Nsrc = lam ? U2c : c.T2();
-  auto M = [&](int x, int y) { return c.Kvvoo + v2 * (x + o * y); };
-  auto N = [&](int x, int y) { return Nsrc + v2 * (x + o * y); };
+  // the energy kernel reads g, f, M and N in K's precision: FP32 copies in
+  // mixed precision (they enter only the singles/Fock term sum X Y)
+  const void* gfe = gf;
+  const void* Me = c.Kvvoo;
+  const void* Ne = Nsrc;
+  if (mixed) {
+    const int64_t n2 = v2 * o * o;
+    float* t32 = reinterpret_cast<float*>(c.alloc((2 * v * o + 2 * n2 + 1) / 2, "(T) FP32 terms"));
+    check(dev::to_f32(s, 2 * v * o, gf, t32), "FP32 g, f");
+    check(dev::to_f32(s, n2, c.Kvvoo, t32 + 2 * v * o), "FP32 <ij|ab>");
+    check(dev::to_f32(s, n2, Nsrc, t32 + 2 * v * o + n2), "FP32 amplitudes");
+    gfe = t32;
+    Me = t32 + 2 * v * o;
+    Ne = t32 + 2 * v * o + n2;
+  }
+  auto at = [&](const void* p, int64_t off) {
+    return static_cast<const void*>(static_cast<const char*>(p) + esz * off);
+  };
+  auto M = [&](int x, int y) { return at(Me, v2 * (x + o * y)); };
+  auto N = [&](int x, int y) { return at(Ne, v2 * (x + o * y)); };
   std::vector<dev::TriplesTerms> terms(nt);
   std::vector<double> eijk(nt);
   for (int64_t t = 0; t < nt; ++t) {
     const int i = tr[t].i, j = tr[t].j, k = tr[t].k;
     dev::TriplesTerms& tt = terms[t];
-    tt.g[0] = gf + v * i; tt.g[1] = gf + v * j; tt.g[2] = gf + v * k;
-    tt.f[0] = gf + v * (o + i); tt.f[1] = gf + v * (o + j); tt.f[2] = gf + v * (o + k);
+    tt.g[0] = at(gfe, v * i); tt.g[1] = at(gfe, v * j); tt.g[2] = at(gfe, v * k);
+    tt.f[0] = at(gfe, v * (o + i)); tt.f[1] = at(gfe, v * (o + j)); tt.f[2] = at(gfe, v * (o + k));
     tt.M[0] = M(j, k); tt.M[1] = M(i, k); tt.M[2] = M(i, j);
     tt.N[0] = N(j, k); tt.N[1] = N(i, k); tt.N[2] = N(i, j);
     eijk[t] = tr[t].eijk;
