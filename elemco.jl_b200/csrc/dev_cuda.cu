@@ -787,6 +787,23 @@ int to_f32(stream_t s, int64_t n, const double* x, float* y) {
   return launched();
 }
 
+// exponent field all ones: infinity or NaN
+__global__ void nonfinite_kernel(int64_t n, const double* __restrict__ x, double* flag) {
+  bool bad = false;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    bad |= ((__double_as_longlong(x[i]) >> 52) & 0x7ff) == 0x7ff;
+  if (__syncthreads_or(bad) && threadIdx.x == 0) *flag = 1.0;
+}
+
+int nonfinite(stream_t s, int64_t n, const double* x, double* flag) {
+  cudaError_t e = cudaMemsetAsync(flag, 0, sizeof(double), (cudaStream_t)s);
+  if (e != cudaSuccess) return (int)e;
+  if (n <= 0) return 0;
+  nonfinite_kernel<<<grid_for(n, 256, 148 * 8), 256, 0, (cudaStream_t)s>>>(n, x, flag);
+  return launched();
+}
+
 int axpby(stream_t s, int64_t n, double alpha, const double* x, double beta, double* y) {
   if (n <= 0) return 0;
   axpby_kernel<<<grid_for(n), 256, 0, (cudaStream_t)s>>>(n, alpha, x, beta, y);

@@ -64,13 +64,36 @@ static void opts_or_default(const ecg_cc_opts* in, ecg_cc_opts& o) {
   if (o.maxit < 0) throw Error(ECG_ERR_ARG, "maxit must be >= 0");
 }
 
+// Device scalar slot of the non-finite input flag.
+constexpr int kFlagSlot = 255;
+
+// Copies n host doubles to device memory d and checks them there (one pass
+// over HBM instead of a host scan); a non-finite value raises
+// ECG_ERR_NONFINITE after the copy.
+static void h2d_finite(Ctx& c, double* d, const double* h, int64_t n, const char* what) {
+  check(dev::h2d(d, h, n * 8, c.st), what);
+  check(dev::nonfinite(c.st, n, d, c.dscal + kFlagSlot), what);
+  check(dev::d2h(c.hscal + kFlagSlot, c.dscal + kFlagSlot, sizeof(double), c.st), "d2h flag");
+  check(dev::sync(c.st), "sync");
+  if (c.hscal[kFlagSlot] != 0.0)
+    throw Error(ECG_ERR_NONFINITE, std::string("non-finite value in ") + what);
+}
+
 static void load_T(Ctx& c, const double* T1, const double* T2) {
   need_ptr(T1, "T1");
   need_ptr(T2, "T2");
   check_finite(T1, c.n1(), "T1");
-  check_finite(T2, c.n2(), "T2");
+  c.t_resident = false;
   check(dev::h2d(c.T1(), T1, c.n1() * 8, c.st), "h2d T1");
-  check(dev::h2d(c.T2(), T2, c.n2() * 8, c.st), "h2d T2");
+  h2d_finite(c, c.T2(), T2, c.n2(), "T2");
+  c.t_resident = true;
+}
+
+// Host amplitudes, or (both NULL) the amplitudes the context holds.
+static void load_T_or_resident(Ctx& c, const double* T1, const double* T2) {
+  if (T1 || T2) return load_T(c, T1, T2);
+  if (!c.t_resident)
+    throw Error(ECG_ERR_STATE, "no amplitudes on the device: pass T1 and T2");
 }
 
 extern "C" {
@@ -181,6 +204,7 @@ int ecg_mp2(ecg_ctx* c, double* T1, double* T2, double* e_mp2) {
     if (T1) check(dev::d2h(T1, c->T1(), c->n1() * 8, s), "d2h");
     if (T2) check(dev::d2h(T2, c->T2(), c->n2() * 8, s), "d2h");
     sync_scalars(*c, 3);
+    c->t_resident = true;
     if (e_mp2) *e_mp2 = 2.0 * c->hscal[0] - c->hscal[1] + 2.0 * c->hscal[2];
   });
 }
@@ -204,7 +228,7 @@ int ecg_cc_load(ecg_ctx* c, const double* T1, const double* T2, const ecg_cc_opt
     need_system(*c);
     ecg_cc_opts o;
     opts_or_default(opts, o);
-    if (T1 || T2) load_T(*c, T1, T2);
+    load_T_or_resident(*c, T1, T2);
     cc_init_iterations(*c, o);
     check(dev::sync(c->st), "sync");
   });
@@ -296,7 +320,7 @@ int ecg_pert_t(ecg_ctx* c, const double* T1, const double* T2, double* e_t, doub
   if (!c) return ECG_ERR_ARG;
   return guarded(c, [&] {
     need_system(*c);
-    load_T(*c, T1, T2);
+    load_T_or_resident(*c, T1, T2);
     double et = 0, etb = 0;
     c->mixed_active = (c->prec == ECG_PREC_MIXED);
     struct Restore {
@@ -314,7 +338,7 @@ int ecg_lambda_pert_t(ecg_ctx* c, const double* T1, const double* T2, const doub
   if (!c) return ECG_ERR_ARG;
   return guarded(c, [&] {
     need_system(*c);
-    load_T(*c, T1, T2);
+    load_T_or_resident(*c, T1, T2);
     need_ptr(U1, "U1");
     need_ptr(U2, "U2");
     check_finite(U1, c->n1(), "U1");

@@ -80,6 +80,7 @@ void Ctx::free_all() {
   if (hscal) dev::hfree_pinned(hscal);
   hscal = nullptr;
   have_system = false;
+  t_resident = false;
   // buffers allocated on first use must be allocated again for the next system
   U = RU = vT = D1 = dD1 = nullptr;
   lambda_ready = false;

@@ -54,6 +54,8 @@ struct Ctx {
 
   // amplitudes: T = [T1 (nv*no) | T2 (nv^2 no^2)], same for R
   double *T = nullptr, *R = nullptr;
+  // T holds amplitudes of this system (from mp2, a load or the CC iterations)
+  bool t_resident = false;
   double* TT = nullptr;  // outer-product scratch nv^2 no^2
 
   // device scalars + reduction scratch, pinned host mirror

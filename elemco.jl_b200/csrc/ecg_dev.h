@@ -168,6 +168,8 @@ int combine(stream_t s, int64_t n, int m, const double* const* X, const double* 
 
 // y[i] = (float)x[i]
 int to_f32(stream_t s, int64_t n, const double* x, float* y);
+// *flag = 1 if any of x[0..n) is an infinity or NaN, else 0 (device double)
+int nonfinite(stream_t s, int64_t n, const double* x, double* flag);
 
 // (T) energies of occupied triplets (src/cc/cc_triples.jl:113-156) from
 // K[a,b,c] (FP64, or FP32 when k_f32), without storing X:

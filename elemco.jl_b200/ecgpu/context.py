@@ -120,8 +120,11 @@ class Context:
         self._chk(self._L.ecg_cc_store(self._h, dptr(T1), dptr(T2)))
         return T1, T2
 
-    def pert_t(self, T1, T2):
-        T1, T2 = as_f(T1), as_f(T2)
+    def pert_t(self, T1=None, T2=None):
+        """(T) and [T] energies; T1 = T2 = None uses the amplitudes the context
+        holds (from the last mp2 / cc_solve on this system) without an upload."""
+        if T1 is not None or T2 is not None:
+            T1, T2 = as_f(T1), as_f(T2)
         e, eb = C.c_double(), C.c_double()
         self._chk(self._L.ecg_pert_t(self._h, dptr(T1), dptr(T2), C.byref(e), C.byref(eb)))
         return e.value, eb.value
@@ -145,8 +148,11 @@ class Context:
                 "iterations": it.value, "converged": bool(conv.value)}
 
     def lambda_pert_t(self, T1, T2, U1, U2):
+        """Lambda-(T); T1 = T2 = None uses the amplitudes the context holds."""
+        if T1 is not None or T2 is not None:
+            T1, T2 = as_f(T1), as_f(T2)
         e, eb = C.c_double(), C.c_double()
-        self._chk(self._L.ecg_lambda_pert_t(self._h, dptr(as_f(T1)), dptr(as_f(T2)),
+        self._chk(self._L.ecg_lambda_pert_t(self._h, dptr(T1), dptr(T2),
                                             dptr(as_f(U1)), dptr(as_f(U2)), C.byref(e),
                                             C.byref(eb)))
         return e.value, eb.value

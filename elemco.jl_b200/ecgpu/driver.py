@@ -318,10 +318,11 @@ def ccdriver(EC, method, fcidump=""):
             miosave(os.path.join(EC.scr, o["cc"].save_lm + "_1" + EC.ext), U1)
             miosave(os.path.join(EC.scr, o["cc"].save_lm + "_2" + EC.ext), U2)
     if pert:
+        # the context still holds the converged amplitudes: no re-upload
         if lam:
-            ET3, ET3b = ctx.lambda_pert_t(T1, T2, U1, U2)
+            ET3, ET3b = ctx.lambda_pert_t(None, None, U1, U2)
         else:
-            ET3, ET3b = ctx.pert_t(T1, T2)
+            ET3, ET3b = ctx.pert_t()
         out["[T]"] = ET3b
         out["(T)"] = ET3
         out[main + "(T)c"] = E + ET3

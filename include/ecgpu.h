@@ -98,13 +98,17 @@ int ecg_cc_solve(ecg_ctx* ctx, int dc, const ecg_cc_opts* opts, double* T1,
  * the loop on the host: load amplitudes into the context's device state,
  * run `nsteps` iterations of the cc_iterations! body (residual, Hylleraas
  * energy, update, DIIS, energy), read the amplitudes back.  Host pointers may
- * be NULL to skip the copy (device-resident amplitudes). */
+ * be NULL to skip the copy (device-resident amplitudes; ECG_ERR_STATE if the
+ * context holds none for this system). */
 int ecg_cc_load(ecg_ctx* ctx, const double* T1, const double* T2, const ecg_cc_opts* opts);
 int ecg_cc_step(ecg_ctx* ctx, int dc, int32_t nsteps, double* out);
 int ecg_cc_store(ecg_ctx* ctx, double* T1, double* T2);
 
 /* Closed-shell (T) and [T]: calc_pertT_closed_shell
- * (src/cc/cc_triples.jl:39-157). */
+ * (src/cc/cc_triples.jl:39-157).  T1 and T2 may both be NULL to use the
+ * amplitudes the context holds (those of the last ecg_mp2, ecg_cc_solve,
+ * amplitude load or iteration on this system; ECG_ERR_STATE if there are
+ * none), which skips their upload.  The same holds for ecg_lambda_pert_t. */
 int ecg_pert_t(ecg_ctx* ctx, const double* T1, const double* T2, double* e_t,
                double* e_t_bracket);
 

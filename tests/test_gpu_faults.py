@@ -66,3 +66,28 @@ def test_bad_arguments(h2o_df):
         with pytest.raises(ecgpu.ECGError) as e:
             c.diag_permute(np.zeros((2, 2)), (0, 0))
         assert e.value.code == ECG_ERR_ARG
+
+
+def test_resident_amplitudes(h2o_df):
+    """(T) without amplitudes uses those the context holds (no upload) and
+    gives the same energy as with the host copy; with none on the device
+    (a fresh system, or after a rejected load) it is a state error.  A NaN in
+    the last element of T2 is caught by the device-side check."""
+    B, S = h2o_df
+    with ecgpu.Context(0) as c:
+        c.set_system(B, S.h, S.e0, S.no)
+        with pytest.raises(ecgpu.ECGError) as e:
+            c.pert_t()
+        assert e.value.code == ECG_ERR_STATE
+        _, T1, T2 = c.mp2()
+        r = c.cc_solve(T1, T2)
+        assert c.pert_t() == c.pert_t(r["T1"], r["T2"])
+        T2bad = np.array(r["T2"], order="F")
+        T2bad[-1, -1, -1, -1] = np.nan
+        with pytest.raises(ecgpu.ECGError) as e:
+            c.pert_t(r["T1"], T2bad)
+        assert e.value.code == ECG_ERR_NONFINITE
+        with pytest.raises(ecgpu.ECGError) as e:
+            c.pert_t()
+        assert e.value.code == ECG_ERR_STATE
+        assert c.pert_t(r["T1"], r["T2"])[0] < 0.0  # still usable
