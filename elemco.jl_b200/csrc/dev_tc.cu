@@ -39,7 +39,7 @@ constexpr int TILE_BYTES_B = TN * TK * 2;
 constexpr int RING_BYTES = 192 * 1024;
 // longest K (in 64-wide k-blocks) one FP32 tensor-memory accumulator sums
 // before its partial product is handed to an FP64 reduction
-constexpr int KB_ACC = 16;
+constexpr int KB_ACC = (int)(TC_ACC_K / TK);
 constexpr unsigned long long WAIT_NS = 1000000000ull;  // 1 s bound on every mbarrier wait
 
 template <int NSL>
@@ -672,6 +672,103 @@ int tc_split(stream_t s, const double* src, int64_t rows, int64_t k, int64_t sr,
   if (e) return e;
   return make_map(enc, reinterpret_cast<CUtensorMap*>(op->map), dst, op->rows_p, op->k_p,
                   slices);
+}
+
+int64_t tc_pad_rows(int64_t rows) { return pad_rows(rows); }
+int64_t tc_pad_k(int64_t k) { return pad_k(k); }
+
+int tc_bind(void* dst, int64_t rows, int64_t k, int slices, TcOperand* op) {
+  if (rows <= 0 || k <= 0 || !dst || !op || (slices != 2 && slices != 3))
+    return (int)cudaErrorInvalidValue;
+  if (((uintptr_t)dst & 15) != 0) return (int)cudaErrorMisalignedAddress;
+  EncodeFn enc = nullptr;
+  int e = encode_fn(&enc);
+  if (e) return e;
+  op->rows = rows;
+  op->k = k;
+  op->rows_p = pad_rows(rows);
+  op->k_p = pad_k(k);
+  op->slices = slices;
+  op->base = dst;
+  op->slice_stride = op->rows_p * op->k_p;
+  return make_map(enc, reinterpret_cast<CUtensorMap*>(op->map), dst, op->rows_p, op->k_p,
+                  slices);
+}
+
+namespace {
+
+// dst[k + t*sl] = slice t of x (t = 0, 1, 2), the split of split_kernel
+__device__ __forceinline__ void put_slices3(__nv_bfloat16* dst, int64_t sl, int64_t k, double x) {
+  const __nv_bfloat16 h0 = __double2bfloat16(x);
+  const double e1 = x - (double)__bfloat162float(h0);
+  const __nv_bfloat16 h1 = __double2bfloat16(e1);
+  const double e2 = e1 - (double)__bfloat162float(h1);
+  dst[k] = h0;
+  dst[k + sl] = h1;
+  dst[k + 2 * sl] = __double2bfloat16(e2);
+}
+
+// One thread per (pair row pr, packed index k < kp_p) of the symmetric
+// operand, in the element order of ladder_pack_v: X[c,d] = V[c + v a' + lda
+// (d + v b')] with (c, d) = cdp[k], c <= d; X[d,c] is reread from L2 by the
+// neighbouring rows' threads.  Row pr gets X[c,d] + X[d,c] (X[c,c] on the
+// diagonal) at k, and for a < b and c < d row pr - a' - 1 of the
+// antisymmetric operand gets X[c,d] - X[d,c] at k - d = d(d-1)/2 + c; the K
+// padding of both is written as zeros.
+template <typename VT>
+__global__ void ladder_pack_split_kernel(int nv, int a0, int na, int npairs,
+                                         const int2* __restrict__ pairs,
+                                         const int2* __restrict__ cdp, const VT* __restrict__ V,
+                                         int64_t kp_p, int64_t sl_p, int64_t kp_m, int64_t sl_m,
+                                         __nv_bfloat16* __restrict__ Vp,
+                                         __nv_bfloat16* __restrict__ Vm) {
+  const int64_t v = nv, lda = v * na, ncdp = v * (v + 1) / 2, ncdm = v * (v - 1) / 2;
+  const int64_t total = kp_p * npairs, mpad = kp_m - ncdm;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = idx % kp_p, pr = idx / kp_p;
+    const int2 ab = pairs[pr];
+    const int64_t ap = ab.x - a0, bp = ab.y - a0;
+    const bool minus = ab.x < ab.y;
+    __nv_bfloat16* om = minus ? Vm + (pr - ap - 1) * kp_m : Vm;
+    if (k < ncdp) {
+      const int2 cd = cdp[k];
+      const double x = (double)V[cd.x + v * ap + lda * (cd.y + v * bp)];
+      const double y = (double)V[cd.y + v * ap + lda * (cd.x + v * bp)];
+      put_slices3(Vp + pr * kp_p, sl_p, k, cd.x == cd.y ? x : x + y);
+      if (minus && cd.x < cd.y) put_slices3(om, sl_m, k - cd.y, x - y);
+    } else {
+      put_slices3(Vp + pr * kp_p, sl_p, k, 0.0);
+    }
+    if (minus && k < mpad) put_slices3(om, sl_m, ncdm + k, 0.0);
+  }
+}
+
+}  // namespace
+
+int ladder_pack_v_split(stream_t s, int nv, int a0, int na, int npairs, const int* pairs,
+                        const int* cdp, const void* V, bool v_f32, void* Vp, void* Vm) {
+  if (nv <= 0 || npairs <= 0 || !V || !Vp || !cdp) return (int)cudaErrorInvalidValue;
+  const int64_t v = nv;
+  const int npm = npairs - na;  // the block's a < b pairs
+  if (npm > 0 && !Vm) return (int)cudaErrorInvalidValue;
+  const int64_t kp_p = pad_k(v * (v + 1) / 2), sl_p = pad_rows(npairs) * kp_p;
+  const int64_t kp_m = v > 1 ? pad_k(v * (v - 1) / 2) : 0;
+  const int64_t sl_m = npm > 0 ? pad_rows(npm) * kp_m : 0;
+  if (kp_m - v * (v - 1) / 2 > kp_p) return (int)cudaErrorInvalidValue;
+  const int64_t total = kp_p * npairs;
+  const unsigned g = (unsigned)std::min<int64_t>((total + 255) / 256, 148 * 16);
+  cudaStream_t st = (cudaStream_t)s;
+  if (v_f32)
+    ladder_pack_split_kernel<float><<<g, 256, 0, st>>>(
+        nv, a0, na, npairs, (const int2*)pairs, (const int2*)cdp, (const float*)V, kp_p, sl_p,
+        kp_m, sl_m, (__nv_bfloat16*)Vp, (__nv_bfloat16*)Vm);
+  else
+    ladder_pack_split_kernel<double><<<g, 256, 0, st>>>(
+        nv, a0, na, npairs, (const int2*)pairs, (const int2*)cdp, (const double*)V, kp_p, sl_p,
+        kp_m, sl_m, (__nv_bfloat16*)Vp, (__nv_bfloat16*)Vm);
+  note_launches(1);
+  return (int)cudaGetLastError();
 }
 
 int tc_view(const TcOperand& parent, int64_t row0, int64_t rows, TcOperand* out) {

@@ -349,8 +349,9 @@ void ladder(Ctx& c, const double* Bf, const double* BfT, const double* T2, doubl
   // Mixed precision: the operands shared by every a-block (BfT for the V
   // build, the packed T2 for the contractions) are split into BF16 slices once
   // per call, each block reads row ranges of them; the per-block V+/- are
-  // split per block.  Which GEMMs go to the tensor cores follows gemm_prec's
-  // size rule.
+  // packed straight into BF16 slices (one pass over V, written in FP32 by the
+  // tensor cores, which accumulate it in FP32).  Which GEMMs go to the tensor
+  // cores follows gemm_prec's size rule.
   const double big = 67108864.0;
   const bool mv = c.mixed_active && (double)(v * c.lblocks[0].na) * (double)(v * v) * Q >= big;
   const bool mp = c.mixed_active && (double)maxpp * nijp * ncdp >= big;
@@ -374,6 +375,8 @@ void ladder(Ctx& c, const double* Bf, const double* BfT, const double* T2, doubl
     if (mp) check(dev::tc_split(s, Ts, nijp, ncdp, ncdp, 1, NSL, pTs, &oTs), "split T+");
     if (mm) check(dev::tc_split(s, Ta, nijm, ncdm, ncdm, 1, NSL, pTa, &oTa), "split T-");
   }
+  const bool fused = mp && mm;  // V+/- packed into BF16 slices directly
+  const bool vf32 = fused && mv && Q <= dev::TC_ACC_K;
   for (auto& b : c.lblocks) {
     const int64_t nb = v - b.a0;
     // V[c,a',d,b''] = sum_Q BfT[c,a0+a',Q] BfT[d,a0+b'',Q]
@@ -383,7 +386,7 @@ void ladder(Ctx& c, const double* Bf, const double* BfT, const double* T2, doubl
       check(dev::tc_view(oB, v * b.a0, v * nb, &bb), "view BfT");
       dev::TcGemm g;
       g.m = v * b.na; g.n = v * nb; g.A[0] = &a; g.B[0] = &bb;
-      g.C = V; g.scm = 1; g.scn = v * b.na;
+      g.C = V; g.scm = 1; g.scn = v * b.na; g.f32 = vf32;
       check(dev::tc_gemm(s, g), "gemm ladder V");
     } else {
       check(dev::gemm(s, 'N', 'T', v * b.na, v * nb, Q, 1.0, BfT + v * b.a0, v * v,
@@ -391,9 +394,17 @@ void ladder(Ctx& c, const double* Bf, const double* BfT, const double* T2, doubl
             "gemm ladder V");
     }
     const int* pairs = c.pairs + 2 * b.poff;
-    check(dev::ladder_pack_v(s, (int)v, b.a0, b.na, b.npp, pairs, c.cdp, V, Vp, Vm), "pack V");
+    if (fused) {
+      check(dev::ladder_pack_v_split(s, (int)v, b.a0, b.na, b.npp, pairs, c.cdp, V, vf32, pVp,
+                                     pVm),
+            "pack V");
+      check(dev::tc_bind(pVp, b.npp, ncdp, NSL, &oVp), "bind V+");
+      if (b.npm > 0) check(dev::tc_bind(pVm, b.npm, ncdm, NSL, &oVm), "bind V-");
+    } else {
+      check(dev::ladder_pack_v(s, (int)v, b.a0, b.na, b.npp, pairs, c.cdp, V, Vp, Vm), "pack V");
+    }
     if (mp) {
-      check(dev::tc_split(s, Vp, b.npp, ncdp, ncdp, 1, NSL, pVp, &oVp), "split V+");
+      if (!fused) check(dev::tc_split(s, Vp, b.npp, ncdp, ncdp, 1, NSL, pVp, &oVp), "split V+");
       dev::TcGemm g;
       g.m = b.npp; g.n = nijp; g.A[0] = &oVp; g.B[0] = &oTs;
       g.C = Lp; g.scm = 1; g.scn = b.npp;
@@ -404,7 +415,7 @@ void ladder(Ctx& c, const double* Bf, const double* BfT, const double* T2, doubl
     }
     if (b.npm > 0 && nijm > 0) {
       if (mm) {
-        check(dev::tc_split(s, Vm, b.npm, ncdm, ncdm, 1, NSL, pVm, &oVm), "split V-");
+        if (!fused) check(dev::tc_split(s, Vm, b.npm, ncdm, ncdm, 1, NSL, pVm, &oVm), "split V-");
         dev::TcGemm g;
         g.m = b.npm; g.n = nijm; g.A[0] = &oVm; g.B[0] = &oTa;
         g.C = Lm; g.scm = 1; g.scn = b.npm;

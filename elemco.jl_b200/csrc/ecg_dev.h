@@ -93,6 +93,18 @@ int tc_split(stream_t s, const double* src, int64_t rows, int64_t k, int64_t sr,
 // Rows [row0, row0 + rows) of a split operand as an operand of their own (no
 // copy: a descriptor over the same storage; rows past the view read as zero).
 int tc_view(const TcOperand& parent, int64_t row0, int64_t rows, TcOperand* out);
+// Descriptor over slices already written to dst in tc_split's layout
+// ([slice][tc_pad_rows(rows)][tc_pad_k(k)], K fastest, zero K padding).
+int tc_bind(void* dst, int64_t rows, int64_t k, int slices, TcOperand* op);
+int64_t tc_pad_rows(int64_t rows);
+int64_t tc_pad_k(int64_t k);
+// ladder_pack_v fused with the three-slice split of its outputs: the a-block's
+// V (FP32 when v_f32, else FP64; layout of ladder_pack_v) is packed into the
+// symmetric (rows: the block's npairs pairs, K = v(v+1)/2) and antisymmetric
+// (rows: its a < b pairs, K = v(v-1)/2) operands, written as BF16 slices in
+// tc_split's layout at Vp / Vm (bind them with tc_bind).
+int ladder_pack_v_split(stream_t s, int nv, int a0, int na, int npairs, const int* pairs,
+                        const int* cdp, const void* V, bool v_f32, void* Vp, void* Vm);
 // C(m,n) = alpha sum_k A(m,k) B(k,n) + beta C(m,n) over pre-split operands
 // (all with the same slice count): the K sum runs over up to TC_MAX_SEG
 // segments A[s]/B[s], s = 0, 1, ... (the first null A[s] ends the list), each
@@ -103,6 +115,10 @@ int tc_view(const TcOperand& parent, int64_t row0, int64_t rows, TcOperand* out)
 // (dm = 0: m*scm) and coloff(n) = (n % dn)*scn + (n / dn)*scn2 (dn = 0:
 // n*scn).  Stores are coalesced when scm == 1.
 constexpr int TC_MAX_SEG = 4;
+// Longest K one FP32 tensor-memory accumulator sums: FP64 outputs with a
+// longer K are computed in K slices whose partial products are added in FP64;
+// FP32 outputs are one accumulation, so callers keep their K within this.
+constexpr int64_t TC_ACC_K = 1024;
 struct TcGemm {
   int64_t m = 0, n = 0;
   double alpha = 1.0, beta = 0.0;
