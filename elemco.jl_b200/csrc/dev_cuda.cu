@@ -1326,15 +1326,17 @@ __global__ void __launch_bounds__(512, 1) triples_energy_kernel(
   int b = 0;
   for (int t = blockIdx.x; t < ntri; t += gridDim.x, ti += gridDim.x,
            b = (b + 1 == NB) ? 0 : b + 1) {
+    // NB-2 later orbits may still be in flight; this one has landed for this
+    // thread, and after the barrier for every thread, which has also finished
+    // evaluating the previous orbit, so its buffer can be refilled
+    cp_async_wait<NB - 2>();
+    __syncthreads();
     {
-      // into the buffer evaluated last iteration (released by its trailing barrier)
       const int S[3] = {nS[0], nS[1], nS[2]};
       origins(ti + gridDim.x, nS);
       if (ti < ntri) issue(b == 0 ? NB - 1 : b - 1, S);
       else cp_async_commit();
     }
-    cp_async_wait<NB - 1>();  // this orbit's copies have landed ...
-    __syncthreads();          // ... for every thread
     const unsigned char* base = tsm_raw + b * L::BUF;
     const T* cK = reinterpret_cast<const T*>(base);
     const T* cU = cK + L::CUBES;
@@ -1391,7 +1393,6 @@ __global__ void __launch_bounds__(512, 1) triples_energy_kernel(
       eK += wgt * ek;
       eY += wgt * ey;
     }
-    __syncthreads();  // buffer b is refilled by the next iteration's issue
   }
   cp_async_wait<0>();
   const double r0 = block_sum(eK, sh);
