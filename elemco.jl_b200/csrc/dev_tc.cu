@@ -33,21 +33,31 @@ namespace dev {
 
 namespace {
 
-constexpr int TM = 128, TN = 128, TK = 64;
+// Tiles: 128 rows (M) x TN columns (N), TN = 128 or TN_WIDE = 160 (chosen per
+// GEMM: 160 covers N = 300 or 318 in 320 columns where 128 needs 384), K = 64.
+constexpr int TM = 128, TK = 64, TN_WIDE = 160;
 constexpr int TILE_BYTES_A = TM * TK * 2;  // 16 KiB per slice
-constexpr int TILE_BYTES_B = TN * TK * 2;
-constexpr int RING_BYTES = 192 * 1024;
+constexpr int RING_BYTES = 216 * 1024;
 // longest K (in 64-wide k-blocks) one FP32 tensor-memory accumulator sums
 // before its partial product is handed to an FP64 reduction
 constexpr int KB_ACC = (int)(TC_ACC_K / TK);
 constexpr unsigned long long WAIT_NS = 1000000000ull;  // 1 s bound on every mbarrier wait
 
-template <int NSL>
+template <int NSL, int TN>
 struct TcCfg {
+  static constexpr int TILE_BYTES_B = TN * TK * 2;
   static constexpr int STAGE_BYTES = NSL * (TILE_BYTES_A + TILE_BYTES_B);
   static constexpr int STAGES = RING_BYTES / STAGE_BYTES;
   static constexpr int NPAIR = NSL == 3 ? 6 : 3;
   static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*barriers*/ + 1024 /*align*/;
+  // two TN-column accumulators; allocations are powers of two
+  static constexpr uint32_t TMEM_COLS = 2 * TN <= 256 ? 256 : 512;
+  // instruction descriptor: kind::f16, A/B BF16, D F32, both K-major, M=128, N=TN
+  static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) |
+                                    ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+  static_assert(TN % 16 == 0 && TN <= 256 && STAGES >= 2, "tile shape");
+  static_assert(SMEM_BYTES <= 227 * 1024, "shared memory");
+  static_assert(TILE_BYTES_B % 1024 == 0, "128-byte-swizzle tiles start on 1024 bytes");
 };
 // slice pairs (a, b): hi*hi, hi*mid, mid*hi, mid*mid, hi*lo, lo*hi (the first
 // three for NSL = 2)
@@ -112,15 +122,12 @@ __device__ __forceinline__ uint64_t umma_desc(const void* p) {
   return d;
 }
 
-// Instruction descriptor: kind::f16, A/B BF16, D F32, both K-major, M=128, N=128.
-constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) |
-                           ((uint32_t)(TM >> 4) << 24);
-
-__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t acc) {
+__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
+                                     uint32_t acc) {
   asm volatile(
       "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
       " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
-      "l"(da), "l"(db), "r"(IDESC), "r"(acc));
+      "l"(da), "l"(db), "r"(idesc), "r"(acc));
 }
 
 __device__ __forceinline__ void umma_commit(uint64_t* bar) {
@@ -132,14 +139,13 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
 // Persistent, warp-specialised kernel: gridDim.x CTAs (one per SM) loop over
 // work items (m-tile, n-tile, k-slice).  Warp 0 lane 0: TMA producer over a
 // STAGES-deep shared-memory ring (full/empty mbarriers).  Warp 1: owns the
-// 256-column tensor-memory allocation, lane 0 issues the MMAs into one of two
-// 128-column accumulators and commits.  Warps 2..9: epilogue, each reading
+// tensor-memory allocation, lane 0 issues the MMAs into one of two TN-column
+// accumulators and commits.  Warps 2..9: epilogue, each reading
 // the 32 accumulator lanes its warp index (mod 4) may access and one half of
 // the columns, writing C and releasing the accumulator, so the epilogue of
 // one tile overlaps the MMAs of the next.
-constexpr int EPI_WARPS = 8;  // two per TMEM lane quarter, 64 columns each
+constexpr int EPI_WARPS = 8;  // two per TMEM lane quarter, TN/2 columns each
 constexpr int THREADS_TC = 32 * (2 + EPI_WARPS);
-constexpr uint32_t TMEM_COLS_P = 2 * TN;
 
 // TMA descriptors of up to TC_MAX_SEG K segments, each read from its own k = 0.
 struct TcMaps {
@@ -242,15 +248,16 @@ __device__ __forceinline__ void prefetch_cols(const CT* C, int64_t rowoff, int64
   }
 }
 
-template <int NSL>
+template <int NSL, int TN>
 __global__ void __launch_bounds__(THREADS_TC, 1)
     mgemm_bf16_kernel(const __grid_constant__ TcMaps maps, TcOut out, int64_t M, int64_t N,
                       double alpha, double beta, const TcSegs segs, int kb_per_split,
                       int kblocks_total,
                       int64_t split_stride, int mtiles, int ntiles, int nsplit,
                       const TcMaps* __restrict__ mtab) {
-  using Cfg = TcCfg<NSL>;
+  using Cfg = TcCfg<NSL, TN>;
   constexpr int STAGES = Cfg::STAGES, STAGE_BYTES = Cfg::STAGE_BYTES;
+  constexpr int TILE_BYTES_B = Cfg::TILE_BYTES_B;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint8_t* tiles = smem;
@@ -280,7 +287,7 @@ __global__ void __launch_bounds__(THREADS_TC, 1)
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
                      smem_u32(tmem_slot)),
-                 "r"(TMEM_COLS_P));
+                 "r"(Cfg::TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
@@ -381,7 +388,7 @@ __global__ void __launch_bounds__(THREADS_TC, 1)
 #pragma unroll
             for (int kk = 0; kk < TK / 16; ++kk)
               if (kk < nkk)
-                umma(dcol, da + (uint64_t)(kk * 2), db + (uint64_t)(kk * 2),
+                umma(dcol, da + (uint64_t)(kk * 2), db + (uint64_t)(kk * 2), Cfg::IDESC,
                      (kb > 0 || p > 0 || kk > 0) ? 1u : 0u);
           }
           umma_commit(&empty[s]);
@@ -454,7 +461,7 @@ __global__ void __launch_bounds__(THREADS_TC, 1)
   __syncthreads();
   if (warp == 1) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem),
-                 "r"(TMEM_COLS_P));
+                 "r"(Cfg::TMEM_COLS));
   }
 }
 
@@ -538,11 +545,11 @@ __nv_bfloat16* split_buffer(size_t n) {
 // rows: extent of the map (rows past it read as zero); slice_stride in BF16
 // elements (default: rows * k_p, a dense [slice][row][k] block)
 int make_map(EncodeFn enc, CUtensorMap* m, const void* base, int64_t rows, int64_t k_p, int nsl,
-             int64_t slice_stride = 0) {
+             int64_t slice_stride = 0, int box_rows = TM) {
   if (slice_stride == 0) slice_stride = rows * k_p;
   cuuint64_t dims[3] = {(cuuint64_t)k_p, (cuuint64_t)rows, (cuuint64_t)nsl};
   cuuint64_t strides[2] = {(cuuint64_t)(k_p * 2), (cuuint64_t)(slice_stride * 2)};
-  cuuint32_t box[3] = {(cuuint32_t)TK, (cuuint32_t)TM, 1};
+  cuuint32_t box[3] = {(cuuint32_t)TK, (cuuint32_t)box_rows, 1};
   cuuint32_t es[3] = {1, 1, 1};
   CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(base), dims, strides,
                    box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
@@ -552,6 +559,27 @@ int make_map(EncodeFn enc, CUtensorMap* m, const void* base, int64_t rows, int64
 
 int64_t pad_rows(int64_t r) { return (r + TM - 1) / TM * TM; }
 int64_t pad_k(int64_t k) { return (k + TK - 1) / TK * TK; }
+
+// Tile width for N columns: 160 where N >= 160 and 160 pads N less than 128
+// does.  A B operand has N rows at least, so its 160-row map exists then.
+int tile_n(int64_t n) {
+  const int64_t p128 = (n + 127) / 128 * 128, p160 = (n + TN_WIDE - 1) / TN_WIDE * TN_WIDE;
+  return (n >= TN_WIDE && p160 < p128) ? TN_WIDE : 128;
+}
+
+// Both descriptors of an operand whose fields are set; the map's row extent
+// is `extent` (rows past it read as zero).
+int encode_operand(EncodeFn enc, TcOperand* op, int64_t extent) {
+  op->wide = false;
+  std::memset(op->map_w, 0, sizeof(op->map_w));
+  int e = make_map(enc, reinterpret_cast<CUtensorMap*>(op->map), op->base, extent, op->k_p,
+                   op->slices, op->slice_stride);
+  if (e || extent < TN_WIDE) return e;
+  e = make_map(enc, reinterpret_cast<CUtensorMap*>(op->map_w), op->base, extent, op->k_p,
+               op->slices, op->slice_stride, TN_WIDE);
+  op->wide = (e == 0);
+  return e;
+}
 
 // Segment k-block layout of nseg segments of K depths k[s] (padded to TK).
 TcSegs make_segs(int nseg, const int64_t* k) {
@@ -610,24 +638,29 @@ int split_count(int64_t tiles, int kbt) {
 
 // Launch over pre-split operands; S > 1 splits the combined k-blocks into S
 // slices that write FP64 partial products P[z][n][m] (column-major m x n).
-template <int NSL>
+template <int NSL, int TN>
+void set_smem_attr() {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(mgemm_bf16_kernel<NSL, TN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         TcCfg<NSL, TN>::SMEM_BYTES);
+    attr = true;
+  }
+}
+
+template <int NSL, int TN>
 int launch_tc(cudaStream_t st, const TcMaps& maps, const TcSegs& segs, int kbt, int64_t m,
               int64_t n, int64_t mp, int64_t np, double alpha, double beta, const TcOut& out,
               int S) {
-  using Cfg = TcCfg<NSL>;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(mgemm_bf16_kernel<NSL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         Cfg::SMEM_BYTES);
-    attr = true;
-  }
+  using Cfg = TcCfg<NSL, TN>;
+  set_smem_attr<NSL, TN>();
   const int mt = (int)(mp / TM), nt = (int)(np / TN);
   const int kps = (kbt + S - 1) / S;
   S = (kbt + kps - 1) / kps;
   const int64_t items = (int64_t)mt * nt * S;
   const unsigned grid = (unsigned)(items < 148 ? items : 148);
   if (S == 1) {
-    mgemm_bf16_kernel<NSL><<<grid, THREADS_TC, Cfg::SMEM_BYTES, st>>>(
+    mgemm_bf16_kernel<NSL, TN><<<grid, THREADS_TC, Cfg::SMEM_BYTES, st>>>(
         maps, out, m, n, alpha, beta, segs, kps, kbt, 0, mt, nt, 1, nullptr);
     note_launches(1);
     return (int)cudaGetLastError();
@@ -636,7 +669,7 @@ int launch_tc(cudaStream_t st, const TcMaps& maps, const TcSegs& segs, int kbt, 
   double* P = splitk_buffer((size_t)S * m * n);
   if (!P) return (int)cudaErrorMemoryAllocation;
   TcOut po{P, 1, m, 0, 0, 0, 0, 0};
-  mgemm_bf16_kernel<NSL><<<grid, THREADS_TC, Cfg::SMEM_BYTES, st>>>(
+  mgemm_bf16_kernel<NSL, TN><<<grid, THREADS_TC, Cfg::SMEM_BYTES, st>>>(
       maps, po, m, n, 1.0, 0.0, segs, kps, kbt, m * n, mt, nt, S, nullptr);
   note_launches(1);
   int e = (int)cudaGetLastError();
@@ -670,8 +703,7 @@ int tc_split(stream_t s, const double* src, int64_t rows, int64_t k, int64_t sr,
                (__nv_bfloat16*)dst);
   e = (int)cudaGetLastError();
   if (e) return e;
-  return make_map(enc, reinterpret_cast<CUtensorMap*>(op->map), dst, op->rows_p, op->k_p,
-                  slices);
+  return encode_operand(enc, op, op->rows_p);
 }
 
 int64_t tc_pad_rows(int64_t rows) { return pad_rows(rows); }
@@ -691,8 +723,7 @@ int tc_bind(void* dst, int64_t rows, int64_t k, int slices, TcOperand* op) {
   op->slices = slices;
   op->base = dst;
   op->slice_stride = op->rows_p * op->k_p;
-  return make_map(enc, reinterpret_cast<CUtensorMap*>(op->map), dst, op->rows_p, op->k_p,
-                  slices);
+  return encode_operand(enc, op, op->rows_p);
 }
 
 namespace {
@@ -781,8 +812,7 @@ int tc_view(const TcOperand& parent, int64_t row0, int64_t rows, TcOperand* out)
   out->rows = rows;
   out->rows_p = pad_rows(rows);
   out->base = (__nv_bfloat16*)parent.base + row0 * parent.k_p;
-  return make_map(enc, reinterpret_cast<CUtensorMap*>(out->map), out->base, rows, parent.k_p,
-                  parent.slices, parent.slice_stride);
+  return encode_operand(enc, out, rows);
 }
 
 int tc_gemm(stream_t s, const TcGemm& g) {
@@ -790,75 +820,88 @@ int tc_gemm(stream_t s, const TcGemm& g) {
   int64_t k[TC_MAX_SEG];
   const int ns = gemm_segments(g, k);
   if (ns == 0) return (int)cudaErrorInvalidValue;
+  bool wide = tile_n(g.n) == TN_WIDE;
+  for (int t = 0; t < ns; ++t) wide = wide && g.B[t]->wide;
+  const int tn = wide ? TN_WIDE : 128;
   TcMaps maps;
   for (int t = 0; t < TC_MAX_SEG; ++t) {
+    const TcOperand* b = g.B[t < ns ? t : 0];
     std::memcpy(&maps.a[t], g.A[t < ns ? t : 0]->map, sizeof(CUtensorMap));
-    std::memcpy(&maps.b[t], g.B[t < ns ? t : 0]->map, sizeof(CUtensorMap));
+    std::memcpy(&maps.b[t], wide ? b->map_w : b->map, sizeof(CUtensorMap));
   }
   const TcSegs segs = make_segs(ns, k);
   const int kbt = segs.kb_end[TC_MAX_SEG - 1];
   TcOut out{g.C, g.scm, g.scn, g.dn, g.scn2, g.dm, g.scm2, g.f32 ? 1 : 0};
-  const int64_t mp = pad_rows(g.m), np = pad_rows(g.n);
+  const int64_t mp = pad_rows(g.m), np = (g.n + tn - 1) / tn * tn;
   int S = 1;
-  if (!g.f32 && g.dn == 0 && g.dm == 0) S = split_count(mp / TM * (np / TN), kbt);
+  if (!g.f32 && g.dn == 0 && g.dm == 0) S = split_count(mp / TM * (np / tn), kbt);
+  cudaStream_t st = (cudaStream_t)s;
   if (g.A[0]->slices == 3)
-    return launch_tc<3>((cudaStream_t)s, maps, segs, kbt, g.m, g.n, mp, np, g.alpha, g.beta, out,
-                        S);
-  return launch_tc<2>((cudaStream_t)s, maps, segs, kbt, g.m, g.n, mp, np, g.alpha, g.beta, out,
-                      S);
+    return wide ? launch_tc<3, TN_WIDE>(st, maps, segs, kbt, g.m, g.n, mp, np, g.alpha, g.beta,
+                                        out, S)
+                : launch_tc<3, 128>(st, maps, segs, kbt, g.m, g.n, mp, np, g.alpha, g.beta, out,
+                                    S);
+  return wide ? launch_tc<2, TN_WIDE>(st, maps, segs, kbt, g.m, g.n, mp, np, g.alpha, g.beta, out,
+                                      S)
+              : launch_tc<2, 128>(st, maps, segs, kbt, g.m, g.n, mp, np, g.alpha, g.beta, out, S);
 }
 
 size_t tc_maps_bytes() { return sizeof(TcMaps); }
 
-int tc_maps_fill(int nseg, const TcOperand* const* A, const TcOperand* const* B, void* dst) {
-  if (nseg < 1 || nseg > TC_MAX_SEG || !A || !B || !dst) return (int)cudaErrorInvalidValue;
+int tc_maps_fill(int nseg, const TcOperand* const* A, const TcOperand* const* B, int64_t n,
+                 void* dst) {
+  if (nseg < 1 || nseg > TC_MAX_SEG || !A || !B || !dst || n <= 0)
+    return (int)cudaErrorInvalidValue;
+  const bool wide = tile_n(n) == TN_WIDE;
   for (int t = 0; t < nseg; ++t)
-    if (!A[t] || !B[t]) return (int)cudaErrorInvalidValue;
+    if (!A[t] || !B[t] || (wide && !B[t]->wide)) return (int)cudaErrorInvalidValue;
   TcMaps* m = reinterpret_cast<TcMaps*>(dst);
   for (int t = 0; t < TC_MAX_SEG; ++t) {
+    const TcOperand* b = B[t < nseg ? t : 0];
     std::memcpy(&m->a[t], A[t < nseg ? t : 0]->map, sizeof(CUtensorMap));
-    std::memcpy(&m->b[t], B[t < nseg ? t : 0]->map, sizeof(CUtensorMap));
+    std::memcpy(&m->b[t], wide ? b->map_w : b->map, sizeof(CUtensorMap));
   }
   return 0;
 }
+
+namespace {
+template <int NSL, int TN>
+void launch_batched(cudaStream_t st, const TcOut& out, const TcGemm& g, const TcSegs& segs,
+                    int kbt, int64_t c_stride, int mt, int nt, int batch, const void* mtab) {
+  using Cfg = TcCfg<NSL, TN>;
+  set_smem_attr<NSL, TN>();
+  const int64_t items = (int64_t)mt * nt * batch;
+  const unsigned grid = (unsigned)(items < 148 ? items : 148);
+  TcMaps dummy;
+  std::memset(&dummy, 0, sizeof(dummy));
+  mgemm_bf16_kernel<NSL, TN><<<grid, THREADS_TC, Cfg::SMEM_BYTES, st>>>(
+      dummy, out, g.m, g.n, g.alpha, g.beta, segs, kbt, kbt, c_stride, mt, nt, batch,
+      (const TcMaps*)mtab);
+}
+}  // namespace
 
 int tc_gemm_batched(stream_t s, const TcGemm& g, int batch, const void* mtab, int64_t c_stride) {
   if (g.m <= 0 || g.n <= 0 || batch <= 0) return 0;
   int64_t k[TC_MAX_SEG];
   const int ns = gemm_segments(g, k);
   if (ns == 0 || !mtab || ((uintptr_t)mtab & 63) != 0) return (int)cudaErrorInvalidValue;
+  // the tables were filled by tc_maps_fill with the same tile-width rule
+  const bool wide = tile_n(g.n) == TN_WIDE;
+  for (int t = 0; t < ns; ++t)
+    if (wide && !g.B[t]->wide) return (int)cudaErrorInvalidValue;
+  const int tn = wide ? TN_WIDE : 128;
   const TcSegs segs = make_segs(ns, k);
   const int kbt = segs.kb_end[TC_MAX_SEG - 1];
-  const int64_t mp = pad_rows(g.m), np = pad_rows(g.n);
-  const int mt = (int)(mp / TM), nt = (int)(np / TN);
-  const int64_t items = (int64_t)mt * nt * batch;
-  const unsigned grid = (unsigned)(items < 148 ? items : 148);
+  const int64_t mp = pad_rows(g.m), np = (g.n + tn - 1) / tn * tn;
+  const int mt = (int)(mp / TM), nt = (int)(np / tn);
   TcOut out{g.C, g.scm, g.scn, g.dn, g.scn2, g.dm, g.scm2, g.f32 ? 1 : 0};
-  TcMaps dummy;
-  std::memset(&dummy, 0, sizeof(dummy));
   cudaStream_t st = (cudaStream_t)s;
   if (g.A[0]->slices == 3) {
-    using Cfg = TcCfg<3>;
-    static bool attr = false;
-    if (!attr) {
-      cudaFuncSetAttribute(mgemm_bf16_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           Cfg::SMEM_BYTES);
-      attr = true;
-    }
-    mgemm_bf16_kernel<3><<<grid, THREADS_TC, Cfg::SMEM_BYTES, st>>>(
-        dummy, out, g.m, g.n, g.alpha, g.beta, segs, kbt, kbt, c_stride, mt, nt, batch,
-        (const TcMaps*)mtab);
+    if (wide) launch_batched<3, TN_WIDE>(st, out, g, segs, kbt, c_stride, mt, nt, batch, mtab);
+    else launch_batched<3, 128>(st, out, g, segs, kbt, c_stride, mt, nt, batch, mtab);
   } else {
-    using Cfg = TcCfg<2>;
-    static bool attr = false;
-    if (!attr) {
-      cudaFuncSetAttribute(mgemm_bf16_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           Cfg::SMEM_BYTES);
-      attr = true;
-    }
-    mgemm_bf16_kernel<2><<<grid, THREADS_TC, Cfg::SMEM_BYTES, st>>>(
-        dummy, out, g.m, g.n, g.alpha, g.beta, segs, kbt, kbt, c_stride, mt, nt, batch,
-        (const TcMaps*)mtab);
+    if (wide) launch_batched<2, TN_WIDE>(st, out, g, segs, kbt, c_stride, mt, nt, batch, mtab);
+    else launch_batched<2, 128>(st, out, g, segs, kbt, c_stride, mt, nt, batch, mtab);
   }
   note_launches(1);
   return (int)cudaGetLastError();
@@ -874,7 +917,6 @@ int gemm_strided_mixed(stream_t s, const Gemm& q) {
   EncodeFn enc = nullptr;
   int e = encode_fn(&enc);
   if (e) return e;
-  static_assert(TM == TN, "one padding rule for A and B");
   constexpr int NSL = 3;
   const int64_t m = q.m, n = q.n, k = q.k;
   const int64_t mp = pad_rows(m), np = pad_rows(n), kp = pad_k(k);
@@ -885,18 +927,24 @@ int gemm_strided_mixed(stream_t s, const Gemm& q) {
   cudaStream_t st = (cudaStream_t)s;
   launch_split(st, q.A, m, k, q.sam, q.sak, mp, kp, NSL, As);  // A(m,k) = A[m sam + k sak]
   launch_split(st, q.B, n, k, q.sbn, q.sbk, np, kp, NSL, Bs);  // B(k,n) = B[k sbk + n sbn]
+  // B rows are padded to 128; a 160-wide tile (tile_n) reads 160-row boxes
+  // from them (n >= 160 then, and the tiles end before np)
+  const int tn = tile_n(n);
+  const int64_t npt = (n + tn - 1) / tn * tn;
   TcMaps maps;
   if ((e = make_map(enc, &maps.a[0], As, mp, kp, NSL))) return e;
-  if ((e = make_map(enc, &maps.b[0], Bs, np, kp, NSL))) return e;
+  if ((e = make_map(enc, &maps.b[0], Bs, np, kp, NSL, 0, tn))) return e;
   for (int t = 1; t < TC_MAX_SEG; ++t) {
     maps.a[t] = maps.a[0];
     maps.b[t] = maps.b[0];
   }
   const TcSegs segs = make_segs(1, &k);
   const int kbt = (int)(kp / TK);
-  const int S = split_count((mp / TM) * (np / TN), kbt);
+  const int S = split_count((mp / TM) * (npt / tn), kbt);
   TcOut out{q.C, q.scm, q.scn, 0, 0, 0, 0, 0};
-  return launch_tc<NSL>(st, maps, segs, kbt, m, n, mp, np, q.alpha, q.beta, out, S);
+  if (tn == TN_WIDE)
+    return launch_tc<NSL, TN_WIDE>(st, maps, segs, kbt, m, n, mp, npt, q.alpha, q.beta, out, S);
+  return launch_tc<NSL, 128>(st, maps, segs, kbt, m, n, mp, npt, q.alpha, q.beta, out, S);
 }
 
 int gemm_mixed(stream_t s, char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha,

@@ -82,6 +82,10 @@ int gemm_strided_mixed(stream_t s, const Gemm& g);
 // ~2^-16 relative.
 struct TcOperand {
   alignas(64) unsigned char map[128];
+  // the same operand with 160-row boxes, for 160-column tiles when it is the
+  // B operand (encoded, and wide set, when its row extent is at least 160)
+  alignas(64) unsigned char map_w[128];
+  bool wide = false;
   int64_t rows = 0, rows_p = 0, k = 0, k_p = 0;
   int slices = 0;
   void* base = nullptr;        // first BF16 element of row 0, slice 0
@@ -135,7 +139,9 @@ int tc_gemm(stream_t s, const TcGemm& g);
 // the host from nseg segments A[s]/B[s]) and writing C + b*c_stride through
 // g's index map.  One launch.
 size_t tc_maps_bytes();
-int tc_maps_fill(int nseg, const TcOperand* const* A, const TcOperand* const* B, void* host_dst);
+// n: the GEMM's column count (it selects the tile width, as in tc_gemm_batched).
+int tc_maps_fill(int nseg, const TcOperand* const* A, const TcOperand* const* B, int64_t n,
+                 void* host_dst);
 int tc_gemm_batched(stream_t s, const TcGemm& g, int batch, const void* mtab, int64_t c_stride);
 
 // out = alpha * permute(in) + beta * out.  in has rank nd with dims

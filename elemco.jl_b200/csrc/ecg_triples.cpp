@@ -174,7 +174,8 @@ void fill_tables(Ctx& c, const TriplesOps& ops, const SplitAmps* Sp, const std::
       const bool rows_a = p0.scm == 1;
       const dev::TcOperand* A[4] = {rows_a ? T0 : V0, rows_a ? T1 : V1, ovoo[q][0], ovoo[q][1]};
       const dev::TcOperand* B[4] = {rows_a ? V0 : T0, rows_a ? V1 : T1, ovoo[q][2], ovoo[q][3]};
-      check(dev::tc_maps_fill(4, A, B, kt.mtab.data() + (q * nt + t) * mb), "maps");
+      check(dev::tc_maps_fill(4, A, B, rows_a ? v2 : v, kt.mtab.data() + (q * nt + t) * mb),
+            "maps");
     }
   }
 }

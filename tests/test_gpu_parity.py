@@ -265,3 +265,27 @@ def test_mixed_precision_triples():
         lmx = c.lambda_pert_t(r["T1"], r["T2"], lr["U1"], lr["U2"])
     assert abs(emx[0] - e64[0]) < 1e-8 and abs(emx[1] - e64[1]) < 1e-8
     assert abs(lmx[0] - l64[0]) < 1e-8
+
+
+def test_mixed_precision_triples_wide_tiles():
+    """v = 300: the (T) GEMMs whose columns run over v use 160-column
+    tensor-core tiles (N = 300 in 320 columns instead of 384); (T), [T] and
+    Lambda-(T) from MP2 amplitudes agree with FP64 to 2e-5 relative, the
+    precision of the two-slice BF16 products (~2^-16; a tile that dropped or
+    misplaced columns would be off by O(1))."""
+    import ecgpu
+    from ecgpu.synthetic import make_system
+    no = 3
+    B, h1, e0, _ = make_system(no, 300, 400)
+    with ecgpu.Context(0) as c:
+        c.set_system(B, h1, e0, no)
+        _, T1, T2 = c.mp2()
+        U1, U2 = 2.0 * T1, 2.0 * T2
+        e64 = c.pert_t(T1, T2)
+        l64 = c.lambda_pert_t(T1, T2, U1, U2)
+        c.set_precision(ecgpu.ECG_PREC_MIXED)
+        emx = c.pert_t(T1, T2)
+        lmx = c.lambda_pert_t(T1, T2, U1, U2)
+    assert e64[0] < -1e-6
+    for x, ref in ((emx[0], e64[0]), (emx[1], e64[1]), (lmx[0], l64[0])):
+        assert abs(x - ref) < 2e-5 * abs(ref), (x, ref)
