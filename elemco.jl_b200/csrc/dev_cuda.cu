@@ -1217,12 +1217,12 @@ struct EnergySmem {
 };
 
 // Batch item y = blockIdx.y reads K + y*kstride (and KU), its denominator
-// shift and terms from eijk_tab / tt_tab when given (else eijk0 / tt0), and
+// shift and terms from eijk_tab[y] / tt_tab[y], and
 // leaves its partial sums at part[(2y + c) * gridDim.x + blockIdx.x].
 template <typename T, bool HAS_U>
 __global__ void __launch_bounds__(512, 1) triples_energy_kernel(
-    int nv, const T* __restrict__ K, const T* __restrict__ KU, int64_t kstride, double eijk0,
-    const double* __restrict__ eijk_tab, const double* __restrict__ ev, TriplesTerms tt0,
+    int nv, const T* __restrict__ K, const T* __restrict__ KU, int64_t kstride,
+    const double* __restrict__ eijk_tab, const double* __restrict__ ev,
     const TriplesTerms* __restrict__ tt_tab, const int* __restrict__ tri, int ntri,
     double* part) {
   using L = EnergySmem<T, HAS_U>;
@@ -1230,8 +1230,8 @@ __global__ void __launch_bounds__(512, 1) triples_energy_kernel(
   const int y = blockIdx.y;
   K += (int64_t)y * kstride;
   if (HAS_U) KU += (int64_t)y * kstride;
-  const TriplesTerms tt = tt_tab ? tt_tab[y] : tt0;
-  const double eijk = eijk_tab ? eijk_tab[y] : eijk0;
+  const TriplesTerms tt = tt_tab[y];
+  const double eijk = eijk_tab[y];
   extern __shared__ __align__(16) unsigned char tsm_raw[];
   __shared__ double sh[32];
   const int v = nv, tid = threadIdx.x;
@@ -1422,12 +1422,13 @@ static int64_t energy_grid(int nv) {
 
 int64_t triples_energy_scratch_len(int nv, int nitems) { return 2 * energy_grid(nv) * nitems; }
 
-static int launch_energy(cudaStream_t st, int nv, int nitems, const void* K, const void* KU,
-                         int64_t kstride, bool k_f32, double eijk0, const double* eijk_tab,
-                         const double* ev, const TriplesTerms& tt0, const TriplesTerms* tt_tab,
-                         const int* tri, double* scratch, double* out) {
+int triples_energy_batched(stream_t s, int nv, int nitems, const void* K, const void* KU,
+                           int64_t kstride, bool k_f32, const double* eijk_tab, const double* ev,
+                           const TriplesTerms* tt_tab, const int* tri, double* scratch,
+                           double* out) {
   const int64_t ntri = triples_cube_count(nv);
-  if (nv > 1290 || nitems <= 0 || nitems > 65535) return (int)cudaErrorInvalidValue;
+  if (nv > 1290 || nitems <= 0 || nitems > 65535 || !eijk_tab || !tt_tab)
+    return (int)cudaErrorInvalidValue;
   const int g = (int)energy_grid(nv);
   static bool attr = false;
   if (!attr) {
@@ -1445,39 +1446,30 @@ static int launch_energy(cudaStream_t st, int nv, int nitems, const void* K, con
                          EnergySmem<float, true>::BYTES);
     attr = true;
   }
+  cudaStream_t st = (cudaStream_t)s;
   const dim3 grid((unsigned)g, (unsigned)nitems);
   if (k_f32) {
     if (KU)
       triples_energy_kernel<float, true><<<grid, 512, EnergySmem<float, true>::BYTES, st>>>(
-          nv, (const float*)K, (const float*)KU, kstride, eijk0, eijk_tab, ev, tt0, tt_tab, tri,
-          (int)ntri, scratch);
+          nv, (const float*)K, (const float*)KU, kstride, eijk_tab, ev, tt_tab, tri, (int)ntri,
+          scratch);
     else
       triples_energy_kernel<float, false><<<grid, 512, EnergySmem<float, false>::BYTES, st>>>(
-          nv, (const float*)K, nullptr, kstride, eijk0, eijk_tab, ev, tt0, tt_tab, tri,
-          (int)ntri, scratch);
+          nv, (const float*)K, nullptr, kstride, eijk_tab, ev, tt_tab, tri, (int)ntri, scratch);
   } else {
     if (KU)
       triples_energy_kernel<double, true><<<grid, 512, EnergySmem<double, true>::BYTES, st>>>(
-          nv, (const double*)K, (const double*)KU, kstride, eijk0, eijk_tab, ev, tt0, tt_tab,
-          tri, (int)ntri, scratch);
+          nv, (const double*)K, (const double*)KU, kstride, eijk_tab, ev, tt_tab, tri,
+          (int)ntri, scratch);
     else
       triples_energy_kernel<double, false><<<grid, 512, EnergySmem<double, false>::BYTES, st>>>(
-          nv, (const double*)K, nullptr, kstride, eijk0, eijk_tab, ev, tt0, tt_tab, tri,
-          (int)ntri, scratch);
+          nv, (const double*)K, nullptr, kstride, eijk_tab, ev, tt_tab, tri, (int)ntri,
+          scratch);
   }
   int e = launched();
   if (e) return e;
   final_sum_pairs_kernel<<<2 * nitems, 256, 0, st>>>(g, scratch, out);
   return launched();
-}
-
-int triples_energy_batched(stream_t s, int nv, int nitems, const void* K, const void* KU,
-                           int64_t kstride, bool k_f32, const double* eijk_tab, const double* ev,
-                           const TriplesTerms* tt_tab, const int* tri, double* scratch,
-                           double* out) {
-  TriplesTerms none{};
-  return launch_energy((cudaStream_t)s, nv, nitems, K, KU, kstride, k_f32, 0.0, eijk_tab, ev,
-                       none, tt_tab, tri, scratch, out);
 }
 
 }  // namespace dev
