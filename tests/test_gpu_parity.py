@@ -289,3 +289,37 @@ def test_mixed_precision_triples_wide_tiles():
     assert e64[0] < -1e-6
     for x, ref in ((emx[0], e64[0]), (emx[1], e64[1]), (lmx[0], l64[0])):
         assert abs(x - ref) < 2e-5 * abs(ref), (x, ref)
+
+
+@pytest.mark.parametrize("no", [1, 2])
+def test_pert_t_few_occupied(no):
+    """(T), [T] and Lambda-(T) with one and two occupied orbitals (no triplet
+    at all, or only i = j < k and i < j = k) on a synthetic system with
+    v = 20 (ragged 8^3 cubes), FP64 against the oracle (cc_triples.jl:39-295),
+    mixed against FP64; with one occupied orbital every energy is 0."""
+    import ecgpu
+    from ecgpu.synthetic import make_system
+    B, h1, e0, _ = make_system(no, 20, 30)
+    S = O.System.from_df(np.ascontiguousarray(B.transpose(2, 0, 1)), h1, e0, no)
+    f = O.gen_fock(S)
+    rng = np.random.default_rng(11)
+    with ecgpu.Context(0) as c:
+        c.set_system(B, h1, e0, no)
+        _, T1, T2 = c.mp2()
+        U1 = T1 + 0.01 * rng.standard_normal(T1.shape)
+        Y = 0.01 * rng.standard_normal(T2.shape)
+        U2 = np.asfortranarray(T2 + Y + Y.transpose(1, 0, 3, 2))
+        et, etb = c.pert_t(T1, T2)
+        lt, ltb = c.lambda_pert_t(T1, T2, U1, U2)
+        c.set_precision(ecgpu.ECG_PREC_MIXED)
+        mt, mtb = c.pert_t(T1, T2)
+    eto, etbo = O.pert_t(S, T1, T2, f)
+    lto, ltbo = O.lambda_pert_t(S, T1, T2, U1, U2, f)
+    if no == 1:
+        assert et == etb == lt == ltb == mt == mtb == 0.0
+        assert eto == etbo == lto == ltbo == 0.0
+        return
+    assert et < -1e-8
+    assert abs(et - eto) < 1e-13 and abs(etb - etbo) < 1e-13
+    assert abs(lt - lto) < 1e-13 and abs(ltb - ltbo) < 1e-13
+    assert abs(mt - et) < 2e-5 * abs(et) and abs(mtb - etb) < 2e-5 * abs(etb)
