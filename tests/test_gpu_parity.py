@@ -247,6 +247,28 @@ def test_mixed_precision_solve_within_1_uEh(dc):
     assert dE < 1e-6, dE
 
 
+def test_mixed_precision_solve_wide_ladder_tiles():
+    """o = 24, v = 64: the ladder contractions have N = o(o+1)/2 = 300 and
+    o(o-1)/2 = 276 columns and run on 160-column tensor-core tiles, with V
+    written in FP32 and packed straight into BF16 slices; the mixed CCSD
+    energy (after FP64 refinement) is within 1 microhartree of FP64."""
+    import ecgpu
+    from ecgpu.synthetic import make_system
+    no = 24
+    B, h1, e0, _ = make_system(no, 64, 128)
+    out = {}
+    for prec in (ecgpu.ECG_PREC_FP64, ecgpu.ECG_PREC_MIXED):
+        with ecgpu.Context(0) as c:
+            c.set_precision(prec)
+            c.set_system(B, h1, e0, no)
+            _, T1, T2 = c.mp2()
+            r = c.cc_solve(T1, T2)
+            assert r["converged"]
+            out[prec] = r["E"]
+    dE = abs(out[ecgpu.ECG_PREC_MIXED] - out[ecgpu.ECG_PREC_FP64])
+    assert dE < 1e-6, dE
+
+
 def test_mixed_precision_triples():
     """(T) and Lambda-(T) with split-BF16 tensor-core W products agree with FP64
     to 1e-8 Eh on the (H2O)_3/cc-pVDZ-sized system."""
