@@ -33,9 +33,12 @@ namespace dev {
 
 namespace {
 
-// Tiles: 128 rows (M) x TN columns (N), TN = 128 or TN_WIDE = 160 (chosen per
-// GEMM: 160 covers N = 300 or 318 in 320 columns where 128 needs 384), K = 64.
-constexpr int TM = 128, TK = 64, TN_WIDE = 160;
+// Tiles: 128 rows (M) x TN columns (N), K = 64; TN = 128, TN_WIDE = 160 or
+// TN_XWIDE = 256, chosen per GEMM by tile_n: 160 covers N = 300 or 318 in 320
+// columns where 128 needs 384; 256 (two-slice operands only: two stages of
+// 96 KiB) halves the A-operand traffic per MMA where it pads N by at most 2%
+// more than 128 does.
+constexpr int TM = 128, TK = 64, TN_WIDE = 160, TN_XWIDE = 256;
 constexpr int TILE_BYTES_A = TM * TK * 2;  // 16 KiB per slice
 constexpr int RING_BYTES = 216 * 1024;
 // longest K (in 64-wide k-blocks) one FP32 tensor-memory accumulator sums
@@ -560,24 +563,40 @@ int make_map(EncodeFn enc, CUtensorMap* m, const void* base, int64_t rows, int64
 int64_t pad_rows(int64_t r) { return (r + TM - 1) / TM * TM; }
 int64_t pad_k(int64_t k) { return (k + TK - 1) / TK * TK; }
 
-// Tile width for N columns: 160 where N >= 160 and 160 pads N less than 128
-// does.  A B operand has N rows at least, so its 160-row map exists then.
-int tile_n(int64_t n) {
+// Tile width for N columns of operands with nsl slices: 256 (two slices,
+// N >= 256) where it pads N by at most 2% more than 128 does, else 160
+// (N >= 160) where it pads N less than 128, else 128.  A B operand has N rows
+// at least, so the map of the chosen box exists.
+int tile_n(int64_t n, int nsl) {
   const int64_t p128 = (n + 127) / 128 * 128, p160 = (n + TN_WIDE - 1) / TN_WIDE * TN_WIDE;
+  const int64_t p256 = (n + TN_XWIDE - 1) / TN_XWIDE * TN_XWIDE;
+  if (nsl == 2 && n >= TN_XWIDE && p256 * 50 <= p128 * 51) return TN_XWIDE;
   return (n >= TN_WIDE && p160 < p128) ? TN_WIDE : 128;
 }
 
-// Both descriptors of an operand whose fields are set; the map's row extent
+// The B-operand descriptor for tile width tn, or nullptr if not encoded.
+const unsigned char* b_map(const TcOperand* b, int tn) {
+  if (tn == TN_XWIDE) return b->xwide ? b->map_x : nullptr;
+  if (tn == TN_WIDE) return b->wide ? b->map_w : nullptr;
+  return b->map;
+}
+
+// All descriptors of an operand whose fields are set; the maps' row extent
 // is `extent` (rows past it read as zero).
 int encode_operand(EncodeFn enc, TcOperand* op, int64_t extent) {
-  op->wide = false;
+  op->wide = op->xwide = false;
   std::memset(op->map_w, 0, sizeof(op->map_w));
+  std::memset(op->map_x, 0, sizeof(op->map_x));
   int e = make_map(enc, reinterpret_cast<CUtensorMap*>(op->map), op->base, extent, op->k_p,
                    op->slices, op->slice_stride);
   if (e || extent < TN_WIDE) return e;
   e = make_map(enc, reinterpret_cast<CUtensorMap*>(op->map_w), op->base, extent, op->k_p,
                op->slices, op->slice_stride, TN_WIDE);
   op->wide = (e == 0);
+  if (e || extent < TN_XWIDE) return e;
+  e = make_map(enc, reinterpret_cast<CUtensorMap*>(op->map_x), op->base, extent, op->k_p,
+               op->slices, op->slice_stride, TN_XWIDE);
+  op->xwide = (e == 0);
   return e;
 }
 
@@ -820,14 +839,14 @@ int tc_gemm(stream_t s, const TcGemm& g) {
   int64_t k[TC_MAX_SEG];
   const int ns = gemm_segments(g, k);
   if (ns == 0) return (int)cudaErrorInvalidValue;
-  bool wide = tile_n(g.n) == TN_WIDE;
-  for (int t = 0; t < ns; ++t) wide = wide && g.B[t]->wide;
-  const int tn = wide ? TN_WIDE : 128;
+  const int nsl = g.A[0]->slices;
+  int tn = tile_n(g.n, nsl);
+  for (int t = 0; t < ns; ++t)
+    if (!b_map(g.B[t], tn)) tn = 128;
   TcMaps maps;
   for (int t = 0; t < TC_MAX_SEG; ++t) {
-    const TcOperand* b = g.B[t < ns ? t : 0];
     std::memcpy(&maps.a[t], g.A[t < ns ? t : 0]->map, sizeof(CUtensorMap));
-    std::memcpy(&maps.b[t], wide ? b->map_w : b->map, sizeof(CUtensorMap));
+    std::memcpy(&maps.b[t], b_map(g.B[t < ns ? t : 0], tn), sizeof(CUtensorMap));
   }
   const TcSegs segs = make_segs(ns, k);
   const int kbt = segs.kb_end[TC_MAX_SEG - 1];
@@ -836,14 +855,19 @@ int tc_gemm(stream_t s, const TcGemm& g) {
   int S = 1;
   if (!g.f32 && g.dn == 0 && g.dm == 0) S = split_count(mp / TM * (np / tn), kbt);
   cudaStream_t st = (cudaStream_t)s;
-  if (g.A[0]->slices == 3)
-    return wide ? launch_tc<3, TN_WIDE>(st, maps, segs, kbt, g.m, g.n, mp, np, g.alpha, g.beta,
-                                        out, S)
-                : launch_tc<3, 128>(st, maps, segs, kbt, g.m, g.n, mp, np, g.alpha, g.beta, out,
-                                    S);
-  return wide ? launch_tc<2, TN_WIDE>(st, maps, segs, kbt, g.m, g.n, mp, np, g.alpha, g.beta, out,
-                                      S)
-              : launch_tc<2, 128>(st, maps, segs, kbt, g.m, g.n, mp, np, g.alpha, g.beta, out, S);
+  if (nsl == 3)
+    return tn == TN_WIDE
+               ? launch_tc<3, TN_WIDE>(st, maps, segs, kbt, g.m, g.n, mp, np, g.alpha, g.beta,
+                                       out, S)
+               : launch_tc<3, 128>(st, maps, segs, kbt, g.m, g.n, mp, np, g.alpha, g.beta, out,
+                                   S);
+  if (tn == TN_XWIDE)
+    return launch_tc<2, TN_XWIDE>(st, maps, segs, kbt, g.m, g.n, mp, np, g.alpha, g.beta, out,
+                                  S);
+  return tn == TN_WIDE
+             ? launch_tc<2, TN_WIDE>(st, maps, segs, kbt, g.m, g.n, mp, np, g.alpha, g.beta, out,
+                                     S)
+             : launch_tc<2, 128>(st, maps, segs, kbt, g.m, g.n, mp, np, g.alpha, g.beta, out, S);
 }
 
 size_t tc_maps_bytes() { return sizeof(TcMaps); }
@@ -852,14 +876,15 @@ int tc_maps_fill(int nseg, const TcOperand* const* A, const TcOperand* const* B,
                  void* dst) {
   if (nseg < 1 || nseg > TC_MAX_SEG || !A || !B || !dst || n <= 0)
     return (int)cudaErrorInvalidValue;
-  const bool wide = tile_n(n) == TN_WIDE;
   for (int t = 0; t < nseg; ++t)
-    if (!A[t] || !B[t] || (wide && !B[t]->wide)) return (int)cudaErrorInvalidValue;
+    if (!A[t] || !B[t]) return (int)cudaErrorInvalidValue;
+  const int tn = tile_n(n, A[0]->slices);
+  for (int t = 0; t < nseg; ++t)
+    if (!b_map(B[t], tn)) return (int)cudaErrorInvalidValue;
   TcMaps* m = reinterpret_cast<TcMaps*>(dst);
   for (int t = 0; t < TC_MAX_SEG; ++t) {
-    const TcOperand* b = B[t < nseg ? t : 0];
     std::memcpy(&m->a[t], A[t < nseg ? t : 0]->map, sizeof(CUtensorMap));
-    std::memcpy(&m->b[t], wide ? b->map_w : b->map, sizeof(CUtensorMap));
+    std::memcpy(&m->b[t], b_map(B[t < nseg ? t : 0], tn), sizeof(CUtensorMap));
   }
   return 0;
 }
@@ -886,22 +911,27 @@ int tc_gemm_batched(stream_t s, const TcGemm& g, int batch, const void* mtab, in
   const int ns = gemm_segments(g, k);
   if (ns == 0 || !mtab || ((uintptr_t)mtab & 63) != 0) return (int)cudaErrorInvalidValue;
   // the tables were filled by tc_maps_fill with the same tile-width rule
-  const bool wide = tile_n(g.n) == TN_WIDE;
+  const int nsl = g.A[0]->slices;
+  const int tn = tile_n(g.n, nsl);
   for (int t = 0; t < ns; ++t)
-    if (wide && !g.B[t]->wide) return (int)cudaErrorInvalidValue;
-  const int tn = wide ? TN_WIDE : 128;
+    if (!b_map(g.B[t], tn)) return (int)cudaErrorInvalidValue;
   const TcSegs segs = make_segs(ns, k);
   const int kbt = segs.kb_end[TC_MAX_SEG - 1];
   const int64_t mp = pad_rows(g.m), np = (g.n + tn - 1) / tn * tn;
   const int mt = (int)(mp / TM), nt = (int)(np / tn);
   TcOut out{g.C, g.scm, g.scn, g.dn, g.scn2, g.dm, g.scm2, g.f32 ? 1 : 0};
   cudaStream_t st = (cudaStream_t)s;
-  if (g.A[0]->slices == 3) {
-    if (wide) launch_batched<3, TN_WIDE>(st, out, g, segs, kbt, c_stride, mt, nt, batch, mtab);
-    else launch_batched<3, 128>(st, out, g, segs, kbt, c_stride, mt, nt, batch, mtab);
+  if (nsl == 3) {
+    if (tn == TN_WIDE)
+      launch_batched<3, TN_WIDE>(st, out, g, segs, kbt, c_stride, mt, nt, batch, mtab);
+    else
+      launch_batched<3, 128>(st, out, g, segs, kbt, c_stride, mt, nt, batch, mtab);
+  } else if (tn == TN_XWIDE) {
+    launch_batched<2, TN_XWIDE>(st, out, g, segs, kbt, c_stride, mt, nt, batch, mtab);
+  } else if (tn == TN_WIDE) {
+    launch_batched<2, TN_WIDE>(st, out, g, segs, kbt, c_stride, mt, nt, batch, mtab);
   } else {
-    if (wide) launch_batched<2, TN_WIDE>(st, out, g, segs, kbt, c_stride, mt, nt, batch, mtab);
-    else launch_batched<2, 128>(st, out, g, segs, kbt, c_stride, mt, nt, batch, mtab);
+    launch_batched<2, 128>(st, out, g, segs, kbt, c_stride, mt, nt, batch, mtab);
   }
   note_launches(1);
   return (int)cudaGetLastError();
@@ -929,7 +959,7 @@ int gemm_strided_mixed(stream_t s, const Gemm& q) {
   launch_split(st, q.B, n, k, q.sbn, q.sbk, np, kp, NSL, Bs);  // B(k,n) = B[k sbk + n sbn]
   // B rows are padded to 128; a 160-wide tile (tile_n) reads 160-row boxes
   // from them (n >= 160 then, and the tiles end before np)
-  const int tn = tile_n(n);
+  const int tn = tile_n(n, NSL);
   const int64_t npt = (n + tn - 1) / tn * tn;
   TcMaps maps;
   if ((e = make_map(enc, &maps.a[0], As, mp, kp, NSL))) return e;

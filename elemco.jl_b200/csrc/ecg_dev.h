@@ -82,10 +82,12 @@ int gemm_strided_mixed(stream_t s, const Gemm& g);
 // ~2^-16 relative.
 struct TcOperand {
   alignas(64) unsigned char map[128];
-  // the same operand with 160-row boxes, for 160-column tiles when it is the
-  // B operand (encoded, and wide set, when its row extent is at least 160)
+  // the same operand with 160- and 256-row boxes, for 160- and 256-column
+  // tiles when it is the B operand (each encoded, and its flag set, when the
+  // row extent is at least the box)
   alignas(64) unsigned char map_w[128];
-  bool wide = false;
+  alignas(64) unsigned char map_x[128];
+  bool wide = false, xwide = false;
   int64_t rows = 0, rows_p = 0, k = 0, k_p = 0;
   int slices = 0;
   void* base = nullptr;        // first BF16 element of row 0, slice 0
