@@ -8,10 +8,10 @@
 // x0y0 x0y1 x1y0 (~2^-16, for sums whose element errors average out, such as
 // the (T) energy).
 //
-// Kernel: persistent, one CTA per SM over 128x128 output tiles.  TMA loads
-// (3-D tensor maps: k, row, slice; 64x128 boxes, 128-byte swizzle) feed a
-// ring of 192 KiB (2 stages of 3 slices or 3 stages of 2 slices);
-// tcgen05.mma kind::f16 (BF16 x BF16 -> F32, M=128 N=128 K=16) accumulates in
+// Kernel: persistent, one CTA per SM over 128 x TN output tiles (TN = 128,
+// 160 or 256).  TMA loads (3-D tensor maps: k, row, slice; 64-wide boxes of
+// 128 or TN rows, 128-byte swizzle) feed a ring of at most 216 KiB (2 or 3
+// stages); tcgen05.mma kind::f16 (BF16 x BF16 -> F32, M=128 N=TN K=16) accumulates in
 // one of two tensor-memory accumulators while eight epilogue warps drain the
 // other with tcgen05.ld and write C (FP64 or FP32, through an index map whose
 // rows run along the lanes).  Every mbarrier wait is bounded (1 s); on
