@@ -563,15 +563,17 @@ int make_map(EncodeFn enc, CUtensorMap* m, const void* base, int64_t rows, int64
 int64_t pad_rows(int64_t r) { return (r + TM - 1) / TM * TM; }
 int64_t pad_k(int64_t k) { return (k + TK - 1) / TK * TK; }
 
-// Tile width for N columns of operands with nsl slices: 256 (two slices,
-// N >= 256) where it pads N by at most 2% more than 128 does, else 160
-// (N >= 160) where it pads N less than 128, else 128.  A B operand has N rows
-// at least, so the map of the chosen box exists.
+// Tile width for N columns of operands with nsl slices: the widest of 256
+// (two slices only) and 160 that pads N by at most 2% more than 128 does (and
+// N >= the width), else 128.  Wider tiles read fewer operand bytes per MMA.
+// A B operand has N rows at least, so the map of the chosen box exists; a
+// last tile reaching past the operand's rows reads zeros (TMA out-of-bounds
+// fill).
 int tile_n(int64_t n, int nsl) {
   const int64_t p128 = (n + 127) / 128 * 128, p160 = (n + TN_WIDE - 1) / TN_WIDE * TN_WIDE;
   const int64_t p256 = (n + TN_XWIDE - 1) / TN_XWIDE * TN_XWIDE;
   if (nsl == 2 && n >= TN_XWIDE && p256 * 50 <= p128 * 51) return TN_XWIDE;
-  return (n >= TN_WIDE && p160 < p128) ? TN_WIDE : 128;
+  return (n >= TN_WIDE && p160 * 50 <= p128 * 51) ? TN_WIDE : 128;
 }
 
 // The B-operand descriptor for tile width tn, or nullptr if not encoded.
@@ -957,8 +959,8 @@ int gemm_strided_mixed(stream_t s, const Gemm& q) {
   cudaStream_t st = (cudaStream_t)s;
   launch_split(st, q.A, m, k, q.sam, q.sak, mp, kp, NSL, As);  // A(m,k) = A[m sam + k sak]
   launch_split(st, q.B, n, k, q.sbn, q.sbk, np, kp, NSL, Bs);  // B(k,n) = B[k sbk + n sbn]
-  // B rows are padded to 128; a 160-wide tile (tile_n) reads 160-row boxes
-  // from them (n >= 160 then, and the tiles end before np)
+  // B rows are padded to 128; a wider tile (tile_n) reads 160-row boxes from
+  // them (n >= 160 then; rows past np read as zero)
   const int tn = tile_n(n, NSL);
   const int64_t npt = (n + tn - 1) / tn * tn;
   TcMaps maps;
