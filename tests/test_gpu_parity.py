@@ -247,15 +247,17 @@ def test_mixed_precision_solve_within_1_uEh(dc):
     assert dE < 1e-6, dE
 
 
-def test_mixed_precision_solve_wide_ladder_tiles():
-    """o = 24, v = 64: the ladder contractions have N = o(o+1)/2 = 300 and
+@pytest.mark.parametrize("no,nq", [(24, 128), (13, 30)])
+def test_mixed_precision_solve_wide_ladder_tiles(no, nq):
+    """v = 64.  o = 24: the ladder contractions have N = o(o+1)/2 = 300 and
     o(o-1)/2 = 276 columns and run on 160-column tensor-core tiles, with V
-    written in FP32 and packed straight into BF16 slices; the mixed CCSD
-    energy (after FP64 refinement) is within 1 microhartree of FP64."""
+    written in FP32 by the tensor cores and packed straight into BF16 slices.
+    o = 13, nQ = 30: the V build is below the tensor-core size rule, so the
+    FP64 V is packed into BF16 slices.  The mixed CCSD energy (after FP64
+    refinement) is within 1 microhartree of FP64."""
     import ecgpu
     from ecgpu.synthetic import make_system
-    no = 24
-    B, h1, e0, _ = make_system(no, 64, 128)
+    B, h1, e0, _ = make_system(no, 64, nq)
     out = {}
     for prec in (ecgpu.ECG_PREC_FP64, ecgpu.ECG_PREC_MIXED):
         with ecgpu.Context(0) as c:
