@@ -428,14 +428,18 @@ double* splitk_buffer(size_t n) {
   return g_splitk;
 }
 
-__global__ void splitk_reduce_kernel(int64_t m, int64_t n, int S, const double* __restrict__ P,
+// C = alpha sum_z P[z] + beta C, the partials (FP64, or FP32 for the
+// tensor-core GEMM, whose partials are FP32 accumulations) summed in FP64 in
+// slice order.
+template <typename PT>
+__global__ void splitk_reduce_kernel(int64_t m, int64_t n, int S, const PT* __restrict__ P,
                                      double alpha, double beta, double* C, int64_t scm,
                                      int64_t scn) {
   const int64_t total = m * n;
   for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
        idx += (int64_t)gridDim.x * blockDim.x) {
     double acc = 0.0;
-    for (int z = 0; z < S; ++z) acc += P[z * total + idx];
+    for (int z = 0; z < S; ++z) acc += (double)P[z * total + idx];
     double* c = C + (idx % m) * scm + (idx / m) * scn;
     double v = alpha * acc;
     if (beta != 0.0) v += beta * *c;
@@ -507,6 +511,13 @@ int gemm_splitk_noalloc(stream_t s, char ta, char tb, int64_t m, int64_t n, int6
 
 int splitk_reduce(stream_t s, int64_t m, int64_t n, int S, const double* P, double alpha,
                   double beta, double* C, int64_t scm, int64_t scn) {
+  splitk_reduce_kernel<<<grid_for(m * n), 256, 0, (cudaStream_t)s>>>(m, n, S, P, alpha, beta, C,
+                                                                     scm, scn);
+  return launched();
+}
+
+int splitk_reduce_f32(stream_t s, int64_t m, int64_t n, int S, const float* P, double alpha,
+                      double beta, double* C, int64_t scm, int64_t scn) {
   splitk_reduce_kernel<<<grid_for(m * n), 256, 0, (cudaStream_t)s>>>(m, n, S, P, alpha, beta, C,
                                                                      scm, scn);
   return launched();

@@ -687,15 +687,18 @@ int launch_tc(cudaStream_t st, const TcMaps& maps, const TcSegs& segs, int kbt, 
     return (int)cudaGetLastError();
   }
   if (out.f32 || out.dn > 0 || out.dm > 0) return (int)cudaErrorInvalidValue;
-  double* P = splitk_buffer((size_t)S * m * n);
+  // partial products in FP32, exactly as tensor memory accumulated them (one
+  // accumulation each), summed in FP64 by the reduction
+  float* P = reinterpret_cast<float*>(splitk_buffer(((size_t)S * m * n + 1) / 2));
   if (!P) return (int)cudaErrorMemoryAllocation;
-  TcOut po{P, 1, m, 0, 0, 0, 0, 0};
+  TcOut po{P, 1, m, 0, 0, 0, 0, 1};
   mgemm_bf16_kernel<NSL, TN><<<grid, THREADS_TC, Cfg::SMEM_BYTES, st>>>(
       maps, po, m, n, 1.0, 0.0, segs, kps, kbt, m * n, mt, nt, S, nullptr);
   note_launches(1);
   int e = (int)cudaGetLastError();
   if (e) return e;
-  return splitk_reduce((stream_t)st, m, n, S, P, alpha, beta, (double*)out.C, out.scm, out.scn);
+  return splitk_reduce_f32((stream_t)st, m, n, S, P, alpha, beta, (double*)out.C, out.scm,
+                           out.scn);
 }
 
 }  // namespace

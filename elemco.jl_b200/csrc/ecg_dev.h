@@ -245,6 +245,9 @@ int tc_error(int* code);
 double* splitk_buffer(size_t n);
 int splitk_reduce(stream_t s, int64_t m, int64_t n, int S, const double* P, double alpha,
                   double beta, double* C, int64_t scm, int64_t scn);
+// The same for FP32 partials (summed in FP64).
+int splitk_reduce_f32(stream_t s, int64_t m, int64_t n, int S, const float* P, double alpha,
+                      double beta, double* C, int64_t scm, int64_t scn);
 
 // GEMM event timing (process-wide): enable, then read and reset the totals.
 void gemm_timing(bool enable);
