@@ -5,8 +5,9 @@
 
 #include <algorithm>
 #include <atomic>
-#include <mutex>
 #include <cstdio>
+#include <map>
+#include <mutex>
 #include <utility>
 #include <vector>
 
@@ -24,13 +25,122 @@ static inline int launched() {
 }
 
 int set_device(int device) { return (int)cudaSetDevice(device); }
+
+// ---- per-stream state ------------------------------------------------------
+//
+// Scratch that the GEMM launchers need beyond their operands — the split-K
+// partial products and the BF16 slices of gemm_mixed — belongs to the stream
+// (and device) the GEMM runs on.  A context owns one stream, so contexts on
+// different devices, or on different host threads, never share it.  A buffer
+// grows only after its stream has drained, so no kernel of that stream still
+// reads the old one, and never during stream capture.  The tensor-core wait
+// bound is kept here too.  Entries of streams the library did not create
+// (a caller's stream) live until process exit.
+namespace {
+struct StreamState {
+  double* splitk = nullptr;
+  size_t splitk_len = 0;  // doubles
+  void* split = nullptr;
+  size_t split_bytes = 0;
+  unsigned long long tc_wait_ns = 0;  // 0: the default bound
+};
+std::mutex g_ss_mu;
+std::map<std::pair<cudaStream_t, int>, StreamState> g_ss;
+
+int current_device() {
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  return d;
+}
+
+// The state of stream s on the current device (created empty on first use);
+// the caller holds g_ss_mu.  std::map nodes stay put while others are added.
+StreamState& stream_state_locked(cudaStream_t s) { return g_ss[{s, current_device()}]; }
+
+bool capturing(cudaStream_t s) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) {
+    cudaGetLastError();
+    return true;
+  }
+  return cs != cudaStreamCaptureStatusNone;
+}
+
+// Grow *p (holding *have bytes) to at least `want` bytes (plus `extra`
+// headroom) for stream s; nullptr if that needs an allocation during capture
+// or the allocation fails.
+void* grow(cudaStream_t s, void** p, size_t* have, size_t want, size_t extra) {
+  if (want <= *have) return *p;
+  if (capturing(s)) return nullptr;
+  if (*p) {
+    cudaStreamSynchronize(s);
+    cudaFree(*p);
+  }
+  *p = nullptr;
+  *have = 0;
+  if (cudaMalloc(p, want + extra) != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return nullptr;
+  }
+  *have = want + extra;
+  return *p;
+}
+}  // namespace
+
 int stream_create(stream_t* s) {
   cudaStream_t st;
   int e = (int)cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
   *s = (stream_t)st;
   return e;
 }
-void stream_destroy(stream_t s) { cudaStreamDestroy((cudaStream_t)s); }
+
+void stream_destroy(stream_t s) {
+  cudaStream_t st = (cudaStream_t)s;
+  cudaStreamSynchronize(st);
+  {
+    std::lock_guard<std::mutex> lk(g_ss_mu);
+    auto it = g_ss.find({st, current_device()});
+    if (it != g_ss.end()) {
+      if (it->second.splitk) cudaFree(it->second.splitk);
+      if (it->second.split) cudaFree(it->second.split);
+      g_ss.erase(it);
+    }
+  }
+  cudaStreamDestroy(st);
+}
+
+double* splitk_buffer(stream_t s, size_t n) {
+  std::lock_guard<std::mutex> lk(g_ss_mu);
+  StreamState& ss = stream_state_locked((cudaStream_t)s);
+  size_t have = ss.splitk_len * sizeof(double);
+  const size_t want = std::max(n, (size_t)1 << 22) * sizeof(double);
+  void* p = ss.splitk;
+  void* r = grow((cudaStream_t)s, &p, &have, want, 0);
+  ss.splitk = (double*)p;
+  ss.splitk_len = have / sizeof(double);
+  return (double*)r;
+}
+
+void* split_scratch(stream_t s, size_t bytes) {
+  std::lock_guard<std::mutex> lk(g_ss_mu);
+  StreamState& ss = stream_state_locked((cudaStream_t)s);
+  return grow((cudaStream_t)s, &ss.split, &ss.split_bytes, bytes, bytes / 4);
+}
+
+int set_tc_wait(stream_t s, uint64_t ns) {
+  std::lock_guard<std::mutex> lk(g_ss_mu);
+  stream_state_locked((cudaStream_t)s).tc_wait_ns = ns;
+  return 0;
+}
+
+uint64_t tc_wait(stream_t s) {
+  std::lock_guard<std::mutex> lk(g_ss_mu);
+  return stream_state_locked((cudaStream_t)s).tc_wait_ns;
+}
 int sync(stream_t s) { return (int)cudaStreamSynchronize((cudaStream_t)s); }
 const char* error_string(int code) { return cudaGetErrorString((cudaError_t)code); }
 int check_launch() { return (int)cudaGetLastError(); }
@@ -107,6 +217,23 @@ int memset0(void* dst, size_t bytes, stream_t s) {
   if (!bytes) return 0;
   return (int)cudaMemsetAsync(dst, 0, bytes, (cudaStream_t)s);
 }
+
+// One flag per device (cudaFuncSetAttribute acts on the current device only):
+// test() reports whether the current device's flag is set, set(e) sets it when
+// the attribute call e succeeded.  Two threads may both set it; that is
+// harmless (the attribute call is idempotent).
+struct DeviceFlags {
+  std::atomic<bool> f[128] = {};
+  bool test() {
+    const int d = current_device();
+    return d >= 0 && d < 128 && f[d].load(std::memory_order_acquire);
+  }
+  void set(cudaError_t e) {
+    const int d = current_device();
+    if (e == cudaSuccess && d >= 0 && d < 128) f[d].store(true, std::memory_order_release);
+    if (e != cudaSuccess) cudaGetLastError();
+  }
+};
 
 // ---------------------------------------------------------------- GEMM
 //
@@ -393,12 +520,10 @@ template <int BM, int BN, int BK, int WM, int WN, int STAGES, int MINB = 1, int 
           int FLAGS = 0>
 static int launch_gemm(const GemmArgs& g, int64_t batch, cudaStream_t st) {
   using Cfg = GemmCfg<BM, BN, BK, WM, WN, STAGES>;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(dgemm_kernel<BM, BN, BK, WM, WN, STAGES, MINB, KMMA, FLAGS>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
-    attr = true;
-  }
+  static DeviceFlags attr;
+  if (!attr.test())
+    attr.set(cudaFuncSetAttribute(dgemm_kernel<BM, BN, BK, WM, WN, STAGES, MINB, KMMA, FLAGS>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM));
   int64_t gx = (g.m + BM - 1) / BM, gy = (g.n + BN - 1) / BN;
   if (gy > 65535 || batch > 65535) return (int)cudaErrorInvalidConfiguration;
   dim3 grid((unsigned)gx, (unsigned)gy, (unsigned)batch);
@@ -409,24 +534,6 @@ static int launch_gemm(const GemmArgs& g, int64_t batch, cudaStream_t st) {
 
 static unsigned grid_for(int64_t n, int threads = 256, int64_t cap = 148 * 16);
 
-// Device scratch for split-K partial products (grown on demand; cudaFree of
-// the old buffer synchronises the device, so no kernel still uses it).
-static double* g_splitk = nullptr;
-static size_t g_splitk_len = 0;
-double* splitk_buffer(size_t n) {
-  if (n > g_splitk_len) {
-    if (g_splitk) cudaFree(g_splitk);
-    g_splitk = nullptr;
-    g_splitk_len = 0;
-    size_t want = std::max(n, (size_t)1 << 22);
-    if (cudaMalloc(&g_splitk, want * sizeof(double)) != cudaSuccess) {
-      cudaGetLastError();
-      return nullptr;
-    }
-    g_splitk_len = want;
-  }
-  return g_splitk;
-}
 
 // C = alpha sum_z P[z] + beta C, the partials (FP64, or FP32 for the
 // tensor-core GEMM, whose partials are FP32 accumulations) summed in FP64 in
@@ -484,11 +591,23 @@ int gemm_splitk_noalloc(stream_t s, char ta, char tb, int64_t m, int64_t n, int6
                         double alpha, const double* A, int64_t lda, const double* B, int64_t ldb,
                         double beta, double* C, int64_t ldc, int* nsplit) {
   if (m <= 0 || n <= 0 || k <= 0) return (int)cudaErrorInvalidValue;
-  if ((size_t)m * (size_t)n > kNoAllocScratchDoubles) return (int)cudaErrorInvalidValue;
+  if ((uint64_t)n > kNoAllocScratchDoubles / (uint64_t)m) return (int)cudaErrorInvalidValue;
   double* P = nullptr;
   int e = noalloc_scratch_ptr(&P);
   if (e) return e;
-  const bool at = (ta == 'T' || ta == 't'), bt = (tb == 'T' || tb == 't');
+  bool at = (ta == 'T' || ta == 't'), bt = (tb == 'T' || tb == 't');
+  int64_t ldcm = 1, ldcn = ldc;  // C(i,j) at C[i*ldcm + j*ldcn]
+  if ((n + 63) / 64 > 65535) {
+    // more column tiles than the grid's y extent: compute C^T = op(B)^T op(A)^T
+    // (the m <-> n swap puts the long dimension on the grid's x axis)
+    std::swap(m, n);
+    std::swap(A, B);
+    std::swap(lda, ldb);
+    const bool t = at;
+    at = !bt;
+    bt = !t;
+    std::swap(ldcm, ldcn);
+  }
   const int64_t tiles64 = ((m + 63) / 64) * ((n + 63) / 64);
   int64_t S = std::min<int64_t>((2 * 148 + tiles64 - 1) / tiles64, (k + 255) / 256);
   S = std::max<int64_t>(1, std::min<int64_t>(S, 64));
@@ -504,7 +623,8 @@ int gemm_splitk_noalloc(stream_t s, char ta, char tb, int64_t m, int64_t n, int6
   cudaStream_t st = (cudaStream_t)s;
   e = launch_gemm<64, 64, 16, 32, 32, 3, 3>(h, S, st);
   if (e) return e;
-  splitk_reduce_kernel<<<grid_for(m * n), 256, 0, st>>>(m, n, (int)S, P, alpha, beta, C, 1, ldc);
+  splitk_reduce_kernel<<<grid_for(m * n), 256, 0, st>>>(m, n, (int)S, P, alpha, beta, C, ldcm,
+                                                        ldcn);
   if (nsplit) *nsplit = (int)S;
   return launched();
 }
@@ -622,7 +742,7 @@ static int gemm_launch(stream_t s, const Gemm& q) {
     int64_t kc = (q.k + S - 1) / S;
     kc = (kc + 15) / 16 * 16;
     S = (q.k + kc - 1) / kc;
-    double* P = splitk_buffer((size_t)S * q.m * q.n);
+    double* P = splitk_buffer(s, (size_t)S * q.m * q.n);
     if (!P) return (int)cudaErrorMemoryAllocation;
     GemmArgs h = g;
     h.k = kc;
@@ -1441,21 +1561,24 @@ int triples_energy_batched(stream_t s, int nv, int nitems, const void* K, const 
   if (nv > 1290 || nitems <= 0 || nitems > 65535 || !eijk_tab || !tt_tab)
     return (int)cudaErrorInvalidValue;
   const int g = (int)energy_grid(nv);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(triples_energy_kernel<double, false>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         EnergySmem<double, false>::BYTES);
-    cudaFuncSetAttribute(triples_energy_kernel<float, false>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         EnergySmem<float, false>::BYTES);
-    cudaFuncSetAttribute(triples_energy_kernel<double, true>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         EnergySmem<double, true>::BYTES);
-    cudaFuncSetAttribute(triples_energy_kernel<float, true>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         EnergySmem<float, true>::BYTES);
-    attr = true;
+  static DeviceFlags attr;
+  if (!attr.test()) {
+    cudaError_t e = cudaFuncSetAttribute(triples_energy_kernel<double, false>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         EnergySmem<double, false>::BYTES);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(triples_energy_kernel<float, false>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               EnergySmem<float, false>::BYTES);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(triples_energy_kernel<double, true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               EnergySmem<double, true>::BYTES);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(triples_energy_kernel<float, true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               EnergySmem<float, true>::BYTES);
+    attr.set(e);
   }
   cudaStream_t st = (cudaStream_t)s;
   const dim3 grid((unsigned)g, (unsigned)nitems);

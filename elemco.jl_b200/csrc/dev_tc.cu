@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <cstring>
 #include <mutex>
@@ -44,7 +45,12 @@ constexpr int RING_BYTES = 216 * 1024;
 // longest K (in 64-wide k-blocks) one FP32 tensor-memory accumulator sums
 // before its partial product is handed to an FP64 reduction
 constexpr int KB_ACC = (int)(TC_ACC_K / TK);
-constexpr unsigned long long WAIT_NS = 1000000000ull;  // 1 s bound on every mbarrier wait
+// Bound on every mbarrier wait: 1 s.  The main-loop waits (producer, MMA
+// issuer, epilogue) take the stream's bound instead when one is set (kernel
+// argument wait_ns); the final waits for the kernel's own TMA loads and MMAs
+// in flight always keep the full second, so nothing is in flight when the CTA
+// frees its tensor memory and exits.
+constexpr unsigned long long WAIT_NS = 1000000000ull;
 
 template <int NSL, int TN>
 struct TcCfg {
@@ -88,8 +94,10 @@ __device__ __forceinline__ unsigned long long gtime() {
   return t;
 }
 
-// Parity wait bounded by WAIT_NS of wall time; returns false on time-out.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Parity wait bounded by `limit` ns of wall time (limit 0: gives up at the
+// first try_wait that finds the phase incomplete); returns false on time-out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
+                                          unsigned long long limit = WAIT_NS) {
   const uint32_t a = smem_u32(bar);
   const unsigned long long t0 = gtime();
   for (;;) {
@@ -100,7 +108,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
         : "=r"(done)
         : "r"(a), "r"(parity));
     if (done) return true;
-    if (gtime() - t0 > WAIT_NS) return false;
+    if (gtime() - t0 >= limit) return false;
   }
 }
 
@@ -257,7 +265,7 @@ __global__ void __launch_bounds__(THREADS_TC, 1)
                       double alpha, double beta, const TcSegs segs, int kb_per_split,
                       int kblocks_total,
                       int64_t split_stride, int mtiles, int ntiles, int nsplit,
-                      const TcMaps* __restrict__ mtab) {
+                      const TcMaps* __restrict__ mtab, unsigned long long wait_ns) {
   using Cfg = TcCfg<NSL, TN>;
   constexpr int STAGES = Cfg::STAGES, STAGE_BYTES = Cfg::STAGE_BYTES;
   constexpr int TILE_BYTES_B = Cfg::TILE_BYTES_B;
@@ -328,7 +336,7 @@ __global__ void __launch_bounds__(THREADS_TC, 1)
         for (int kb = 0; kb < nk; ++kb, ++g) {
           const int s = (int)(g % STAGES);
           const int64_t u = g / STAGES;
-          if (u > 0 && !mbar_wait(&empty[s], (uint32_t)((u - 1) & 1))) {
+          if (u > 0 && !mbar_wait(&empty[s], (uint32_t)((u - 1) & 1), wait_ns)) {
             atomicExch(&g_tc_error, 1);
             atomicExch(abort_flag, 1);
             break;
@@ -362,7 +370,7 @@ __global__ void __launch_bounds__(THREADS_TC, 1)
         const int nk = item_kblocks(z), kb0 = mtab ? 0 : z * kb_per_split;
         const int acc = (int)(lt & 1);
         const int64_t ua = lt >> 1;
-        if (ua > 0 && !mbar_wait(&tempty[acc], (uint32_t)((ua - 1) & 1))) {
+        if (ua > 0 && !mbar_wait(&tempty[acc], (uint32_t)((ua - 1) & 1), wait_ns)) {
           atomicExch(&g_tc_error, 4);
           atomicExch(abort_flag, 1);
           break;
@@ -372,7 +380,7 @@ __global__ void __launch_bounds__(THREADS_TC, 1)
         bool ok = true;
         for (int kb = 0; kb < nk; ++kb, ++g) {
           const int s = (int)(g % STAGES);
-          if (!mbar_wait(&full[s], (uint32_t)((g / STAGES) & 1))) {
+          if (!mbar_wait(&full[s], (uint32_t)((g / STAGES) & 1), wait_ns)) {
             atomicExch(&g_tc_error, 2);
             atomicExch(abort_flag, 1);
             ok = false;
@@ -427,7 +435,7 @@ __global__ void __launch_bounds__(THREADS_TC, 1)
         else
           prefetch_cols((const double*)out.C, rowoff, col0, TN / 2, N, out);
       }
-      if (!mbar_wait(&tfull[acc], (uint32_t)((lt >> 1) & 1))) {
+      if (!mbar_wait(&tfull[acc], (uint32_t)((lt >> 1) & 1), wait_ns)) {
         atomicExch(&g_tc_error, 3);
         atomicExch(abort_flag, 1);
         break;
@@ -512,8 +520,6 @@ typedef CUresult (*EncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void
                              CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 EncodeFn g_encode = nullptr;
 std::mutex g_tc_mu;
-__nv_bfloat16* g_split = nullptr;
-size_t g_split_len = 0;
 
 int encode_fn(EncodeFn* out) {
   std::lock_guard<std::mutex> lk(g_tc_mu);
@@ -529,21 +535,6 @@ int encode_fn(EncodeFn* out) {
   return 0;
 }
 
-__nv_bfloat16* split_buffer(size_t n) {
-  std::lock_guard<std::mutex> lk(g_tc_mu);
-  if (n > g_split_len) {
-    if (g_split) cudaFree(g_split);
-    g_split = nullptr;
-    g_split_len = 0;
-    size_t want = n + n / 4;
-    if (cudaMalloc(&g_split, want * sizeof(__nv_bfloat16)) != cudaSuccess) {
-      cudaGetLastError();
-      return nullptr;
-    }
-    g_split_len = want;
-  }
-  return g_split;
-}
 
 // rows: extent of the map (rows past it read as zero); slice_stride in BF16
 // elements (default: rows * k_p, a dense [slice][row][k] block)
@@ -659,14 +650,28 @@ int split_count(int64_t tiles, int kbt) {
 
 // Launch over pre-split operands; S > 1 splits the combined k-blocks into S
 // slices that write FP64 partial products P[z][n][m] (column-major m x n).
+// cudaFuncSetAttribute acts on the current device only: one flag per device.
 template <int NSL, int TN>
 void set_smem_attr() {
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(mgemm_bf16_kernel<NSL, TN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         TcCfg<NSL, TN>::SMEM_BYTES);
-    attr = true;
+  static std::atomic<bool> done[128] = {};
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess) {
+    cudaGetLastError();
+    d = -1;
   }
+  if (d >= 0 && d < 128 && done[d].load(std::memory_order_acquire)) return;
+  if (cudaFuncSetAttribute(mgemm_bf16_kernel<NSL, TN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           TcCfg<NSL, TN>::SMEM_BYTES) == cudaSuccess) {
+    if (d >= 0 && d < 128) done[d].store(true, std::memory_order_release);
+  } else {
+    cudaGetLastError();
+  }
+}
+
+// The stream's main-loop wait bound (0: the default second).
+unsigned long long wait_bound(cudaStream_t st) {
+  const uint64_t w = tc_wait((stream_t)st);
+  return w ? (unsigned long long)w : WAIT_NS;
 }
 
 template <int NSL, int TN>
@@ -680,20 +685,21 @@ int launch_tc(cudaStream_t st, const TcMaps& maps, const TcSegs& segs, int kbt, 
   S = (kbt + kps - 1) / kps;
   const int64_t items = (int64_t)mt * nt * S;
   const unsigned grid = (unsigned)(items < 148 ? items : 148);
+  const unsigned long long wns = wait_bound(st);
   if (S == 1) {
     mgemm_bf16_kernel<NSL, TN><<<grid, THREADS_TC, Cfg::SMEM_BYTES, st>>>(
-        maps, out, m, n, alpha, beta, segs, kps, kbt, 0, mt, nt, 1, nullptr);
+        maps, out, m, n, alpha, beta, segs, kps, kbt, 0, mt, nt, 1, nullptr, wns);
     note_launches(1);
     return (int)cudaGetLastError();
   }
   if (out.f32 || out.dn > 0 || out.dm > 0) return (int)cudaErrorInvalidValue;
   // partial products in FP32, exactly as tensor memory accumulated them (one
   // accumulation each), summed in FP64 by the reduction
-  float* P = reinterpret_cast<float*>(splitk_buffer(((size_t)S * m * n + 1) / 2));
+  float* P = reinterpret_cast<float*>(splitk_buffer((stream_t)st, ((size_t)S * m * n + 1) / 2));
   if (!P) return (int)cudaErrorMemoryAllocation;
   TcOut po{P, 1, m, 0, 0, 0, 0, 1};
   mgemm_bf16_kernel<NSL, TN><<<grid, THREADS_TC, Cfg::SMEM_BYTES, st>>>(
-      maps, po, m, n, 1.0, 0.0, segs, kps, kbt, m * n, mt, nt, S, nullptr);
+      maps, po, m, n, 1.0, 0.0, segs, kps, kbt, m * n, mt, nt, S, nullptr, wns);
   note_launches(1);
   int e = (int)cudaGetLastError();
   if (e) return e;
@@ -906,7 +912,7 @@ void launch_batched(cudaStream_t st, const TcOut& out, const TcGemm& g, const Tc
   std::memset(&dummy, 0, sizeof(dummy));
   mgemm_bf16_kernel<NSL, TN><<<grid, THREADS_TC, Cfg::SMEM_BYTES, st>>>(
       dummy, out, g.m, g.n, g.alpha, g.beta, segs, kbt, kbt, c_stride, mt, nt, batch,
-      (const TcMaps*)mtab);
+      (const TcMaps*)mtab, wait_bound(st));
 }
 }  // namespace
 
@@ -955,7 +961,8 @@ int gemm_strided_mixed(stream_t s, const Gemm& q) {
   constexpr int NSL = 3;
   const int64_t m = q.m, n = q.n, k = q.k;
   const int64_t mp = pad_rows(m), np = pad_rows(n), kp = pad_k(k);
-  __nv_bfloat16* buf = split_buffer((size_t)NSL * (mp + np) * kp);
+  __nv_bfloat16* buf = (__nv_bfloat16*)split_scratch(
+      s, (size_t)NSL * (mp + np) * kp * sizeof(__nv_bfloat16));
   if (!buf) return (int)cudaErrorMemoryAllocation;
   __nv_bfloat16* As = buf;
   __nv_bfloat16* Bs = buf + (size_t)NSL * mp * kp;

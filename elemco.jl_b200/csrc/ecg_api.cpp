@@ -62,6 +62,8 @@ static void opts_or_default(const ecg_cc_opts* in, ecg_cc_opts& o) {
   else ecg_default_opts(&o);
   if (o.maxdiis < 1 || o.maxdiis > 8) throw Error(ECG_ERR_ARG, "maxdiis must be in 1..8");
   if (o.maxit < 0) throw Error(ECG_ERR_ARG, "maxit must be >= 0");
+  if (o.diis_dot != ECG_DIIS_CS && o.diis_dot != ECG_DIIS_PLAIN)
+    throw Error(ECG_ERR_ARG, "diis_dot must be ECG_DIIS_CS or ECG_DIIS_PLAIN");
 }
 
 // Device scalar slot of the non-finite input flag.
@@ -107,6 +109,7 @@ void ecg_default_opts(ecg_cc_opts* o) {
   o->shiftp = 0.2;
   o->maxdiis = 6;
   o->resthr = 10.0;
+  o->diis_dot = ECG_DIIS_CS;
 }
 
 int ecg_create(int device, ecg_ctx** out) {
@@ -155,6 +158,24 @@ int ecg_set_precision(ecg_ctx* c, int prec) {
     if (prec != ECG_PREC_FP64 && prec != ECG_PREC_MIXED)
       throw Error(ECG_ERR_ARG, "precision must be ECG_PREC_FP64 or ECG_PREC_MIXED");
     c->prec = prec;
+  });
+}
+
+int ecg_set_option(ecg_ctx* c, int32_t key, int64_t value) {
+  if (!c) return ECG_ERR_ARG;
+  return guarded(c, [&] {
+    if (value < 0) throw Error(ECG_ERR_ARG, "option values must be >= 0");
+    switch (key) {
+      case ECG_OPT_TRIPLES_BATCH:
+        c->triples_batch = value;
+        break;
+      case ECG_OPT_TC_WAIT_NS:
+        check(dev::set_device(c->device), "cudaSetDevice");
+        check(dev::set_tc_wait(c->st, (uint64_t)value), "set_tc_wait");
+        break;
+      default:
+        throw Error(ECG_ERR_ARG, "unknown option key " + std::to_string(key));
+    }
   });
 }
 
@@ -491,8 +512,8 @@ int ecg_gemm_noalloc(char ta, char tb, int64_t m, int64_t n, int64_t k, double a
     if (lda < (at ? k : m) || ldb < (bt ? n : k) || ldc < m)
       throw Error(ECG_ERR_ARG, "leading dimension too small");
     const uint64_t cap = dev::noalloc_scratch_doubles();
-    if ((uint64_t)m * (uint64_t)n > cap)
-      throw Error(ECG_ERR_ARG, "m*n = " + std::to_string((uint64_t)m * (uint64_t)n) +
+    if ((uint64_t)n > cap / (uint64_t)m)  // m*n > cap, without forming the product
+      throw Error(ECG_ERR_ARG, "m*n = " + std::to_string(m) + "*" + std::to_string(n) +
                                    " exceeds the allocation-free scratch (" +
                                    std::to_string(cap) + " output elements)");
     int S = 0;

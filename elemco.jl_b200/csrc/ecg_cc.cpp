@@ -651,7 +651,7 @@ void diis_perform(Ctx& c, DiisState& d, double* amps, const double* res) {
 
 void cc_init_iterations(Ctx& c, const ecg_cc_opts& o) {
   c.opts = o;
-  diis_reset(c, c.diis, o.maxdiis, o.resthr, c.n1() + c.n2(), true);
+  diis_reset(c, c.diis, o.maxdiis, o.resthr, c.n1() + c.n2(), o.diis_dot == ECG_DIIS_CS);
 }
 
 // Energy-type reductions of T (and R) into scalars starting at `base`:

@@ -31,6 +31,7 @@ struct Ctx {
   std::vector<std::pair<void*, size_t>> allocs;
   uint64_t generation = 0;  // bumped whenever free_all() releases the system's buffers
   int prec = ECG_PREC_FP64;
+  int64_t triples_batch = 0;  // ECG_OPT_TRIPLES_BATCH (0 = automatic)
   bool mixed_active = false;  // route large GEMMs to the split-BF16 tensor-core GEMM
 
   // system

@@ -14,6 +14,8 @@ using stream_t = void*;
 
 int set_device(int device);
 int stream_create(stream_t* s);
+// Waits for s, frees the scratch the layer holds for it (splitk_buffer,
+// split_scratch) and destroys it.
 void stream_destroy(stream_t s);
 int sync(stream_t s);
 const char* error_string(int code);
@@ -240,9 +242,17 @@ int gemm_mixed(stream_t s, char ta, char tb, int64_t m, int64_t n, int64_t k, do
                const double* A, int64_t lda, const double* B, int64_t ldb, double beta,
                double* C, int64_t ldc);
 int tc_error(int* code);
-// Shared split-K scratch (grown on demand) and its fixed-order reduction
+// Split-K scratch of stream s on the current device (at least n doubles;
+// grown on demand, after s has drained, never during stream capture: nullptr
+// then, or when the allocation fails) and its fixed-order reduction
 // C(i,j) = alpha sum_z P[z][i + j m] + beta C(i,j), C at C[i*scm + j*scn].
-double* splitk_buffer(size_t n);
+double* splitk_buffer(stream_t s, size_t n);
+// Scratch of stream s for gemm_mixed's BF16 operand slices (same rules).
+void* split_scratch(stream_t s, size_t bytes);
+// Bound (ns) of the tensor-core kernels' main-loop waits on stream s
+// (0 = the default second); the kernels' final waits keep the second.
+int set_tc_wait(stream_t s, uint64_t ns);
+uint64_t tc_wait(stream_t s);
 int splitk_reduce(stream_t s, int64_t m, int64_t n, int S, const double* P, double alpha,
                   double beta, double* C, int64_t scm, int64_t scn);
 // The same for FP32 partials (summed in FP64).

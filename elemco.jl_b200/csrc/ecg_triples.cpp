@@ -362,7 +362,9 @@ void pert_triples(Ctx& c, const double* U1h, const double* U2h, double* et, doub
   const int64_t esz = mixed ? 4 : 8;
   const int64_t kstride = (v3 + 31) / 32 * 32;
   const int64_t per = kstride * esz * (lam ? 2 : 1);
-  const int NB = (int)std::max<int64_t>(1, std::min<int64_t>({256, nt, ((int64_t)4 << 30) / per}));
+  int64_t nbmax = std::min<int64_t>({256, nt, ((int64_t)4 << 30) / per});
+  if (c.triples_batch > 0) nbmax = std::min(nbmax, c.triples_batch);
+  const int NB = (int)std::max<int64_t>(1, nbmax);
   void* K = c.alloc((NB * kstride * esz + 7) / 8, "(T) K slots");
   void* KU = lam ? (void*)c.alloc((NB * kstride * esz + 7) / 8, "(T) K(Lambda) slots") : nullptr;
   KTables KT, KUt;

@@ -20,6 +20,10 @@ ECG_ERR_TIMEOUT = 5
 ECG_ERR_STATE = 6
 ECG_PREC_FP64 = 0
 ECG_PREC_MIXED = 1
+ECG_DIIS_CS = 0
+ECG_DIIS_PLAIN = 1
+ECG_OPT_TRIPLES_BATCH = 1
+ECG_OPT_TC_WAIT_NS = 2
 
 _NAMES = {1: "ECG_ERR_ARG", 2: "ECG_ERR_CUDA", 3: "ECG_ERR_OOM", 4: "ECG_ERR_NONFINITE",
           5: "ECG_ERR_TIMEOUT", 6: "ECG_ERR_STATE"}
@@ -36,7 +40,7 @@ class ECGError(RuntimeError):
 class CcOpts(C.Structure):
     _fields_ = [("thr", C.c_double), ("conven", C.c_double), ("maxit", C.c_int32),
                 ("shifts", C.c_double), ("shiftp", C.c_double), ("maxdiis", C.c_int32),
-                ("resthr", C.c_double)]
+                ("resthr", C.c_double), ("diis_dot", C.c_int32)]
 
 
 _D = C.POINTER(C.c_double)
@@ -51,6 +55,7 @@ SIGNATURES = {
     "ecg_last_error": (C.c_char_p, [_P]),
     "ecg_set_mem_cap": (C.c_int, [_P, C.c_uint64]),
     "ecg_set_precision": (C.c_int, [_P, C.c_int]),
+    "ecg_set_option": (C.c_int, [_P, C.c_int32, C.c_int64]),
     "ecg_set_system": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, _D, _D, C.c_double]),
     "ecg_fock": (C.c_int, [_P, _D, _D, _D]),
     "ecg_mp2": (C.c_int, [_P, _D, _D, _D]),

@@ -50,6 +50,10 @@ class Context:
     def set_precision(self, prec=ECG_PREC_FP64):
         self._chk(self._L.ecg_set_precision(self._h, int(prec)))
 
+    def set_option(self, key, value):
+        """``ecg_set_option``: ECG_OPT_TRIPLES_BATCH, ECG_OPT_TC_WAIT_NS (0 = automatic)."""
+        self._chk(self._L.ecg_set_option(self._h, int(key), int(value)))
+
     def set_system(self, B, h1, e0, nocc):
         """B[p,q,Q] (n x n x nQ) DF factors, h1 (n x n), core energy e0."""
         B = as_f(B)

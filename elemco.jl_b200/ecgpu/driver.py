@@ -19,7 +19,7 @@ import re
 
 import numpy as np
 
-from ._lib import ECG_PREC_FP64, ECG_PREC_MIXED
+from ._lib import ECG_DIIS_CS, ECG_DIIS_PLAIN, ECG_PREC_FP64, ECG_PREC_MIXED
 from .context import Context
 
 # ---------------------------------------------------------------- options
@@ -35,12 +35,16 @@ class _Group(dict):
 
 def _default_options():
     """Fields of CcOptions/DiisOptions the path reads (src/infos/options.jl:128-282)
-    plus a ``gpu`` group (precision, device)."""
+    plus a ``gpu`` group (precision, device).  ``diis.dot`` selects the dot
+    product of the CC DIIS: "cs", the closed-shell custom dots of the current
+    reference (src/cc/cc.jl:2498-2499,2598), or "plain", the unweighted dot
+    closed-shell CC used before ElemCo.jl 0.13 (src/solvers/diis.jl:155-167),
+    which replays the trajectories behind older pinned energies."""
     return {
         "cc": _Group(thr=1.0e-10, conven=0.1, maxit=50, shifts=0.15, shiftp=0.2,
                      properties=False, save="cc_amplitudes", save_lm="cc_multipliers",
                      nomp2=0),
-        "diis": _Group(maxdiis=6, resthr=10.0, crop=False, maxcrop=3),
+        "diis": _Group(maxdiis=6, resthr=10.0, crop=False, maxcrop=3, dot="cs"),
         "cholesky": _Group(thr=1.0e-12),
         "gpu": _Group(precision="fp64", device=0),
     }
@@ -277,6 +281,15 @@ def _system_from(EC, fcidump):
     return fd.B, fd.h, fd.e0, fd.nelec // 2
 
 
+def _solver_opts(ctx, o):
+    dots = {"cs": ECG_DIIS_CS, "plain": ECG_DIIS_PLAIN}
+    if o["diis"].dot not in dots:
+        raise ValueError(f"diis.dot must be 'cs' or 'plain', not {o['diis'].dot!r}")
+    return ctx.opts(thr=o["cc"].thr, conven=o["cc"].conven, maxit=o["cc"].maxit,
+                    shifts=o["cc"].shifts, shiftp=o["cc"].shiftp, maxdiis=o["diis"].maxdiis,
+                    resthr=o["diis"].resthr, diis_dot=dots[o["diis"].dot])
+
+
 def ccdriver(EC, method, fcidump=""):
     """``ccdriver`` (src/cc/ccdriver.jl:37-76) for closed-shell methods on the GPU."""
     name, dc, lam, pert = parse_method(method)
@@ -292,9 +305,7 @@ def ccdriver(EC, method, fcidump=""):
     emp2, T1, T2 = ctx.mp2()
     out["MP2c"] = emp2
     out["MP2"] = emp2 + EHF
-    opts = ctx.opts(thr=o["cc"].thr, conven=o["cc"].conven, maxit=o["cc"].maxit,
-                    shifts=o["cc"].shifts, shiftp=o["cc"].shiftp, maxdiis=o["diis"].maxdiis,
-                    resthr=o["diis"].resthr)
+    opts = _solver_opts(ctx, o)
     r = ctx.cc_solve(T1, T2, dc=dc, opts=opts)
     if not r["converged"]:
         print("WARNING: CC iterations did not converge!")
@@ -352,9 +363,7 @@ def rrule_cc_energy(EC, method, h=None, fcidump=""):
     ctx.set_system(B, h, e0, nocc)
     _, _, EHF = ctx.fock()
     _, T1, T2 = ctx.mp2()
-    opts = ctx.opts(thr=o["cc"].thr, conven=o["cc"].conven, maxit=o["cc"].maxit,
-                    shifts=o["cc"].shifts, shiftp=o["cc"].shiftp, maxdiis=o["diis"].maxdiis,
-                    resthr=o["diis"].resthr)
+    opts = _solver_opts(ctx, o)
     r = ctx.cc_solve(T1, T2, dc=dc, opts=opts)
     if not r["converged"]:
         raise RuntimeError("CC iterations did not converge")

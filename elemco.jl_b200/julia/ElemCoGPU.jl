@@ -7,8 +7,9 @@ replacements for ElemCo.jl's closed-shell `calc_cc`, `calc_pertT` and
 src/cc/cc_lagrange.jl:1120).  They read the same inputs (the `mmL` DF factors
 or EC.fd, the Fock matrix) and write the same scratch files (`T_vo`,
 `T_vvoo`, `U_vo`, `U_vvoo`, `cc_amplitudes_*`, `cc_multipliers_*`), so the
-rest of `ccdriver` is unchanged.  Wiring into `eval_cc_groundstate` is shown
-in INTEGRATION.md.
+rest of `ccdriver` is unchanged.  `eval_cc_groundstate`
+(src/cc/ccdriver.jl:348-393) calls them in place of `calc_cc`, `calc_lm_cc`
+and `calc_pertT` when a GPU context is set.
 
 Host arrays are passed as `Ptr{Cdouble}` inside `GC.@preserve`; Julia's
 column-major layout is the library's layout.  Status codes other than 0 raise

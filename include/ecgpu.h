@@ -33,6 +33,10 @@ extern "C" {
 #define ECG_PREC_FP64 0      /* all-FP64 path                                 */
 #define ECG_PREC_MIXED 1     /* reduced-precision tensor-core products + FP64 refinement */
 
+/* Dot product of the CC DIIS (ecg_cc_opts.diis_dot). */
+#define ECG_DIIS_CS 0        /* closed-shell custom dots of perform! (src/cc/cc.jl:2498-2499,2598) */
+#define ECG_DIIS_PLAIN 1     /* plain dot (diis.jl:155-167), closed-shell CC before ElemCo.jl 0.13 */
+
 typedef struct ecg_ctx ecg_ctx;
 
 /* Options of the iterative solvers; mirrors CcOptions/DiisOptions
@@ -45,6 +49,7 @@ typedef struct ecg_cc_opts {
   double shiftp;   /* doubles level shift, default 0.2 (options.jl:138)               */
   int32_t maxdiis; /* default 6 (options.jl:274)                                      */
   double resthr;   /* default 10.0 (options.jl:276)                                   */
+  int32_t diis_dot; /* ECG_DIIS_CS (default) or ECG_DIIS_PLAIN; CC iterations only    */
 } ecg_cc_opts;
 
 /* Fill *o with the reference defaults. */
@@ -59,6 +64,19 @@ const char* ecg_last_error(const ecg_ctx* ctx);
  * ECG_ERR_OOM.  Used to test the out-of-memory path without exhausting HBM. */
 int ecg_set_mem_cap(ecg_ctx* ctx, uint64_t bytes);
 int ecg_set_precision(ecg_ctx* ctx, int prec);
+
+/* Context options (no counterpart in the reference), value 0 = automatic:
+ *  ECG_OPT_TRIPLES_BATCH  at most this many occupied triplets per (T) batch
+ *                         (one K slot each; the sweep's batches after the first
+ *                         replay from one CUDA graph)
+ *  ECG_OPT_TC_WAIT_NS     bound in ns on the tensor-core GEMM's main-loop
+ *                         waits on this context's stream (default 1 s); a wait
+ *                         that runs out makes the call return ECG_ERR_TIMEOUT
+ *                         and the context stays usable (the kernel's final
+ *                         waits on its own copies keep the 1 s bound) */
+#define ECG_OPT_TRIPLES_BATCH 1
+#define ECG_OPT_TC_WAIT_NS 2
+int ecg_set_option(ecg_ctx* ctx, int32_t key, int64_t value);
 
 /* Upload the system.  B[p,q,Q] (n x n x nq) are the density-fitting factors
  * with (pq|rs) = sum_Q B[p,q,Q] B[r,s,Q] — the `mmL` file of

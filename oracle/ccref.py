@@ -43,6 +43,11 @@ class Options:
         self.shiftp = 0.2       # :138
         self.maxdiis = 6        # options.jl:274
         self.resthr = 10.0      # :276
+        # dot product of the CC DIIS: "cs" = the closed-shell custom dots
+        # passed to perform! (cc.jl:2498-2499,2598; ElemCo.jl >= 0.13.0,
+        # CHANGELOG.md:76); "plain" = the unweighted dot weighted_dot falls back
+        # to (diis.jl:155-167), which closed-shell CC used before 0.13.0
+        self.diis_dot = "cs"
         for k, v in kw.items():
             if not hasattr(self, k):
                 raise KeyError(k)
@@ -428,7 +433,10 @@ def cc_iterations(S, T1, T2, fock, dc=False, opts=None, log=None):
     opts = opts or Options()
     eps = np.diag(fock)
     eo, ev = eps[S.sl["o"]], eps[S.sl["v"]]
-    diis = Diis(opts.maxdiis, opts.resthr, dots=(cs_singles_dot, cs_doubles_dot))
+    if opts.diis_dot not in ("cs", "plain"):
+        raise ValueError(f"diis_dot must be 'cs' or 'plain', not {opts.diis_dot!r}")
+    dots = (cs_singles_dot, cs_doubles_dot) if opts.diis_dot == "cs" else None
+    diis = Diis(opts.maxdiis, opts.resthr, dots=dots)
     thren = math.sqrt(opts.thr) * opts.conven
     T1 = T1.copy()
     T2 = T2.copy()

@@ -5,7 +5,8 @@ lists in compact ``.npz`` files, plus the reference's pinned energies as JSON.
 Only this script reads the reference checkout; the tests and the GPU box use
 the committed outputs.
 
-Run from the repo root:  python tests/golden/make_fixtures.py [REFERENCE_ROOT]
+Run from the repo root:  python tests/golden/make_fixtures.py REFERENCE_ROOT
+(the ElemCo.jl checkout; or set ELEMCO_REF to it)
 
 Sources (paths inside the ElemCo.jl project):
   test/files/H2O.FCIDUMP      closed shell, NORB=23, NELEC=8   (test/h2o.jl:16)
@@ -105,4 +106,7 @@ def main(refroot):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("ELEMCO_REF")
+    if not root:
+        sys.exit("usage: make_fixtures.py REFERENCE_ROOT  (or set ELEMCO_REF)")
+    main(root)

@@ -129,7 +129,10 @@ def test_lambda_solve_and_lambda_t(ctx, sys_h2o):
 
 def test_driver_reproduces_reference_pins(h2o, gold, tmp_path):
     """ccdriver on the reference's H2O.FCIDUMP integrals (through Cholesky
-    factors) against test/h2o.jl's pinned energies."""
+    factors) against test/h2o.jl's pinned energies: HF, MP2 and CCSD(T) to
+    1e-9 (CCSD(T) with the pre-0.13 DIIS dot that produced the pin, see
+    tests/test_oracle_golden.py), DCSD converged tightly to 1e-9, ΛCCSD(T)
+    to 3e-7; the current-DIIS trajectories equal the oracle's to 1e-9."""
     from ecgpu.driver import ECInfo, FDump, ccdriver
     g = gold["h2o"]
     EC = ECInfo(scr=str(tmp_path))
@@ -137,15 +140,56 @@ def test_driver_reproduces_reference_pins(h2o, gold, tmp_path):
     e = ccdriver(EC, "ccsd(t)")
     assert abs(e["HF"] - g["HF"]) < 1e-9
     assert abs(e["MP2c"] - g["MP2c"]) < 1e-9
-    assert abs(e["CCSD(T)c"] - g["CCSD(T)c"]) < 1e-6
     ref = O.ccdriver(h2o, "ccsd(t)")
+    assert e["iterations"] == ref["iterations"]
     assert abs(e["CCSD(T)c"] - ref["CCSD(T)c"]) < 1e-9
+    assert abs(e["CCSD(T)c"] - g["CCSD(T)c"]) < 3e-7
+    EC.set("diis", dot="plain")
+    e = ccdriver(EC, "ccsd(t)")
+    assert e["iterations"] == 13
+    assert abs(e["CCSD(T)c"] - g["CCSD(T)c"]) < 1e-9
     e = ccdriver(EC, "λccsd(t)")
-    assert abs(e["ΛCCSD(T)c"] - g["LCCSD(T)c"]) < 1e-6
+    assert abs(e["ΛCCSD(T)c"] - g["LCCSD(T)c"]) < 3e-7
+    EC.set("diis", dot="cs")
+    e = ccdriver(EC, "λccsd(t)")
+    ref = O.ccdriver(h2o, "λccsd(t)")
+    assert abs(e["ΛCCSD(T)c"] - ref["ΛCCSD(T)c"]) < 1e-9
+    assert abs(e["ΛCCSD(T)c"] - g["LCCSD(T)c"]) < 3e-7
     EC.set("cc", thr=1e-20, conven=1e-4, maxit=60)
     e = ccdriver(EC, "dcsd")
     assert abs(e["DCSDc"] - g["DCSDc"]) < 1e-9
     assert (tmp_path / "cc_amplitudes_2.bin").exists()
+
+
+@pytest.mark.parametrize("batch", [1, 16])
+def test_pert_t_multibatch_graph_sweep(batch):
+    """The (T) sweep in many batches — the first run directly, the rest replayed
+    from one CUDA graph — on the (H2O)_3/cc-pVDZ shape (o = 12: 352 triplets,
+    352 or 22 batches), (T), [T] and Lambda-(T) against the oracle
+    (cc_triples.jl:39-295) to 1e-11, and equal to the automatic batching."""
+    import ecgpu
+    from ecgpu._lib import ECG_OPT_TRIPLES_BATCH
+    from ecgpu.synthetic import make_workload
+    B, h1, e0, no = make_workload("h2o3_vdz")
+    S = O.System.from_df(np.ascontiguousarray(B.transpose(2, 0, 1)), h1, e0, no)
+    f = O.gen_fock(S)
+    rng = np.random.default_rng(5)
+    with ecgpu.Context(0) as c:
+        c.set_system(B, h1, e0, no)
+        _, T1, T2 = c.mp2()
+        T1 = np.asfortranarray(T1 + 1e-3 * rng.standard_normal(T1.shape))
+        U1 = np.asfortranarray(2.0 * T1)
+        U2 = np.asfortranarray(2.0 * T2 - T2.transpose(0, 1, 3, 2))
+        auto = c.pert_t(T1, T2), c.lambda_pert_t(T1, T2, U1, U2)
+        c.set_option(ECG_OPT_TRIPLES_BATCH, batch)
+        et, etb = c.pert_t(T1, T2)
+        lt, ltb = c.lambda_pert_t(T1, T2, U1, U2)
+    eto, etbo = O.pert_t(S, T1, T2, f)
+    lto, ltbo = O.lambda_pert_t(S, T1, T2, U1, U2, f)
+    assert et < -1e-4
+    assert abs(et - eto) < 1e-11 and abs(etb - etbo) < 1e-11
+    assert abs(lt - lto) < 1e-11 and abs(ltb - ltbo) < 1e-11
+    assert abs(et - auto[0][0]) < 1e-12 and abs(lt - auto[1][0]) < 1e-12
 
 
 def test_synthetic_water_dimer_ccsd_t(ctx):
@@ -224,6 +268,10 @@ def test_mixed_gemm_kernel(ta, tb, m, n, k):
         out = c.diag_gemm(ta, tb, 0.7, A, B, -0.3, C)
     err = np.abs(out - ref) / scale
     assert err.max() < 4.0 * (k / 16 + 16) * 2.0 ** -24, err.max()
+    if k >= 64:
+        # FP32 accumulation of BF16 slice products leaves errors far above an
+        # FP64 GEMM's (~1e-16): the tensor-core kernel computed this result
+        assert err.max() > 1e-11, err.max()
 
 
 @pytest.mark.parametrize("dc", [False, True])
@@ -347,3 +395,27 @@ def test_pert_t_few_occupied(no):
     assert abs(et - eto) < 1e-13 and abs(etb - etbo) < 1e-13
     assert abs(lt - lto) < 1e-13 and abs(ltb - ltbo) < 1e-13
     assert abs(mt - et) < 2e-5 * abs(et) and abs(mtb - etb) < 2e-5 * abs(etb)
+
+
+def test_mixed_ccsd_t_vtz_shape():
+    """The (H2O)_6/cc-pVTZ virtual and auxiliary space (v = 318, nQ = 846) with
+    o = 6: mixed CCSD (FP64 refinement) and mixed (T) within 1 microhartree of
+    FP64.  The mixed GEMMs run with the tile widths of that shape (160 columns
+    for N = v = 318, 256 for the (T) GEMM over v^2 columns)."""
+    import ecgpu
+    from ecgpu.synthetic import make_system
+    no = 6
+    B, h1, e0, _ = make_system(no, 318, 846)
+    out = {}
+    for prec in (ecgpu.ECG_PREC_FP64, ecgpu.ECG_PREC_MIXED):
+        with ecgpu.Context(0) as c:
+            c.set_precision(prec)
+            c.set_system(B, h1, e0, no)
+            _, T1, T2 = c.mp2()
+            r = c.cc_solve(T1, T2)
+            assert r["converged"]
+            out[prec] = (r["E"], c.pert_t()[0])
+    e64, emx = out[ecgpu.ECG_PREC_FP64], out[ecgpu.ECG_PREC_MIXED]
+    assert out[ecgpu.ECG_PREC_FP64][1] < -1e-5
+    assert abs(emx[0] - e64[0]) < 1e-6, (emx[0], e64[0])
+    assert abs(emx[1] - e64[1]) < 1e-6, (emx[1], e64[1])
