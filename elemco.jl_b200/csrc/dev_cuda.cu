@@ -690,6 +690,25 @@ int gemm_strided(stream_t s, const Gemm& q) {
 
 static int gemm_launch(stream_t s, const Gemm& q) {
   if (q.m <= 0 || q.n <= 0 || q.batch <= 0) return 0;
+  if ((q.n + 63) / 64 > 65535 && (q.m + 63) / 64 <= 65535 && q.kseg == 0 && q.dn == 0 &&
+      !q.ptab) {
+    // more column tiles than the grid's y extent: C^T = B^T A^T puts the long
+    // dimension on the grid's x axis
+    Gemm t = q;
+    t.m = q.n;
+    t.n = q.m;
+    t.A = q.B;
+    t.sam = q.sbn;
+    t.sak = q.sbk;
+    t.sab = q.sbb;
+    t.B = q.A;
+    t.sbk = q.sak;
+    t.sbn = q.sam;
+    t.sbb = q.sab;
+    t.scm = q.scn;
+    t.scn = q.scm;
+    return gemm_launch(s, t);
+  }
   cudaStream_t st = (cudaStream_t)s;
   if (q.k <= 0 || q.alpha == 0.0) {
     if (q.beta == 1.0) return 0;

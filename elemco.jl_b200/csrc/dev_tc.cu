@@ -435,12 +435,18 @@ __global__ void __launch_bounds__(THREADS_TC, 1)
         else
           prefetch_cols((const double*)out.C, rowoff, col0, TN / 2, N, out);
       }
-      if (!mbar_wait(&tfull[acc], (uint32_t)((lt >> 1) & 1), wait_ns)) {
-        atomicExch(&g_tc_error, 3);
-        atomicExch(abort_flag, 1);
+      // every lane waits; the warp goes on only if all lanes saw the
+      // accumulator ready and no time-out was recorded, so the warp-wide
+      // tcgen05.ld below always runs converged
+      const bool ready = mbar_wait(&tfull[acc], (uint32_t)((lt >> 1) & 1), wait_ns);
+      if (!__all_sync(0xffffffffu, ready)) {
+        if (lane == 0) {
+          atomicExch(&g_tc_error, 3);
+          atomicExch(abort_flag, 1);
+        }
         break;
       }
-      if (*(volatile int*)abort_flag) break;
+      if (__any_sync(0xffffffffu, *(volatile int*)abort_flag != 0)) break;
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
 #pragma unroll 1
       for (int c = hw * (TN / 2); c < (hw + 1) * (TN / 2); c += 16) {
