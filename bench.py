@@ -1,20 +1,34 @@
 """Benchmark: closed-shell CCSD iterations per second on one B200 per rank.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload h2o4_vdz] [--method ccsd|dcsd] [--precision fp64]
+                    [--workload h2o6_vtz] [--method ccsd|dcsd]
 
-A step is one CCSD iteration (T1-dressing, residual, Hylleraas energy,
-amplitude update, DIIS, energy) of the (H2O)_4/cc-pVDZ-sized closed-shell
-problem (o=16, v=76, nQ=336) built from seeded synthetic density-fitting
-factors (no integral engine: see the workload generator).  Inputs stay in
-HBM; the L2 cache is flushed (256 MiB write) between timed steps, which are
-timed with CUDA events on the library's stream.  With N > 1 each rank runs an
-independent replica (the path runs on one GPU; no data-path collective) and
-the slowest rank's time is reported.
+A step is one FP64 CCSD iteration (T1-dressing, residual, Hylleraas energy,
+amplitude update, DIIS, energy) of the (H2O)_6/cc-pVTZ-sized closed-shell
+problem (o=24, v=318, nQ=846; the largest single-GPU configuration) built
+from seeded synthetic density-fitting factors (no integral engine: see the
+workload generator).  Inputs stay in HBM (T2 466 MB, B 792 MB: larger than
+the 126 MB L2, which is also flushed between steps); steps are timed with CUDA
+events on the library's stream.  The line also carries:
 
-``--impl reference`` times the oracle (the numpy restatement of the
-reference's algorithm — ElemCo.jl itself needs Julia, absent here) on the
-host cores, same workload and metric.
+* ``e2e``: the same iterations through the C ABI with pinned host amplitudes
+  (host-to-device and device-to-host copies inside the timed region);
+* ``mixed``: CCSD(T) time-to-solution from the MP2 guess, all-FP64 against
+  split-BF16 tensor-core products with FP64 refinement, and the energy
+  difference in microhartree;
+* ``rooflines``: the FP64 DMMA GEMM (against cuBLAS DGEMM measured in the same
+  run), the tcgen05 GEMM (against the measured sustained BF16 peak) and the
+  (T) energy kernel (against the measured HBM bandwidth), each from CUDA
+  events around its launches;
+* ``cpu_baseline``: the density-fitted numpy restatement of the reference
+  algorithm (oracle/dfcc.py) on the host cores, sampled.
+
+With N > 1 each rank runs an independent replica (the path runs on one GPU;
+no data-path collective) and the slowest rank's time is reported.
+
+``--impl reference`` times that CPU restatement (ElemCo.jl itself needs Julia,
+absent here) on the host cores: its K timed steps execute exactly one CCSD
+iteration of the same workload, split into K consecutive parts.
 """
 import argparse
 import json
@@ -43,12 +57,13 @@ def parse_args():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=20)
-    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="h2o4_vdz")
+    p.add_argument("--workload", default="h2o6_vtz")
     p.add_argument("--method", default="ccsd", choices=["ccsd", "dcsd"])
     p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    p.add_argument("--cpu-sample", type=int, default=2, help="CPU-baseline iterations")
+    p.add_argument("--cpu-sample", type=int, default=1,
+                   help="ladder a-blocks timed in the CPU baseline (0: no CPU baseline)")
     p.add_argument("--tts", action="store_true",
                    help="CCSD(T) time-to-solution, FP64 vs mixed, on --workload (one line)")
     p.add_argument("--gradient", action="store_true",
@@ -115,27 +130,52 @@ class Clocks:
 # ---------------------------------------------------------------- CPU side
 
 
-def cpu_ccsd_rate(no, nv, nq, dc, iters):
-    """Oracle CCSD iterations/s on the host (all cores via the BLAS)."""
+def _df_state(workload, dc, nsteps=20):
+    """The DF CPU restatement (oracle/dfcc.py) of the workload, started from
+    MP2 amplitudes; the ladder is cut into about 2*nsteps a-blocks."""
+    from oracle.dfcc import DFCC
+    from ecgpu.synthetic import make_workload
+    B, h1, e0, no = make_workload(workload)
+    nv = B.shape[0] - no
+    d = DFCC(B, h1, e0, no, dc=dc, ablock=max(1, nv // (2 * max(nsteps, 1))))
+    d.start()
+    return d
+
+
+def cpu_baseline_sample(workload, dc, nblocks=1, ntrip=4):
+    """CPU iterations/s of the DF restatement: every task of one CCSD iteration
+    except the ladder runs once, the ladder on `nblocks` of its a-blocks; the
+    iteration time is the non-ladder time plus the ladder blocks' mean time
+    times their number (the blocks are alike).  Also (T) TFLOP/s on `ntrip`
+    triplets."""
     import oracle as O
-    from ecgpu.synthetic import make_system
-    B, h1, e0, _ = make_system(no, nv, nq)
-    S = O.System.from_df(np.transpose(B, (2, 0, 1)), h1, e0, no)
-    f = O.gen_fock(S)
-    _, T1, T2 = O.mp2(S, f)
-    eps = np.diag(f)
-    eo, ev = eps[:no], eps[no:]
-    diis = O.Diis(6, 10.0, dots=(O.cs_singles_dot, O.cs_doubles_dot))
+    d = _df_state(workload, dc)
+    t_other, t_lad, nlad, nrun = 0.0, 0.0, 0, 0
+    for name, _, fn in d.iteration_tasks():
+        if name.startswith("ladder"):
+            nlad += 1
+            if nrun >= nblocks:
+                continue
+            t0 = time.perf_counter()
+            fn()
+            t_lad += time.perf_counter() - t0
+            nrun += 1
+        else:
+            t0 = time.perf_counter()
+            fn()
+            t_other += time.perf_counter() - t0
+    t_iter = t_other + t_lad / nrun * nlad
+    trip = list(O.ccref._triplets(d.no))
+    pick = [trip[(i * len(trip)) // ntrip] for i in range(ntrip)]
+    for x in {q for t in pick for q in t[:3]}:
+        d.vvvo_k(x)  # the same work pert_t does per distinct occupied index
     t0 = time.perf_counter()
-    for _ in range(iters):
-        R1, R2 = O.cc_resid(S, T1, T2, dc=dc)
-        O.hylleraas(S, T1, T2, R1, R2, f)
-        T2 = T2 + O.update_doubles(R2, eo, ev, 0.2)
-        T1 = T1 + O.update_singles(R1, eo, ev, 0.15)
-        diis.perform([T1, T2], [R1, R2])
-        O.doubles_energy(S, T2) + O.singles_energy(S, T1, f)
-    dt = time.perf_counter() - t0
-    return iters / dt, dt
+    d.pert_t(d.T1, d.T2, pick)
+    t_t = time.perf_counter() - t0
+    ft = ntrip * (12.0 * d.nv**4 + 12.0 * d.no * d.nv**3)
+    return {"iter_s": t_iter, "sampled_s": t_other + t_lad, "ladder_blocks": nlad,
+            "ladder_blocks_run": nrun, "pert_t_tflops": ft / t_t / 1e12, "pert_t_s": t_t,
+            "triplets": ntrip}
 
 
 def host_cores():
@@ -145,26 +185,62 @@ def host_cores():
         return os.cpu_count() or 1
 
 
+def _chunks(tasks, k):
+    """Split the task list into k consecutive parts of about equal flops."""
+    total = sum(w for _, w, _ in tasks)
+    out, cur, acc, c = [], [], 0.0, 0
+    for i, t in enumerate(tasks):
+        cur.append(t)
+        acc += t[1]
+        left_tasks, left_chunks = len(tasks) - i - 1, k - len(out) - 1
+        if left_chunks > 0 and (acc >= total * (len(out) + 1) / k or left_tasks == left_chunks):
+            out.append(cur)
+            cur = []
+    out.append(cur)
+    while len(out) < k:
+        out.append([])
+    return out
+
+
 # ---------------------------------------------------------------- main
 
 
 def run_reference(a, wl):
+    """The reference arm: the DF numpy restatement of the reference algorithm
+    on the host cores.  The K timed steps run exactly one CCSD iteration (its
+    tasks in order, split into K parts of about equal flops), so the value is
+    1 / (time of the K steps) iterations per second; the W warm-up steps run
+    the first W parts of a preceding iteration."""
     no, nv, nq = wl
-    K = max(1, min(a.steps, a.cpu_sample))
-    for _ in range(min(a.warmup, 1)):
-        pass  # the oracle has no compile/cache warm-up beyond the first BLAS call
-    rate, dt = cpu_ccsd_rate(no, nv, nq, a.method == "dcsd", K)
+    d = _df_state(a.workload, a.method == "dcsd", a.steps)
+    tasks = d.iteration_tasks()
+    K = max(1, a.steps)
+    parts = _chunks(tasks, K)
+    for p_ in parts[:a.warmup]:
+        for _, _, fn in p_:
+            fn()
+    d.start(d.T1, d.T2)  # the timed iteration starts from the current amplitudes
+    parts = _chunks(d._tasks, K)
+    ms = []
+    for p_ in parts:
+        t0 = time.perf_counter()
+        for _, _, fn in p_:
+            fn()
+        ms.append((time.perf_counter() - t0) * 1000.0)
+    total = sum(ms) / 1000.0
+    rate = 1.0 / total
     cores = host_cores()
+    sample = (f"one CCSD iteration ({total:.1f} s) of the workload in {K} steps of about "
+              "equal flops, density-fitted numpy restatement of the reference algorithm "
+              "(oracle/dfcc.py), BLAS threads = all host cores")
     line = {
         "impl": "reference", "metric": "CCSD iter/s", "value": rate, "unit": "iter/s",
-        "n_gpus": a.gpus, "steps": K, "warmup": a.warmup, "ms_per_step": 1000.0 / rate,
+        "n_gpus": a.gpus, "steps": K, "warmup": a.warmup, "ms_per_step": sum(ms) / K,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": {"workload": f"{a.workload} {a.method.upper()} (o={no}, "
                                                     f"v={nv}, nQ={nq}), synthetic DF factors"},
         "cpu_baseline": {"value": rate, "unit": "iter/s", "cores": cores, "kind": "port",
-                         "sample": f"{K} full CCSD iterations of the workload ({dt:.1f} s), "
-                                   "numpy restatement of the reference algorithm, BLAS threads = "
-                                   "all host cores"},
+                         "sample": sample},
         "e2e": {"value": rate, "unit": "iter/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -326,6 +402,51 @@ def run_sweep(a):
     print(json.dumps(line), flush=True)
 
 
+def measured_peaks():
+    """HBM GB/s, burst and sustained dense BF16 TFLOP/s: MEASURED_PEAKS.json
+    (written per pod by the benchmark driver), else the pool's earlier
+    measurement (6650 GB/s, 1590 / 1400 TFLOP/s)."""
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            m = json.load(f)
+        return {"hbm_gbs": float(m["hbm_gbs"]), "bf16": float(m["bf16_tflops"]),
+                "bf16_sustained": float(m.get("bf16_tflops_sustained", m["bf16_tflops"])),
+                "source": "measured (MEASURED_PEAKS.json)"}
+    except (OSError, KeyError, ValueError):
+        return {"hbm_gbs": 6650.0, "bf16": 1590.0, "bf16_sustained": 1400.0,
+                "source": "fallback (earlier measurement on this pool)"}
+
+
+def cublas_dgemm_peak(torch):
+    """cuBLAS DGEMM 8192^3, best of 3 (FP64 is not in MEASURED_PEAKS.json)."""
+    x = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    y = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    torch.matmul(x, y)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(3):
+        e0_ = torch.cuda.Event(enable_timing=True)
+        e1_ = torch.cuda.Event(enable_timing=True)
+        e0_.record()
+        torch.matmul(x, y)
+        e1_.record()
+        torch.cuda.synchronize()
+        best = min(best, e0_.elapsed_time(e1_) / 1000.0)
+    del x, y
+    torch.cuda.empty_cache()
+    return 2 * 8192.0**3 / best / 1e12
+
+
+def traffic_of(key):
+    """DRAM bytes per launch from an ncu capture (profiles/roofline_traffic.json)."""
+    tp = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    if not os.path.exists(tp):
+        return None
+    with open(tp) as f:
+        return json.load(f).get(key)
+
+
 def main():
     a = parse_args()
     if a.tts:
@@ -353,33 +474,17 @@ def main():
         import datetime
         import torch.distributed as dist
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     torch.cuda.set_device(local)
     import ecgpu
+    from ecgpu._lib import ECG_KT_DGEMM, ECG_KT_TCGEMM, ECG_KT_TRIPLES
     dc = a.method == "dcsd"
     no, nv, nq = wl
     B, h1, e0, no = make_workload(a.workload)
-
-    # measured FP64 GEMM peak (cuBLAS DGEMM 8192^3, best of 3) for the roofline
-    x = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
-    y = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
-    torch.matmul(x, y)
-    torch.cuda.synchronize()
-    best = 1e9
-    for _ in range(3):
-        e0_ = torch.cuda.Event(enable_timing=True)
-        e1_ = torch.cuda.Event(enable_timing=True)
-        e0_.record()
-        torch.matmul(x, y)
-        e1_.record()
-        torch.cuda.synchronize()
-        best = min(best, e0_.elapsed_time(e1_) / 1000.0)
-    fp64_peak = 2 * 8192.0**3 / best / 1e12
-    del x, y
+    peaks = measured_peaks()
+    fp64_peak = cublas_dgemm_peak(torch)
 
     ctx = ecgpu.Context(local)
-    if a.precision == "mixed":
-        ctx.set_precision(ecgpu.ECG_PREC_MIXED)
     ctx.set_system(B, h1, e0, no)
     _, T1, T2 = ctx.mp2()
     stream = torch.cuda.ExternalStream(ctx.stream())
@@ -388,9 +493,24 @@ def main():
     def restart():
         ctx.cc_load(T1, T2)
 
+    def timed_steps(k, step):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(k)]
+        for i in range(k):
+            if i and i % RESTART == 0:
+                restart()
+            flush.zero_()
+            torch.cuda.synchronize()
+            ev[i][0].record(stream)
+            step()
+            ev[i][1].record(stream)
+        torch.cuda.synchronize()
+        return sum(s_.elapsed_time(e_) for s_, e_ in ev)
+
+    # ---- timed FP64 CCSD iterations (the value) ----
     RESTART = 8  # re-seed from MP2 amplitudes every 8 steps (outside timing)
     restart()
-    for w in range(a.warmup):
+    for _ in range(a.warmup):
         ctx.cc_step(dc=dc)
     restart()
     torch.cuda.synchronize()
@@ -401,120 +521,139 @@ def main():
     if clocks:
         clocks.start()
     launches0 = ctx.kernel_launches()
-    ms = []
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(a.steps)]
-    for k in range(a.steps):
-        if k and k % RESTART == 0:
-            restart()
-        flush.zero_()
-        torch.cuda.synchronize()
-        ev[k][0].record(stream)
-        ctx.cc_step(dc=dc)
-        ev[k][1].record(stream)
-    torch.cuda.synchronize()
+    total = timed_steps(a.steps, lambda: ctx.cc_step(dc=dc))
     launches = ctx.kernel_launches() - launches0
     if dist:
         dist.barrier()
     clk = clocks.stop() if clocks else None
-    ms = [s.elapsed_time(e) for s, e in ev]
-    total = sum(ms)
     if dist:
         t = torch.tensor([total], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total = float(t.item())
-    steps_launches = launches - (a.steps // RESTART) * 0
 
-    # e2e: the same iterations through the C ABI with pinned host amplitudes
+    # ---- e2e: the same iterations through the C ABI with pinned host amplitudes ----
     n1, n2 = nv * no, nv * nv * no * no
     T1p = torch.empty((no, nv), dtype=torch.float64, pin_memory=True).numpy().T
     T2p = torch.empty((no, no, nv, nv), dtype=torch.float64, pin_memory=True).numpy().T
     T1p[...] = T1
     T2p[...] = T2
     restart()
-    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(a.steps)]
-    for k in range(a.steps):
-        if k and k % RESTART == 0:
-            restart()
-            T1p[...] = T1
-            T2p[...] = T2
-        flush.zero_()
-        torch.cuda.synchronize()
-        ev2[k][0].record(stream)
+
+    def host_step():
         ctx.cc_step_host(T1p, T2p, dc=dc)
-        ev2[k][1].record(stream)
-    torch.cuda.synchronize()
-    total_e2e = sum(s.elapsed_time(e) for s, e in ev2)
+    total_e2e = timed_steps(a.steps, host_step)
     if dist:
         t = torch.tensor([total_e2e], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_e2e = float(t.item())
 
-    # roofline of the dominant kernel (FP64 GEMM), live GEMM event timing
+    # ---- roofline of the FP64 DMMA GEMM: every GEMM launch of R FP64 steps ----
+    R = 2
     restart()
-    R = 4
     ctx.set_gemm_timing(True)
-    ctx.gemm_time()
+    ctx.kernel_time(ECG_KT_DGEMM)
     for _ in range(R):
         flush.zero_()
         torch.cuda.synchronize()
         ctx.cc_step(dc=dc)
-    gms, glaunch, gflops = ctx.gemm_time()
-    ctx.set_gemm_timing(False)
+    gms, glaunch, gflops = ctx.kernel_time(ECG_KT_DGEMM)
     F = algorithmic_flops(no, nv, nq, dc)
     gemm_s = gms / 1000.0 / R
-    achieved = F / gemm_s / 1e12
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "roofline_traffic.json")
-    if os.path.exists(tp):
-        with open(tp) as f:
-            traffic = json.load(f).get(f"{a.workload}_{a.method}_{a.precision}")
+    rl_dgemm = {"bound": "tensor", "achieved": F / gemm_s / 1e12, "peak": fp64_peak,
+                "unit": "TFLOP/s", "frac": F / gemm_s / 1e12 / fp64_peak,
+                "traffic": traffic_of(f"dgemm_{a.workload}_{a.method}"),
+                "kernel": "dgemm_kernel (FP64 mma.sync, the DMMA pipe), all GEMMs of a step",
+                "algorithmic_flops_per_step": F, "gemm_ms_per_step": gms / R,
+                "gemm_launches_per_step": glaunch / R,
+                "executed_gemm_tflops": gflops / R / gemm_s / 1e12,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 is not in "
+                               "MEASURED_PEAKS.json)",
+                "step_frac": F / (total / a.steps / 1000.0) / 1e12 / fp64_peak}
 
-    # time-to-solution, FP64 vs mixed (split-BF16 tensor-core products + FP64
-    # refinement), full solves from the MP2 guess; energy difference in uEh
-    def solve_timed(prec):
-        ctx.set_precision(prec)
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        flush.zero_()
-        torch.cuda.synchronize()
-        ev0.record(stream)
-        r = ctx.cc_solve(T1, T2, dc=dc)
-        ev1.record(stream)
-        torch.cuda.synchronize()
-        return r, ev0.elapsed_time(ev1) / 1000.0
-    solve_timed(ecgpu.ECG_PREC_MIXED)  # warm the tensor-core path (split buffers)
-    r64, t64 = solve_timed(ecgpu.ECG_PREC_FP64)
-    rmx, tmx = solve_timed(ecgpu.ECG_PREC_MIXED)
-    # mixed-precision iteration rate (same step as above, tensor-core products)
+    # ---- mixed precision: iteration rate and the tcgen05 GEMM roofline ----
     ctx.set_precision(ecgpu.ECG_PREC_MIXED)
     restart()
-    ctx.cc_step(dc=dc)
+    ctx.cc_step(dc=dc)  # first-use set-up of the tensor-core path
     restart()
-    evm = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(a.steps)]
-    for k in range(a.steps):
-        if k and k % RESTART == 0:
-            restart()
+    total_mx = timed_steps(a.steps, lambda: ctx.cc_step(dc=dc))
+    restart()
+    ctx.kernel_time(ECG_KT_TCGEMM)
+    for _ in range(R):
         flush.zero_()
         torch.cuda.synchronize()
-        evm[k][0].record(stream)
         ctx.cc_step(dc=dc)
-        evm[k][1].record(stream)
-    torch.cuda.synchronize()
-    total_mx = sum(s_.elapsed_time(e_) for s_, e_ in evm)
+    tms, tlaunch, twork = ctx.kernel_time(ECG_KT_TCGEMM)
+    ctx.set_gemm_timing(False)
+    tc_ach = twork / (tms / 1000.0) / 1e12
+    rl_tc_ccsd = {"bound": "tensor", "achieved": tc_ach, "peak": peaks["bf16_sustained"],
+                  "unit": "TFLOP/s", "frac": tc_ach / peaks["bf16_sustained"],
+                  "traffic": traffic_of(f"mgemm_ccsd_{a.workload}"),
+                  "kernel": "mgemm_bf16_kernel (tcgen05.mma kind::f16, TMA), all tensor-core "
+                            "GEMMs of a mixed CCSD step",
+                  "work": "BF16 products executed: 2 m n k per slice pair (6 pairs)",
+                  "ms_per_step": tms / R, "launches_per_step": tlaunch / R,
+                  "peak_source": "bf16_tflops_sustained, " + peaks["source"]}
     ctx.set_precision(ecgpu.ECG_PREC_FP64)
-    # (T) on the converged FP64 amplitudes
+
+    # ---- CCSD(T) time-to-solution, FP64 then mixed, from the MP2 guess ----
     ntrip = sum(1 for k_ in range(no) for j_ in range(k_ + 1) for i_ in range(j_ + 1)
                 if not (i_ == j_ == k_))
     ft = ntrip * (12.0 * nv**4 + 12.0 * no * nv**3)
-    evt0, evt1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    evt0.record(stream)
-    et, _ = ctx.pert_t(r64["T1"], r64["T2"])
-    evt1.record(stream)
-    torch.cuda.synchronize()
-    t_t = evt0.elapsed_time(evt1) / 1000.0
+    fcc = algorithmic_flops(no, nv, nq, dc)
+    tts = {}
+    for prec, name in ((ecgpu.ECG_PREC_FP64, "fp64"), (ecgpu.ECG_PREC_MIXED, "mixed")):
+        if name == "mixed":
+            # idle before the second leg, so that it does not start on a GPU
+            # that the first one left power-capped (outside the timed region)
+            time.sleep(COOLDOWN_S)
+        ctx.set_precision(prec)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        torch.cuda.synchronize()
+        ck = Clocks(local) if rank == 0 else None
+        if ck:
+            ck.start()
+        ev[0].record(stream)
+        r = ctx.cc_solve(T1, T2, dc=dc)
+        ev[1].record(stream)
+        et, _ = ctx.pert_t()  # on the converged amplitudes the context holds
+        ev[2].record(stream)
+        torch.cuda.synchronize()
+        ck = ck.stop() if ck else None
+        tcc = ev[0].elapsed_time(ev[1]) / 1000.0
+        tt = ev[1].elapsed_time(ev[2]) / 1000.0
+        tts[name] = {"ccsd_s": tcc, "pert_t_s": tt, "total_s": tcc + tt,
+                     "iterations": r["iterations"], "E_ccsd": r["E"], "E_T": et,
+                     "ccsd_tflops_per_iter": fcc * r["iterations"] / tcc / 1e12,
+                     "pert_t_tflops": ft / tt / 1e12, "clocks": ck}
+    f64, mx = tts["fp64"], tts["mixed"]
+
+    # ---- (T) kernels, mixed: first batch of the sweep (the rest replays from
+    # a CUDA graph and is not event-timed) ----
+    ctx.set_precision(ecgpu.ECG_PREC_MIXED)
+    ctx.set_gemm_timing(True)
+    for fam in (ECG_KT_TCGEMM, ECG_KT_TRIPLES):
+        ctx.kernel_time(fam)
+    ctx.pert_t()
+    wms, wlaunch, wwork = ctx.kernel_time(ECG_KT_TCGEMM)
+    ems, elaunch, ebytes = ctx.kernel_time(ECG_KT_TRIPLES)
+    ctx.set_gemm_timing(False)
+    ctx.set_precision(ecgpu.ECG_PREC_FP64)
+    w_ach = wwork / (wms / 1000.0) / 1e12 if wms > 0 else None
+    e_ach = ebytes / (ems / 1000.0) / 1e9 if ems > 0 else None
+    rl_tc_t = {"bound": "tensor", "achieved": w_ach, "peak": peaks["bf16_sustained"],
+               "unit": "TFLOP/s", "frac": w_ach / peaks["bf16_sustained"] if w_ach else None,
+               "traffic": traffic_of(f"mgemm_pert_t_{a.workload}"),
+               "kernel": "mgemm_bf16_kernel, batched four-segment (T) W GEMMs (2 BF16 slices, "
+                         "3 pairs), first batch of the sweep",
+               "launches": wlaunch, "ms": wms,
+               "peak_source": "bf16_tflops_sustained, " + peaks["source"]}
+    rl_energy = {"bound": "hbm", "achieved": e_ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                 "frac": e_ach / peaks["hbm_gbs"] if e_ach else None,
+                 "traffic": traffic_of(f"triples_energy_{a.workload}"),
+                 "kernel": "triples_energy_kernel (FP32 K of mixed (T)), first batch",
+                 "bytes_per_launch": ebytes / max(elaunch, 1), "ms_per_launch":
+                 ems / max(elaunch, 1), "work": "bytes of K read once per element",
+                 "peak_source": "hbm_gbs, " + peaks["source"]}
 
     value = world * a.steps / (total / 1000.0)
     line = {
@@ -524,35 +663,39 @@ def main():
         "data": "synthetic",
         "config": {"workload": f"{a.workload} {a.method.upper()} (o={no}, v={nv}, nQ={nq}), "
                                "seeded synthetic DF factors, canonical HF reference",
-                   "precision": a.precision, "l2": "flushed (256 MiB write) between steps",
+                   "precision": "fp64",
+                   "l2": "inputs larger than L2 (T2 466 MB, B 792 MB) and L2 flushed "
+                         "(256 MiB write) between steps",
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": world * a.steps / (total_e2e / 1000.0), "unit": "iter/s",
                 "h2d_bytes_per_step": 8 * (n1 + n2), "d2h_bytes_per_step": 8 * (n1 + n2)},
-        "gpu_launches": steps_launches,
-        "roofline": {"bound": "tensor", "achieved": achieved, "peak": fp64_peak,
-                     "unit": "TFLOP/s", "frac": achieved / fp64_peak, "traffic": traffic,
-                     "kernel": "dgemm_kernel (FP64 mma.sync m8n8k4), all GEMMs of a step",
-                     "algorithmic_flops_per_step": F, "gemm_ms_per_step": gms / R,
-                     "gemm_launches_per_step": glaunch / R,
-                     "executed_gemm_tflops": gflops / R / gemm_s / 1e12,
-                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 is not in "
-                                    "MEASURED_PEAKS.json)",
-                     "step_frac": F / (total / a.steps / 1000.0) / 1e12 / fp64_peak},
+        "gpu_launches": launches,
+        "roofline": rl_dgemm,
+        "rooflines": {"dgemm_fp64_ccsd": rl_dgemm, "mgemm_bf16_ccsd": rl_tc_ccsd,
+                      "mgemm_bf16_pert_t": rl_tc_t, "triples_energy": rl_energy},
         "clocks": clk,
-        "mixed": {"iter_per_s": world * a.steps / (total_mx / 1000.0),
-                  "precision": "split-BF16 (3 slices, 6 products) tcgen05 GEMMs, FP32 accumulate",
-                  "tts_fp64_s": t64, "tts_mixed_s": tmx, "tts_speedup": t64 / tmx,
-                  "iterations_fp64": r64["iterations"], "iterations_mixed": rmx["iterations"],
-                  "dE_uEh": abs(rmx["E"] - r64["E"]) * 1e6, "E_corr_fp64": r64["E"]},
-        "pert_t": {"seconds": t_t, "tflops": ft / t_t / 1e12, "E_T": et, "triplets": ntrip,
-                   "algorithmic_flops": ft, "precision": "fp64"},
+        "mixed": {"metric": "CCSD(T) time-to-solution from the MP2 guess, FP64 vs mixed",
+                  "precision": "split-BF16 tcgen05 GEMMs (CCSD: 3 slices, 6 products; (T): "
+                               "2 slices, 3 products), FP32 accumulate, FP64 refinement",
+                  "fp64": f64, "mixed": mx, "tts_speedup": f64["total_s"] / mx["total_s"],
+                  "dE_uEh": abs((mx["E_ccsd"] + mx["E_T"]) - (f64["E_ccsd"] + f64["E_T"])) * 1e6,
+                  "dE_T_uEh": abs(mx["E_T"] - f64["E_T"]) * 1e6,
+                  "ccsd_iter_per_s": world * a.steps / (total_mx / 1000.0),
+                  "triplets": ntrip, "pert_t_algorithmic_flops": ft,
+                  "order": f"fp64, {COOLDOWN_S:.0f} s idle, mixed"},
     }
     if rank == 0 and world == 1 and a.cpu_sample > 0:
-        rate, dt = cpu_ccsd_rate(no, nv, nq, dc, a.cpu_sample)
-        line["cpu_baseline"] = {"value": rate, "unit": "iter/s", "cores": host_cores(),
-                                "kind": "port",
-                                "sample": f"{a.cpu_sample} CCSD iterations of the same workload "
-                                          f"({dt:.1f} s), numpy restatement, all host cores"}
+        cb = cpu_baseline_sample(a.workload, dc, nblocks=a.cpu_sample)
+        line["cpu_baseline"] = {
+            "value": 1.0 / cb["iter_s"], "unit": "iter/s", "cores": host_cores(),
+            "kind": "port",
+            "sample": (f"one CCSD iteration of the same workload with the ladder on "
+                       f"{cb['ladder_blocks_run']} of its {cb['ladder_blocks']} a-blocks "
+                       f"({cb['sampled_s']:.1f} s; the other blocks at the sampled block's "
+                       f"time: {cb['iter_s']:.1f} s per iteration), density-fitted numpy "
+                       "restatement (oracle/dfcc.py), BLAS threads = all host cores; (T) on "
+                       f"{cb['triplets']} triplets"),
+            "pert_t_tflops": cb["pert_t_tflops"]}
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()

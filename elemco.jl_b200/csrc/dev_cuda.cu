@@ -643,48 +643,78 @@ int splitk_reduce_f32(stream_t s, int64_t m, int64_t n, int S, const float* P, d
   return launched();
 }
 
-// Event-pair pool for GEMM timing.
-static bool g_timing = false;
-static std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_ev;
-static size_t g_ev_used = 0;
-static double g_flops = 0.0;
+// Event timing of kernel families (a diagnostic; enable, run, read): each
+// timed launch is bracketed by an event pair on its stream, and its
+// algorithmic work (flops or bytes) is added to the family's total.
+// Launches made during stream capture are not timed.
+namespace {
+struct Family {
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+  size_t used = 0;
+  double work = 0.0;
+};
+bool g_timing = false;
+Family g_fam[KT_FAMILIES];
+std::mutex g_fam_mu;
+}  // namespace
 
 void gemm_timing(bool enable) {
+  std::lock_guard<std::mutex> lk(g_fam_mu);
   g_timing = enable;
-  g_ev_used = 0;
-  g_flops = 0.0;
+  for (auto& f : g_fam) {
+    f.used = 0;
+    f.work = 0.0;
+  }
 }
 
-void gemm_time(double* ms, int64_t* n, double* flops) {
+int ktime_begin(stream_t s, int family) {
+  if (!g_timing || family < 0 || family >= KT_FAMILIES || capturing((cudaStream_t)s)) return -1;
+  std::lock_guard<std::mutex> lk(g_fam_mu);
+  Family& f = g_fam[family];
+  if (f.used == f.ev.size()) {
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    f.ev.push_back({a, b});
+  }
+  cudaEventRecord(f.ev[f.used].first, (cudaStream_t)s);
+  return (int)f.used++;
+}
+
+void ktime_end(stream_t s, int family, int slot, double work) {
+  if (slot < 0) return;
+  std::lock_guard<std::mutex> lk(g_fam_mu);
+  Family& f = g_fam[family];
+  cudaEventRecord(f.ev[slot].second, (cudaStream_t)s);
+  f.work += work;
+}
+
+void kernel_time(int family, double* ms, int64_t* n, double* work) {
+  std::lock_guard<std::mutex> lk(g_fam_mu);
   double tot = 0.0;
-  for (size_t i = 0; i < g_ev_used; ++i) {
-    cudaEventSynchronize(g_ev[i].second);
+  Family& f = g_fam[family < 0 || family >= KT_FAMILIES ? 0 : family];
+  for (size_t i = 0; i < f.used; ++i) {
+    cudaEventSynchronize(f.ev[i].second);
     float t = 0.f;
-    cudaEventElapsedTime(&t, g_ev[i].first, g_ev[i].second);
+    cudaEventElapsedTime(&t, f.ev[i].first, f.ev[i].second);
     tot += t;
   }
   if (ms) *ms = tot;
-  if (n) *n = (int64_t)g_ev_used;
-  if (flops) *flops = g_flops;
-  g_ev_used = 0;
-  g_flops = 0.0;
+  if (n) *n = (int64_t)f.used;
+  if (work) *work = f.work;
+  f.used = 0;
+  f.work = 0.0;
 }
+
+void gemm_time(double* ms, int64_t* n, double* flops) { kernel_time(KT_DGEMM, ms, n, flops); }
 
 static int gemm_launch(stream_t s, const Gemm& q);
 
 int gemm_strided(stream_t s, const Gemm& q) {
   if (!g_timing || q.m <= 0 || q.n <= 0 || q.batch <= 0 || q.k <= 0) return gemm_launch(s, q);
-  if (g_ev_used == g_ev.size()) {
-    cudaEvent_t a, b;
-    cudaEventCreate(&a);
-    cudaEventCreate(&b);
-    g_ev.push_back({a, b});
-  }
-  auto& e = g_ev[g_ev_used++];
-  cudaEventRecord(e.first, (cudaStream_t)s);
+  const int slot = ktime_begin(s, KT_DGEMM);
   int r = gemm_launch(s, q);
-  cudaEventRecord(e.second, (cudaStream_t)s);
-  g_flops += 2.0 * (double)q.m * (double)q.n * (double)q.k * (double)q.batch;
+  ktime_end(s, KT_DGEMM, slot, 2.0 * (double)q.m * (double)q.n * (double)q.k * (double)q.batch);
   return r;
 }
 
@@ -1601,6 +1631,10 @@ int triples_energy_batched(stream_t s, int nv, int nitems, const void* K, const 
   }
   cudaStream_t st = (cudaStream_t)s;
   const dim3 grid((unsigned)g, (unsigned)nitems);
+  // algorithmic bytes: each element of K (and of KU) read once
+  const int slot = ktime_begin(s, KT_TRIPLES);
+  const double kbytes = (double)nitems * (double)nv * nv * nv * (k_f32 ? 4.0 : 8.0) *
+                        (KU ? 2.0 : 1.0);
   if (k_f32) {
     if (KU)
       triples_energy_kernel<float, true><<<grid, 512, EnergySmem<float, true>::BYTES, st>>>(
@@ -1619,6 +1653,7 @@ int triples_energy_batched(stream_t s, int nv, int nitems, const void* K, const 
           nv, (const double*)K, nullptr, kstride, eijk_tab, ev, tt_tab, tri, (int)ntri,
           scratch);
   }
+  ktime_end(s, KT_TRIPLES, slot, kbytes);
   int e = launched();
   if (e) return e;
   final_sum_pairs_kernel<<<2 * nitems, 256, 0, st>>>(g, scratch, out);

@@ -616,6 +616,19 @@ TcSegs make_segs(int nseg, const int64_t* k) {
   return sg;
 }
 
+// Total K depth of the segments (without the zero padding of each segment's
+// last k-block).
+double seg_depth(const TcSegs& sg) {
+  double k = 0.0;
+  int prev = 0;
+  for (int t = 0; t < TC_MAX_SEG; ++t) {
+    const int nkb = sg.kb_end[t] - prev;
+    if (nkb > 0) k += (double)(nkb - 1) * TK + 16.0 * sg.kk_last[t];
+    prev = sg.kb_end[t];
+  }
+  return k;
+}
+
 // Checks the segments of g (A[s]/B[s] until the first null A[s]) and returns
 // their number, or 0 if they do not form a valid GEMM of g's shape.
 int gemm_segments(const TcGemm& g, int64_t* k) {
@@ -692,10 +705,14 @@ int launch_tc(cudaStream_t st, const TcMaps& maps, const TcSegs& segs, int kbt, 
   const int64_t items = (int64_t)mt * nt * S;
   const unsigned grid = (unsigned)(items < 148 ? items : 148);
   const unsigned long long wns = wait_bound(st);
+  // useful BF16 products: 2 m n K per slice pair (zero padding not counted)
+  const double work = 2.0 * (double)m * (double)n * (double)seg_depth(segs) * Cfg::NPAIR;
+  const int slot = ktime_begin((stream_t)st, KT_TCGEMM);
   if (S == 1) {
     mgemm_bf16_kernel<NSL, TN><<<grid, THREADS_TC, Cfg::SMEM_BYTES, st>>>(
         maps, out, m, n, alpha, beta, segs, kps, kbt, 0, mt, nt, 1, nullptr, wns);
     note_launches(1);
+    ktime_end((stream_t)st, KT_TCGEMM, slot, work);
     return (int)cudaGetLastError();
   }
   if (out.f32 || out.dn > 0 || out.dm > 0) return (int)cudaErrorInvalidValue;
@@ -709,8 +726,9 @@ int launch_tc(cudaStream_t st, const TcMaps& maps, const TcSegs& segs, int kbt, 
   note_launches(1);
   int e = (int)cudaGetLastError();
   if (e) return e;
-  return splitk_reduce_f32((stream_t)st, m, n, S, P, alpha, beta, (double*)out.C, out.scm,
-                           out.scn);
+  e = splitk_reduce_f32((stream_t)st, m, n, S, P, alpha, beta, (double*)out.C, out.scm, out.scn);
+  ktime_end((stream_t)st, KT_TCGEMM, slot, work);
+  return e;
 }
 
 }  // namespace
@@ -916,9 +934,12 @@ void launch_batched(cudaStream_t st, const TcOut& out, const TcGemm& g, const Tc
   const unsigned grid = (unsigned)(items < 148 ? items : 148);
   TcMaps dummy;
   std::memset(&dummy, 0, sizeof(dummy));
+  const int slot = ktime_begin((stream_t)st, KT_TCGEMM);
   mgemm_bf16_kernel<NSL, TN><<<grid, THREADS_TC, Cfg::SMEM_BYTES, st>>>(
       dummy, out, g.m, g.n, g.alpha, g.beta, segs, kbt, kbt, c_stride, mt, nt, batch,
       (const TcMaps*)mtab, wait_bound(st));
+  ktime_end((stream_t)st, KT_TCGEMM, slot,
+            2.0 * (double)g.m * (double)g.n * (double)seg_depth(segs) * Cfg::NPAIR * batch);
 }
 }  // namespace
 

@@ -556,6 +556,15 @@ int ecg_set_gemm_timing(ecg_ctx* c, int enable) {
   return ECG_OK;
 }
 
+int ecg_kernel_time(ecg_ctx* c, int32_t family, double* ms, int64_t* launches, double* work) {
+  if (!c) return ECG_ERR_ARG;
+  return guarded(c, [&] {
+    if (family < 0 || family >= dev::KT_FAMILIES) throw Error(ECG_ERR_ARG, "unknown family");
+    check(dev::sync(c->st), "sync");
+    dev::kernel_time(family, ms, launches, work);
+  });
+}
+
 int ecg_gemm_time(ecg_ctx* c, double* ms, int64_t* launches, double* flops) {
   if (!c) return ECG_ERR_ARG;
   return guarded(c, [&] {

@@ -259,9 +259,17 @@ int splitk_reduce(stream_t s, int64_t m, int64_t n, int S, const double* P, doub
 int splitk_reduce_f32(stream_t s, int64_t m, int64_t n, int S, const float* P, double alpha,
                       double beta, double* C, int64_t scm, int64_t scn);
 
-// GEMM event timing (process-wide): enable, then read and reset the totals.
+// Event timing of kernel families (process-wide diagnostic): enable, then
+// read and reset a family's summed device ms, launch count and algorithmic
+// work (flops for the GEMMs, bytes for the (T) energy kernel).  Launches
+// during stream capture are not timed.  ktime_begin returns a slot (-1: not
+// timed) for ktime_end, which records the end event and adds the work.
+enum { KT_DGEMM = 0, KT_TCGEMM = 1, KT_TRIPLES = 2, KT_FAMILIES = 3 };
 void gemm_timing(bool enable);
-void gemm_time(double* ms, int64_t* launches, double* flops);
+void gemm_time(double* ms, int64_t* launches, double* flops);  // KT_DGEMM
+void kernel_time(int family, double* ms, int64_t* launches, double* work);
+int ktime_begin(stream_t s, int family);
+void ktime_end(stream_t s, int family, int slot, double work);
 
 // Symmetric/antisymmetric particle-particle ladder helpers.  Pair tables hold
 // (x,y) as int pairs: cdp enumerates c<=d (d outer), ijp i<=j, pairs the

@@ -24,6 +24,9 @@ ECG_DIIS_CS = 0
 ECG_DIIS_PLAIN = 1
 ECG_OPT_TRIPLES_BATCH = 1
 ECG_OPT_TC_WAIT_NS = 2
+ECG_KT_DGEMM = 0
+ECG_KT_TCGEMM = 1
+ECG_KT_TRIPLES = 2
 
 _NAMES = {1: "ECG_ERR_ARG", 2: "ECG_ERR_CUDA", 3: "ECG_ERR_OOM", 4: "ECG_ERR_NONFINITE",
           5: "ECG_ERR_TIMEOUT", 6: "ECG_ERR_STATE"}
@@ -80,6 +83,7 @@ SIGNATURES = {
     "ecg_get_stream": (C.c_int, [_P, C.POINTER(_P)]),
     "ecg_set_gemm_timing": (C.c_int, [_P, C.c_int]),
     "ecg_gemm_time": (C.c_int, [_P, _D, C.POINTER(C.c_int64), _D]),
+    "ecg_kernel_time": (C.c_int, [_P, C.c_int32, _D, C.POINTER(C.c_int64), _D]),
     "ecg_diag_gemm": (C.c_int, [_P, C.c_char, C.c_char, C.c_int64, C.c_int64, C.c_int64,
                                 C.c_double, _D, C.c_int64, _D, C.c_int64, C.c_double, _D,
                                 C.c_int64]),

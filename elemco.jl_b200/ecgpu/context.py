@@ -199,6 +199,14 @@ class Context:
         self._chk(self._L.ecg_gemm_time(self._h, C.byref(ms), C.byref(n), C.byref(fl)))
         return ms.value, n.value, fl.value
 
+    def kernel_time(self, family):
+        """(ms, launches, work) of a kernel family (ECG_KT_*) since the last read."""
+        ms, w = C.c_double(), C.c_double()
+        n = C.c_int64()
+        self._chk(self._L.ecg_kernel_time(self._h, int(family), C.byref(ms), C.byref(n),
+                                          C.byref(w)))
+        return ms.value, n.value, w.value
+
     def diag_gemm(self, ta, tb, alpha, A, B, beta, Cm):
         A, B = as_f(A), as_f(B)
         Cm = as_f(Cm).copy(order="F")

@@ -186,12 +186,23 @@ int ecg_get_stream(ecg_ctx* ctx, void** stream);
 /* Number of kernels launched through the library in this process so far. */
 int64_t ecg_kernel_launches(const ecg_ctx* ctx);
 
-/* GEMM timing: when enabled, every FP64 GEMM launch of this process is
- * bracketed by CUDA events on its stream; ecg_gemm_time returns the summed
- * device milliseconds, the launch count and the summed 2*m*n*k*batch flops
- * since the last reset, and resets them. */
+/* Kernel timing: when enabled, every launch of the FP64 GEMM, the tensor-core
+ * GEMM and the (T) energy kernel in this process (outside CUDA graph
+ * capture) is bracketed by CUDA events on its stream.  ecg_kernel_time
+ * returns, for one family, the summed device milliseconds, the launch count
+ * and the summed algorithmic work since the last read, and resets them:
+ *   ECG_KT_DGEMM    FP64 GEMM (with its split-K reduction), flops 2*m*n*k*batch
+ *   ECG_KT_TCGEMM   split-BF16 tcgen05 GEMM (kernel and split-K reduction),
+ *                   BF16 product flops 2*m*n*k*(slice products)
+ *   ECG_KT_TRIPLES  (T) energy kernel, bytes of K (and K of Lambda) read
+ * ecg_gemm_time is ecg_kernel_time for ECG_KT_DGEMM. */
+#define ECG_KT_DGEMM 0
+#define ECG_KT_TCGEMM 1
+#define ECG_KT_TRIPLES 2
 int ecg_set_gemm_timing(ecg_ctx* ctx, int enable);
 int ecg_gemm_time(ecg_ctx* ctx, double* ms, int64_t* launches, double* flops);
+int ecg_kernel_time(ecg_ctx* ctx, int32_t family, double* ms, int64_t* launches,
+                    double* work);
 
 /* The library's GEMM / permutation on host buffers (column-major), for
  * self-tests of the device kernels:
