@@ -13,7 +13,8 @@
 
 using namespace ecg;
 
-struct ecg_ctx : Ctx {};
+static thread_local std::string g_noctx_err;
+void ecg::noctx_error_store(const char* msg) { g_noctx_err = msg; }
 
 struct ecg_diis {
   ecg_ctx* ctx;
@@ -22,27 +23,6 @@ struct ecg_diis {
   double* v;
   double* r;
 };
-
-static thread_local std::string g_noctx_err;
-
-template <class F>
-static int guarded(Ctx* c, F&& f) {
-  try {
-    f();
-    if (c) c->err.clear();
-    return ECG_OK;
-  } catch (const Error& e) {
-    if (c) c->err = e.what();
-    else g_noctx_err = e.what();
-    return e.code;
-  } catch (const std::bad_alloc&) {
-    if (c) c->err = "host out of memory";
-    return ECG_ERR_OOM;
-  } catch (const std::exception& e) {
-    if (c) c->err = e.what();
-    return ECG_ERR_ARG;
-  }
-}
 
 static void need_system(Ctx& c) {
   if (!c.have_system) throw Error(ECG_ERR_STATE, "no system set (call ecg_set_system first)");

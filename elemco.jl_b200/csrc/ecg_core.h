@@ -2,6 +2,8 @@
 // amplitudes, DIIS history and workspace for one closed-shell CC problem.
 #pragma once
 #include <cstdint>
+#include <exception>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -119,4 +121,28 @@ void diis_perform(Ctx& c, DiisState& d, double* amps, const double* res);
 double scal(Ctx& c, int i);
 void sync_scalars(Ctx& c, int count);
 
+// Runs f, turning the library's exceptions into a status code and a message
+// (per context, or per thread for calls without one).
+void noctx_error_store(const char* msg);  // the message ecg_last_error(NULL) returns
+template <class F>
+int guarded(Ctx* c, F&& f) {
+  try {
+    f();
+    if (c) c->err.clear();
+    return ECG_OK;
+  } catch (const Error& e) {
+    if (c) c->err = e.what();
+    else noctx_error_store(e.what());
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    if (c) c->err = "host out of memory";
+    return ECG_ERR_OOM;
+  } catch (const std::exception& e) {
+    if (c) c->err = e.what();
+    return ECG_ERR_ARG;
+  }
+}
+
 }  // namespace ecg
+
+struct ecg_ctx : ecg::Ctx {};

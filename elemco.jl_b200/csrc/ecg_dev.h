@@ -286,6 +286,30 @@ int ladder_pack_v(stream_t s, int nv, int a0, int na, int npairs, const int* pai
 int ladder_unpack(stream_t s, int nv, int no, int a0, int npairs, const int* pairs,
                   const int* ijp, const double* Lp, const double* Lm, double* R2);
 
+// Gaussian integrals over contracted Cartesian shells (dev_ints.cu).  A shell
+// has centre (x, y, z), angular momentum l <= INT_LMAX, nprim primitives whose
+// exponents/coefficients start at poff in the exponent/coefficient arrays,
+// and its first Cartesian function at boff of the output dimension.
+// Components of degree l are ordered i = l..0, j = l-i..0 (x^i y^j z^k).
+// Outputs are accumulated (zero them first).
+constexpr int INT_LMAX = 4;   // largest shell angular momentum (g)
+constexpr int INT_LTOT = 12;  // largest l_a + l_b + l_c (+ l_d) of a Coulomb integral
+struct IntShell {
+  double x, y, z;
+  int l, nprim, poff, boff;
+};
+// kind 0 overlap, 1 kinetic, 2 nuclear attraction (natom charges Z at xyz),
+// 3 dipole about origin (three nn x nn matrices); out[m + nn*n].
+int int1e_cart(stream_t s, int kind, const IntShell* sh, int nsh, const double* ex,
+               const double* co, int natom, const double* Z, const double* xyz,
+               const double* origin, int64_t nn, double* out);
+// (P|Q), out[P + np*Q]
+int int2c2e_cart(stream_t s, const IntShell* aux, int nsh, const double* ex, const double* co,
+                 int64_t np, double* out);
+// (mn|P), out[m + nm*(n + nm*P)]; ex/co hold both bases' primitives
+int int3c2e_cart(stream_t s, const IntShell* ao, int nao_sh, const IntShell* aux, int naux_sh,
+                 const double* ex, const double* co, int64_t nm, double* out);
+
 // Count of kernels launched through this layer in this process.
 int64_t launches();
 void note_launches(int n);  // add n launches made outside dev_cuda.cu

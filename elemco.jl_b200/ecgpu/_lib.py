@@ -27,6 +27,10 @@ ECG_OPT_TC_WAIT_NS = 2
 ECG_KT_DGEMM = 0
 ECG_KT_TCGEMM = 1
 ECG_KT_TRIPLES = 2
+ECG_INT_OVERLAP = 0
+ECG_INT_KINETIC = 1
+ECG_INT_NUCLEAR = 2
+ECG_INT_DIPOLE = 3
 
 _NAMES = {1: "ECG_ERR_ARG", 2: "ECG_ERR_CUDA", 3: "ECG_ERR_OOM", 4: "ECG_ERR_NONFINITE",
           5: "ECG_ERR_TIMEOUT", 6: "ECG_ERR_STATE"}
@@ -46,8 +50,16 @@ class CcOpts(C.Structure):
                 ("resthr", C.c_double), ("diis_dot", C.c_int32)]
 
 
+class Shells(C.Structure):
+    """``ecg_shells``: a basis as plain arrays (include/ecgpu.h)."""
+    _fields_ = [("nshell", C.c_int32), ("l", C.POINTER(C.c_int32)),
+                ("nprim", C.POINTER(C.c_int32)), ("centre", C.POINTER(C.c_double)),
+                ("exps", C.POINTER(C.c_double)), ("coefs", C.POINTER(C.c_double))]
+
+
 _D = C.POINTER(C.c_double)
 _P = C.c_void_p
+_S = C.POINTER(Shells)
 _lib = None
 
 # name -> (restype, argtypes)
@@ -89,6 +101,10 @@ SIGNATURES = {
                                 C.c_int64]),
     "ecg_diag_permute": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int),
                                    C.c_double, _D, C.c_double, _D]),
+    "ecg_shells_nbf": (C.c_int, [_S, C.POINTER(C.c_int32)]),
+    "ecg_int1e": (C.c_int, [_P, C.c_int32, _S, C.c_int32, _D, _D, _D, _D]),
+    "ecg_int2c2e": (C.c_int, [_P, _S, _D]),
+    "ecg_int3c2e": (C.c_int, [_P, _S, _S, _D]),
     "ecg_gemm_noalloc": (C.c_int, [C.c_char, C.c_char, C.c_int64, C.c_int64, C.c_int64,
                                    C.c_double, _P, C.c_int64, _P, C.c_int64, C.c_double, _P,
                                    C.c_int64, _P, C.POINTER(C.c_int32)]),

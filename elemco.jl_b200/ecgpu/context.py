@@ -207,6 +207,38 @@ class Context:
                                           C.byref(w)))
         return ms.value, n.value, w.value
 
+    # ------------------------------------------------------------ integrals
+    def int1e(self, kind, shells, charges=None, xyz=None, origin=None):
+        """ecg_int1e over a :class:`ecgpu.basis.ShellArrays` basis: (n, n), or
+        (3, n, n) for the dipole, column-major values in numpy's (m, n) order."""
+        from ._lib import ECG_INT_DIPOLE
+        n = shells.nbf
+        ncomp = 3 if kind == ECG_INT_DIPOLE else 1
+        out = np.zeros(ncomp * n * n)
+        st = shells.struct()
+        Z = None if charges is None else np.ascontiguousarray(charges, dtype=np.float64)
+        X = None if xyz is None else np.ascontiguousarray(xyz, dtype=np.float64).ravel()
+        O = None if origin is None else np.ascontiguousarray(origin, dtype=np.float64).ravel()
+        self._chk(self._L.ecg_int1e(self._h, int(kind), C.byref(st), 0 if Z is None else len(Z),
+                                    dptr(Z), dptr(X), dptr(O), dptr(out)))
+        out = out.reshape(ncomp, n, n).transpose(0, 2, 1)
+        return out if ncomp == 3 else out[0]
+
+    def int2c2e(self, fit):
+        n = fit.nbf
+        out = np.zeros(n * n)
+        st = fit.struct()
+        self._chk(self._L.ecg_int2c2e(self._h, C.byref(st), dptr(out)))
+        return out.reshape(n, n).T
+
+    def int3c2e(self, ao, fit):
+        """(mn|P) as an F-ordered (nao, nao, naux) array."""
+        n, m = ao.nbf, fit.nbf
+        out = np.zeros((n, n, m), order="F")
+        sa, sf = ao.struct(), fit.struct()
+        self._chk(self._L.ecg_int3c2e(self._h, C.byref(sa), C.byref(sf), dptr(out)))
+        return out
+
     def diag_gemm(self, ta, tb, alpha, A, B, beta, Cm):
         A, B = as_f(A), as_f(B)
         Cm = as_f(Cm).copy(order="F")

@@ -217,6 +217,50 @@ int ecg_diag_permute(ecg_ctx* ctx, int nd, const int64_t* in_dims, const int* pe
                      const double* in, double beta, double* out);
 
 /* ------------------------------------------------------------------------
+ * Gaussian integrals (the molecular-integral producer of the DF-HF and
+ * integral-transformation steps before the CC path).  A basis is a list of
+ * contracted shells in plain arrays, as ElemCo.jl's BasisSet hands them to
+ * libcint (src/system/libcint5.jl:25-81, src/system/basisset.jl):
+ *   l[s]       angular momentum of shell s (0..4)
+ *   nprim[s]   its primitives
+ *   centre     3 doubles per shell (bohr)
+ *   exps/coefs exponents and contraction coefficients, shell after shell, the
+ *              coefficients multiplying normalised primitives as in the
+ *              basis-set files
+ * Functions are real solid harmonics (2l+1 per shell, m = -l..l) normalised
+ * to unit self-overlap; outputs are column-major over them.  The engine is
+ * McMurchie-Davidson on the GPU.
+ * ---------------------------------------------------------------------- */
+typedef struct ecg_shells {
+  int32_t nshell;
+  const int32_t* l;
+  const int32_t* nprim;
+  const double* centre;
+  const double* exps;
+  const double* coefs;
+} ecg_shells;
+
+/* Number of (spherical) basis functions. */
+int ecg_shells_nbf(const ecg_shells* basis, int32_t* nbf);
+
+/* One-electron integrals (n x n; ECG_INT_DIPOLE: three matrices x, y, z of
+ * <m|(r - origin)|n>, origin NULL = 0): overlap, kinetic, nuclear attraction
+ * over natom point charges, dipole.  The reference's overlap/kinetic/nuclear
+ * (src/system/integrals_2idx.jl:11-100, libcint int1e_ovlp/kin/nuc). */
+#define ECG_INT_OVERLAP 0
+#define ECG_INT_KINETIC 1
+#define ECG_INT_NUCLEAR 2
+#define ECG_INT_DIPOLE 3
+int ecg_int1e(ecg_ctx* ctx, int32_t kind, const ecg_shells* basis, int32_t natom,
+              const double* charge, const double* atom_xyz, const double* origin, double* out);
+/* Two-centre Coulomb metric (P|Q) of a fitting basis (naux x naux):
+ * eri_2e2idx (src/system/integrals_2idx.jl, libcint int2c2e). */
+int ecg_int2c2e(ecg_ctx* ctx, const ecg_shells* fit, double* out);
+/* Three-centre Coulomb integrals (mn|P), out[m + nao*(n + nao*P)]:
+ * eri_2e3idx (src/system/integrals_2e3idx.jl:108-158, libcint int3c2e). */
+int ecg_int3c2e(ecg_ctx* ctx, const ecg_shells* ao, const ecg_shells* fit, double* out);
+
+/* ------------------------------------------------------------------------
  * Allocation-free entry point (no counterpart in the reference).
  *
  * For callers that must not allocate device memory in their call path — code

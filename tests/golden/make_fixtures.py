@@ -11,7 +11,7 @@ Run from the repo root:  python tests/golden/make_fixtures.py REFERENCE_ROOT
 Sources (paths inside the ElemCo.jl project):
   test/files/H2O.FCIDUMP      closed shell, NORB=23, NELEC=8   (test/h2o.jl:16)
   test/files/H2O_ST1.FCIDUMP  non-Hermitian (ST=1), NORB=24    (test/h2o_st1.jl:15)
-  energies pinned in test/h2o.jl:6-10 and test/h2o_st1.jl:6-9
+  energies pinned in test/h2o.jl:6-10, test/h2o_st1.jl:6-9 and test/df_hf.jl:5-7
 """
 import json
 import os
@@ -92,6 +92,13 @@ def main(refroot):
             "CCSD(T)c": -0.329259440500,
             "LCCSD(T)c": -0.326915143863,
             "DCSDc": -0.328754956597,
+        },
+        "df_hf": {
+            "_source": "test/df_hf.jl:5-7: water (bohr, :12-15), cc-pVDZ, jkfit "
+                       "cc-pVTZ-JKFIT, mpfit cc-pVDZ-MPFIT, frozen O 1s",
+            "HF": -76.02145513971418,
+            "MP2c": -0.204723138509385,
+            "DCSDc": -0.219150244853825,
         },
         "h2o_st1": {
             "fixture": "h2o_st1_fcidump.npz",
