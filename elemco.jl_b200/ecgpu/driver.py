@@ -45,7 +45,9 @@ def _default_options():
                      properties=False, save="cc_amplitudes", save_lm="cc_multipliers",
                      nomp2=0),
         "diis": _Group(maxdiis=6, resthr=10.0, crop=False, maxcrop=3, dot="cs"),
-        "cholesky": _Group(thr=1.0e-12),
+        "cholesky": _Group(thr=1.0e-12, thred=1.0e-6),
+        "scf": _Group(thr=1.0e-10, thren=-1.0, maxit=50),
+        "wf": _Group(core="large"),
         "gpu": _Group(precision="fp64", device=0),
     }
 
@@ -59,6 +61,9 @@ class ECInfo:
         self.ext = ".bin"
         self.fd = None
         self._ctx = None
+        self.system = None
+        self.hf = None
+        self._ncore = 0
 
     def set(self, group, **kw):
         """``@set group key=val`` (src/ElemCo.jl:331-357)."""
@@ -67,6 +72,19 @@ class ECInfo:
             if k not in g:
                 raise KeyError(f"unknown option {group}.{k}")
             g[k] = v
+
+    def set_system(self, mol, basis):
+        """The molecule (:class:`ecgpu.molecules.Molecule`, bohr) and its basis
+        sets {"ao": ..., "jkfit": ..., "mpfit": ...}, as
+        ``ECInfo(system=parse_geometry(xyz, basis))`` (src/infos/ecinfos.jl)."""
+        self.system = (mol, {k.lower(): v for k, v in basis.items()})
+        self.hf = None
+
+    def mo_dipole(self, origin=(0.0, 0.0, 0.0)):
+        """<p|r - origin|q> over the active orbitals of the last dfints (3, n, n)."""
+        hf, nc = self.hf, self._ncore
+        C = hf.C[:, nc:]
+        return np.array([C.T @ D @ C for D in hf.ints.dipole(origin)])
 
     def context(self):
         if self._ctx is None:
@@ -377,6 +395,39 @@ def rrule_cc_energy(EC, method, h=None, fcidump=""):
         return dE * G
 
     return E, pullback
+
+
+def dfhf(EC):
+    """``@dfhf`` (src/scf/dfhf.jl:24-94): closed-shell DF-HF with the system's
+    ``ao`` and ``jkfit`` bases; returns {"HF": E, "E": E}."""
+    from .scf import dfhf as _dfhf
+    mol, basis = EC.system
+    o = EC.options["scf"]
+    EC.hf = _dfhf(EC.context(), mol, basis["ao"], basis.get("jkfit", "cc-pvtz-jkfit"),
+                  thr=o.thr, thren=o.thren, maxit=o.maxit, thred=EC.options["cholesky"].thred)
+    if not EC.hf.converged:
+        print("WARNING: DF-HF did not converge!")
+    return {"HF": EC.hf.E, "E": EC.hf.E}
+
+
+def dfints(EC):
+    """``@dfints`` / ``dfdump`` (src/integrals/dfdump.jl:263-301): the active
+    orbitals' DF integrals (``mpfit``) with the ``jkfit``-corrected one-electron
+    part, stored in ``EC.fd`` (DF factors) for ccdriver."""
+    from .scf import dfints as _dfints
+    if EC.hf is None:
+        raise ValueError("run dfhf first")
+    mol, basis = EC.system
+    core = EC.options["wf"].core
+    nc = mol.ncore() if core == "large" else 0 if core == "none" else None
+    if nc is None:
+        raise ValueError("wf.core must be 'large' or 'none'")
+    B, h1, e0, no, eref = _dfints(EC.hf, basis.get("mpfit", "cc-pvdz-mpfit"),
+                                  basis.get("jkfit", "cc-pvtz-jkfit"), ncore=nc,
+                                  thred=EC.options["cholesky"].thred)
+    EC._ncore = nc
+    EC.fd = FDump(h1, e0, 2 * no, B=B)
+    return eref
 
 
 def cc(EC, method, fcidump=""):

@@ -6,8 +6,10 @@
   commutator ``S D F - F D S`` as residual (plain dot, src/solvers/diis.jl),
   convergence on its squared norm (``scf.thr`` 1e-10) and on the energy change
   (``scf.thren``, default sqrt(thr)/10), the generalized eigenproblem
-  ``F C = S C eps`` each iteration.  Start orbitals: the core Hamiltonian
-  (the reference's ``guess = :HCORE`` option).
+  ``F C = S C eps`` each iteration.  Start orbitals: a superposition of
+  atomic densities (the reference's default ``guess = :SAD``; here the atoms'
+  spherically averaged DF-HF densities in the molecule's own basis), or the
+  core Hamiltonian (``guess = :HCORE``).
 * :func:`dfints` restates the closed-shell ``generate_integrals`` of
   ``dfdump`` (src/integrals/dfdump.jl:29-119): the frozen core
   (``core = :large``, first-row 1s), the three-index factors of the active
@@ -145,9 +147,63 @@ class DFHFResult:
         self.F, self.ints, self.AAL = F, ints, AAL
 
 
+# Spherically averaged ground-state occupations of the atoms' lowest orbitals
+# (1s; 2s; 2p x 3) for the atomic-density guess.
+_ATOM_OCC = {"H": [1.0], "C": [2.0, 2.0] + [2.0 / 3.0] * 3, "N": [2.0, 2.0, 1.0, 1.0, 1.0],
+             "O": [2.0, 2.0] + [4.0 / 3.0] * 3}
+
+
+def _atomic_density(ctx, sym, ao, jkfit, thred, library, maxit=100):
+    """Spin-restricted, spherically averaged DF-HF density of an isolated atom
+    in its basis (fractional occupations of the 2p shell)."""
+    from .molecules import Molecule
+    atom = Molecule([sym], [[0.0, 0.0, 0.0]])
+    ints = AOIntegrals(ctx, atom, ao, library)
+    AAL = ints.fitted(jkfit, thred)
+    occ = np.array(_ATOM_OCC[sym])
+    eps, C = _geneig(ints.h, ints.S)
+    diis = _Diis()
+    D = None
+    for _ in range(maxit):
+        X = C[:, :len(occ)] * np.sqrt(occ / 2.0)
+        Dn = 2.0 * X @ X.T
+        if D is not None and np.abs(Dn - D).max() < 1e-10:
+            break
+        D = Dn
+        F = df_fock(ints.h, AAL, X)
+        SDF = ints.S @ D @ F
+        F = diis.perform(F, SDF - SDF.T)
+        eps, C = _geneig(F, ints.S)
+    return D
+
+
+def sad_guess(ctx, mol, ao, jkfit, thred=1e-6, library=None):
+    """Superposition of atomic densities (the reference's default start,
+    ``scf.guess = :SAD``, src/scf/orbtools.jl), each atom's density computed
+    in the molecule's basis; returns the block-diagonal AO density."""
+    shells = Bm.shells(Bm.load(ao, library), mol.symbols, mol.xyz)
+    fa = shells.function_atoms()
+    D = np.zeros((shells.nbf, shells.nbf))
+    cache = {}
+    for a, sym in enumerate(mol.symbols):
+        if sym not in cache:
+            cache[sym] = _atomic_density(ctx, sym, ao, jkfit, thred, library)
+        idx = np.where(fa == a)[0]
+        D[np.ix_(idx, idx)] = cache[sym]
+    return D
+
+
+def _density_factor(D):
+    """X with D = 2 X X^T for a positive semidefinite density D."""
+    w, V = np.linalg.eigh(0.5 * (D + D.T))
+    keep = w > 1e-12
+    return V[:, keep] * np.sqrt(w[keep] / 2.0)
+
+
 def dfhf(ctx, mol, ao="cc-pvdz", jkfit="cc-pvtz-jkfit", thr=1e-10, thren=-1.0, maxit=50,
-         thred=1e-6, library=None, log=None):
-    """Closed-shell DF-HF (src/scf/dfhf.jl:24-94)."""
+         thred=1e-6, library=None, log=None, guess="sad"):
+    """Closed-shell DF-HF (src/scf/dfhf.jl:24-94); guess "sad" (atomic
+    densities) or "hcore" (core Hamiltonian)."""
     if mol.nelec % 2:
         raise ValueError("closed-shell DF-HF needs an even number of electrons")
     ints = AOIntegrals(ctx, mol, ao, library)
@@ -156,7 +212,13 @@ def dfhf(ctx, mol, ao="cc-pvdz", jkfit="cc-pvtz-jkfit", thr=1e-10, thren=-1.0, m
     nocc = mol.nelec // 2
     if thren < 0.0:
         thren = math.sqrt(thr) * 0.1
-    eps, C = _geneig(h, S)
+    if guess == "sad":
+        X = _density_factor(sad_guess(ctx, mol, ao, jkfit, thred, library))
+        eps, C = _geneig(df_fock(h, AAL, X), S)
+    elif guess == "hcore":
+        eps, C = _geneig(h, S)
+    else:
+        raise ValueError("guess must be 'sad' or 'hcore'")
     diis = _Diis()
     E = prev = 0.0
     conv = False
