@@ -4,12 +4,14 @@
                     [--workload h2o6_vtz] [--method ccsd|dcsd]
 
 A step is one FP64 CCSD iteration (T1-dressing, residual, Hylleraas energy,
-amplitude update, DIIS, energy) of the (H2O)_6/cc-pVTZ-sized closed-shell
-problem (o=24, v=318, nQ=846; the largest single-GPU configuration) built
-from seeded synthetic density-fitting factors (no integral engine: see the
-workload generator).  Inputs stay in HBM (T2 466 MB, B 792 MB: larger than
-the 126 MB L2, which is also flushed between steps); steps are timed with CUDA
-events on the library's stream.  The line also carries:
+amplitude update, DIIS, energy) of (H2O)_6/cc-pVTZ (o=24, v=318, nQ=846; the
+largest single-GPU configuration): the water hexamer from the seeded cluster
+generator, DF-HF (cc-pVTZ-JKFIT) and the frozen-core cc-pVTZ-RI integrals from
+the library's GPU integral engine, prepared before any timing
+(``--synthetic`` uses seeded synthetic factors of the same shape instead).
+Inputs stay in HBM (T2 466 MB, B 792 MB: larger than the 126 MB L2, which is
+also flushed between steps); steps are timed with CUDA events on the
+library's stream.  The line also carries:
 
 * ``e2e``: the same iterations through the C ABI with pinned host amplitudes
   (host-to-device and device-to-host copies inside the timed region);
@@ -60,6 +62,9 @@ def parse_args():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="h2o6_vtz")
+    p.add_argument("--synthetic", action="store_true",
+                   help="seeded synthetic DF factors of the workload's shape instead of the "
+                        "molecule's integrals")
     p.add_argument("--method", default="ccsd", choices=["ccsd", "dcsd"])
     p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     p.add_argument("--cpu-sample", type=int, default=1,
@@ -130,26 +135,47 @@ class Clocks:
 # ---------------------------------------------------------------- CPU side
 
 
-def _df_state(workload, dc, nsteps=20):
-    """The DF CPU restatement (oracle/dfcc.py) of the workload, started from
-    MP2 amplitudes; the ladder is cut into about 2*nsteps a-blocks."""
-    from oracle.dfcc import DFCC
+def load_workload(name, synthetic, ctx=None):
+    """(B, h1, e0, no, description) of the workload: the molecule's integrals
+    from the GPU integral engine (DF-HF + dfdump), or synthetic factors."""
     from ecgpu.synthetic import make_workload
-    B, h1, e0, no = make_workload(workload)
+    if synthetic:
+        B, h1, e0, no = make_workload(name)
+        return B, h1, e0, no, "seeded synthetic DF factors, canonical HF reference"
+    import ecgpu
+    from ecgpu.molecular import molecular_workload
+    own = ctx is None
+    c = ecgpu.Context(0) if own else ctx
+    try:
+        B, h1, e0, no, info = molecular_workload(c, name)
+    finally:
+        if own:
+            c.close()
+    desc = (f"{info['molecule']} from the seeded geometry generator: DF-HF {info['ao']}/"
+            f"{info['jkfit']} (E_HF {info['E_HF']:.8f}, {info['scf_iterations']} iterations), "
+            f"frozen-core {info['mpfit']} integrals, on the library's GPU integral engine")
+    return B, h1, e0, no, desc
+
+
+def _df_state(wl, dc, nsteps=20):
+    """The DF CPU restatement (oracle/dfcc.py) of the workload (B, h1, e0, no),
+    started from MP2 amplitudes; the ladder is cut into about 2*nsteps a-blocks."""
+    from oracle.dfcc import DFCC
+    B, h1, e0, no = wl[:4]
     nv = B.shape[0] - no
     d = DFCC(B, h1, e0, no, dc=dc, ablock=max(1, nv // (2 * max(nsteps, 1))))
     d.start()
     return d
 
 
-def cpu_baseline_sample(workload, dc, nblocks=1, ntrip=4):
+def cpu_baseline_sample(wl, dc, nblocks=1, ntrip=4):
     """CPU iterations/s of the DF restatement: every task of one CCSD iteration
     except the ladder runs once, the ladder on `nblocks` of its a-blocks; the
     iteration time is the non-ladder time plus the ladder blocks' mean time
     times their number (the blocks are alike).  Also (T) TFLOP/s on `ntrip`
     triplets."""
     import oracle as O
-    d = _df_state(workload, dc)
+    d = _df_state(wl, dc)
     t_other, t_lad, nlad, nrun = 0.0, 0.0, 0, 0
     for name, _, fn in d.iteration_tasks():
         if name.startswith("ladder"):
@@ -212,7 +238,8 @@ def run_reference(a, wl):
     1 / (time of the K steps) iterations per second; the W warm-up steps run
     the first W parts of a preceding iteration."""
     no, nv, nq = wl
-    d = _df_state(a.workload, a.method == "dcsd", a.steps)
+    W = load_workload(a.workload, a.synthetic)
+    d = _df_state(W, a.method == "dcsd", a.steps)
     tasks = d.iteration_tasks()
     K = max(1, a.steps)
     parts = _chunks(tasks, K)
@@ -237,8 +264,9 @@ def run_reference(a, wl):
         "impl": "reference", "metric": "CCSD iter/s", "value": rate, "unit": "iter/s",
         "n_gpus": a.gpus, "steps": K, "warmup": a.warmup, "ms_per_step": sum(ms) / K,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": {"workload": f"{a.workload} {a.method.upper()} (o={no}, "
-                                                    f"v={nv}, nQ={nq}), synthetic DF factors"},
+        "data": "synthetic" if a.synthetic else "real molecule (seeded geometry)",
+        "config": {"workload": f"{a.workload} {a.method.upper()} (o={no}, v={nv}, nQ={nq}): "
+                               f"{W[4]}"},
         "cpu_baseline": {"value": rate, "unit": "iter/s", "cores": cores, "kind": "port",
                          "sample": sample},
         "e2e": {"value": rate, "unit": "iter/s", "h2d_bytes_per_step": 0,
@@ -480,11 +508,11 @@ def main():
     from ecgpu._lib import ECG_KT_DGEMM, ECG_KT_TCGEMM, ECG_KT_TRIPLES
     dc = a.method == "dcsd"
     no, nv, nq = wl
-    B, h1, e0, no = make_workload(a.workload)
+    ctx = ecgpu.Context(local)
+    W = load_workload(a.workload, a.synthetic, ctx)
+    B, h1, e0, no, wdesc = W
     peaks = measured_peaks()
     fp64_peak = cublas_dgemm_peak(torch)
-
-    ctx = ecgpu.Context(local)
     ctx.set_system(B, h1, e0, no)
     _, T1, T2 = ctx.mp2()
     stream = torch.cuda.ExternalStream(ctx.stream())
@@ -660,9 +688,9 @@ def main():
         "metric": "CCSD iter/s", "value": value, "unit": "iter/s", "n_gpus": world,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": total / a.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic",
-        "config": {"workload": f"{a.workload} {a.method.upper()} (o={no}, v={nv}, nQ={nq}), "
-                               "seeded synthetic DF factors, canonical HF reference",
+        "data": "synthetic" if a.synthetic else "real molecule (seeded geometry)",
+        "config": {"workload": f"{a.workload} {a.method.upper()} (o={no}, v={nv}, nQ={nq}): "
+                               f"{wdesc}",
                    "precision": "fp64",
                    "l2": "inputs larger than L2 (T2 466 MB, B 792 MB) and L2 flushed "
                          "(256 MiB write) between steps",
@@ -685,7 +713,7 @@ def main():
                   "order": f"fp64, {COOLDOWN_S:.0f} s idle, mixed"},
     }
     if rank == 0 and world == 1 and a.cpu_sample > 0:
-        cb = cpu_baseline_sample(a.workload, dc, nblocks=a.cpu_sample)
+        cb = cpu_baseline_sample(W, dc, nblocks=a.cpu_sample)
         line["cpu_baseline"] = {
             "value": 1.0 / cb["iter_s"], "unit": "iter/s", "cores": host_cores(),
             "kind": "port",
