@@ -88,16 +88,19 @@ def test_water_cc_pvdz_shapes(ictx):
 
 def test_df_hf_chain_reproduces_reference_pins(gold):
     """@dfhf with cc-pVDZ / cc-pVTZ-JKFIT on the test/df_hf.jl water, then
-    @dfints (frozen O 1s, cc-pVDZ-MPFIT) and ccdriver, all at the reference's
-    default thresholds: HF, MP2 and DCSD against test/df_hf.jl:5-7.  MP2 and
-    DCSD agree to 1e-8 (measured 4e-9, 2e-9); HF is 1.5e-8 above its pin for
-    every SCF threshold and fitting rank tried (a difference in the integrals
-    or basis data behind the pin, not located), held at 2e-8."""
+    @dfints (frozen O 1s, cc-pVDZ-MPFIT) and ccdriver at the reference's CC
+    thresholds: HF, MP2 and DCSD against test/df_hf.jl:5-7.  The SCF is
+    converged tightly (commutator norm^2 < 1e-14): at the reference's 1e-10 the
+    last orbitals depend on the start guess and move MP2 by up to 2e-8.  MP2
+    and DCSD agree to 1e-8 (measured 3e-9, 2e-9); HF is 1.5e-8 above its pin
+    for every SCF threshold and fitting rank tried (a difference in the
+    integrals or basis data behind the pin, not located), held at 2e-8."""
     from ecgpu.driver import ECInfo, ccdriver, dfhf as run_dfhf, dfints as run_dfints
     from ecgpu.molecules import water
     pins = gold["df_hf"]
     EC = ECInfo()
     EC.set_system(water(), {"ao": "cc-pVDZ", "jkfit": "cc-pvtz-jkfit", "mpfit": "cc-pvdz-mpfit"})
+    EC.set("scf", thr=1e-14)
     e = run_dfhf(EC)
     assert abs(e["HF"] - pins["HF"]) < 2e-8, e["HF"] - pins["HF"]
     run_dfints(EC)
