@@ -1526,34 +1526,30 @@ __global__ void __launch_bounds__(512, 1) triples_energy_kernel(
     const int* sS = reinterpret_cast<const int*>(base + L::S_OFF);
     const int S0 = sS[0], S1 = sS[1], S2 = sS[2];
     if (S0 + l[0] < v && S1 + l[1] < v && S2 + l[2] < v) {
-      // per-element arithmetic in K's precision (FP32 for the mixed path, FP64
-      // for the FP64 path); the sums over elements and orbits are FP64
-      using CT = T;
-      CT k[6];
+      double k[6];
 #pragma unroll
-      for (int q = 0; q < 6; ++q) k[q] = cK[koff[q]];
-      const double den = eijk - pe[l[0]] - pe[8 + l[1]] - pe[16 + l[2]];
-      const CT dinv = sizeof(CT) == 4 ? (CT)__frcp_rn((float)den) : (CT)__drcp_rn(den);
-      CT se = 0, so = 0;
+      for (int q = 0; q < 6; ++q) k[q] = (double)cK[koff[q]];
+      const double dinv = __drcp_rn(eijk - pe[l[0]] - pe[8 + l[1]] - pe[16 + l[2]]);
+      double se = 0.0, so = 0.0;
 #pragma unroll
       for (int q = 0; q < 6; ++q) {
         if (perm3_parity(q)) so += k[q];
         else se += k[q];
       }
-      const CT ce = se - (CT)2 * so, co = so - (CT)2 * se;
-      CT X[6];
+      const double ce = se - 2.0 * so, co = so - 2.0 * se;
+      double X[6];
 #pragma unroll
-      for (int q = 0; q < 6; ++q) X[q] = ((CT)3 * k[q] + (perm3_parity(q) ? co : ce)) * dinv;
+      for (int q = 0; q < 6; ++q) X[q] = (3.0 * k[q] + (perm3_parity(q) ? co : ce)) * dinv;
       // Y of ordering q = (p0,p1,p2): g0[p0] M0[p1,p2] + g1[p1] M1[p0,p2]
       // + g2[p2] M2[p0,p1] + (f, N likewise).  Each ordered pair (x, y) with
       // third position z serves three orderings: (z,x,y) through M0/N0,
       // (x,z,y) through M1/N1 and (x,y,z) through M2/N2.
-      CT vg[3][6];  // vectors at the three positions: vg[pos][w]
+      double vg[3][6];  // vectors at the three positions: vg[pos][w]
 #pragma unroll
       for (int pos = 0; pos < 3; ++pos)
 #pragma unroll
-        for (int w = 0; w < 6; ++w) vg[pos][w] = pv[(w * 3 + pos) * 8 + l[pos]];
-      CT yq[6] = {0, 0, 0, 0, 0, 0};
+        for (int w = 0; w < 6; ++w) vg[pos][w] = (double)pv[(w * 3 + pos) * 8 + l[pos]];
+      double yq[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
 #pragma unroll
       for (int x = 0; x < 3; ++x)
 #pragma unroll
@@ -1562,20 +1558,20 @@ __global__ void __launch_bounds__(512, 1) triples_energy_kernel(
           const int z = 3 - x - yy;
           const int lo = x < yy ? l[x] : l[yy], hi = x < yy ? l[yy] : l[x];
           const T* mb = pm + pair_index(x, yy) * 6 * 64 + lo + 8 * hi;
-          yq[perm3_index(z, x)] += vg[z][0] * mb[0] + vg[z][3] * mb[3 * 64];
-          yq[perm3_index(x, z)] += vg[z][1] * mb[64] + vg[z][4] * mb[4 * 64];
-          yq[perm3_index(x, yy)] += vg[z][2] * mb[2 * 64] + vg[z][5] * mb[5 * 64];
+          yq[perm3_index(z, x)] += vg[z][0] * (double)mb[0] + vg[z][3] * (double)mb[3 * 64];
+          yq[perm3_index(x, z)] += vg[z][1] * (double)mb[64] + vg[z][4] * (double)mb[4 * 64];
+          yq[perm3_index(x, yy)] += vg[z][2] * (double)mb[2 * 64] + vg[z][5] * (double)mb[5 * 64];
         }
-      CT ek = 0, ey = 0;
+      double ek = 0.0, ey = 0.0;
 #pragma unroll
       for (int q = 0; q < 6; ++q) {
-        ek += (HAS_U ? cU[koff[q]] : k[q]) * X[q];
+        ek += (HAS_U ? (double)cU[koff[q]] : k[q]) * X[q];
         ey += X[q] * yq[q];
       }
       const bool ab = (S0 == S1), bc = (S1 == S2);
       const double wgt = (ab && bc) ? (1.0 / 6.0) : (ab || bc) ? 0.5 : 1.0;
-      eK += wgt * (double)ek;
-      eY += wgt * (double)ey;
+      eK += wgt * ek;
+      eY += wgt * ey;
     }
   }
   cp_async_wait<0>();
