@@ -53,3 +53,21 @@ def ctx():
     c = ecgpu.Context(0)
     yield c
     c.close()
+
+
+@pytest.fixture(scope="session")
+def h2o_fcidump_text(tmp_path_factory):
+    """The reference's test/files/H2O.FCIDUMP reassembled as text: its own
+    header (tests/golden/h2o_fcidump_header.txt) and the integral lines of the
+    committed fixture in the file's "value i j k l" form (Fortran E format)."""
+    z = np.load(os.path.join(GOLDEN, "h2o_fcidump.npz"))
+    with open(os.path.join(GOLDEN, "h2o_fcidump_header.txt")) as f:
+        head = f.read()
+    lines = [head.rstrip("\n")]
+    for (i, j, k, l), x in zip(z["idx"].astype(int), z["val"]):
+        m, e = f"{x:.15E}".split("E")
+        lines.append(f" {float(m) / 10:.16f}E{int(e) + 1:+03d} {i:3d} {j:3d} {k:3d} {l:3d}")
+    lines.append(f" {float(z['e0']):.16E}   0   0   0   0")
+    p = tmp_path_factory.mktemp("fcidump") / "H2O.FCIDUMP"
+    p.write_text("\n".join(lines) + "\n")
+    return str(p)

@@ -68,6 +68,16 @@ def main(refroot):
         "h2o_fcidump.npz": "test/files/H2O.FCIDUMP",
         "h2o_st1_fcidump.npz": "test/files/H2O_ST1.FCIDUMP",
     }
+    # the header of H2O.FCIDUMP as it stands (multi-line ORBSYM/OCC/CLOSED/FOCK
+    # values): the FCIDUMP reader is tested on it with the fixture's integrals
+    with open(os.path.join(refroot, files["h2o_fcidump.npz"])) as f:
+        hdr = []
+        for line in f:
+            hdr.append(line)
+            if line.strip() in ("/", "&END"):
+                break
+    with open(os.path.join(HERE, "h2o_fcidump_header.txt"), "w") as f:
+        f.writelines(hdr)
     for out, rel in files.items():
         head, idx, val, e0 = parse_fcidump_text(os.path.join(refroot, rel))
         np.savez_compressed(

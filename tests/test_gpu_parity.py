@@ -419,3 +419,15 @@ def test_mixed_ccsd_t_vtz_shape():
     assert out[ecgpu.ECG_PREC_FP64][1] < -1e-5
     assert abs(emx[0] - e64[0]) < 1e-6, (emx[0], e64[0])
     assert abs(emx[1] - e64[1]) < 1e-6, (emx[1], e64[1])
+
+
+def test_driver_from_fcidump_text(h2o_fcidump_text, gold, tmp_path):
+    """ccdriver(EC, "ccsd(t)"; fcidump) as test/h2o.jl calls it, on the
+    reference's H2O.FCIDUMP text (pre-0.13 DIIS dot, see test_oracle_golden)."""
+    from ecgpu.driver import ECInfo, ccdriver
+    g = gold["h2o"]
+    EC = ECInfo(scr=str(tmp_path))
+    EC.set("diis", dot="plain")
+    e = ccdriver(EC, "ccsd(t)", fcidump=h2o_fcidump_text)
+    assert abs(e["HF"] - g["HF"]) < 1e-9 and abs(e["MP2c"] - g["MP2c"]) < 1e-9
+    assert abs(e["CCSD(T)c"] - g["CCSD(T)c"]) < 1e-9

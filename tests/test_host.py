@@ -96,3 +96,13 @@ def test_oracle_synthetic_ccsd_converges():
     r = O.ccdriver(S, "ccsd(t)")
     assert r["converged"] and r["iterations"] < 20
     assert -1.0 < r["CCSDc"] < 0.0 and r["(T)"] < 0.0
+
+
+def test_read_reference_fcidump_text(h2o_fcidump_text, h2o):
+    """read_fcidump on the reference's H2O.FCIDUMP header (multi-line ORBSYM,
+    OCC, CLOSED and FOCK values) and its integral lines."""
+    fd = D.read_fcidump(h2o_fcidump_text)
+    assert fd.norb == 23 and fd.nelec == 8 and not fd.st
+    assert len(fd.head["FOCK"]) == 23 and fd.head["OCC"][0] == "4"
+    assert np.abs(fd.V - h2o.V).max() < 1e-15 and np.abs(fd.h - h2o.h).max() < 1e-15
+    assert fd.e0 == h2o.e0
