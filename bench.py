@@ -77,6 +77,8 @@ def parse_args():
     p.add_argument("--sweep", action="store_true",
                    help="DCSD time per iteration and device memory, FP64 vs mixed, over the "
                         "C6..C10 alkane sizes (one line)")
+    p.add_argument("--tune", default="",
+                   help="tune every GEMM shape during the warm-up and write the table here")
     p.add_argument("--occ", type=int, default=0,
                    help="--tts only: override the occupied count (smaller profiling cases)")
     return p.parse_args()
@@ -430,6 +432,10 @@ def run_sweep(a):
     print(json.dumps(line), flush=True)
 
 
+# GEMM tuning table for B200 written by `bench.py --tune` (ecg_tune_save)
+TUNE_TABLE = os.path.join(ROOT, "elemco.jl_b200", "ecgpu", "tuning", "b200.txt")
+
+
 def measured_peaks():
     """HBM GB/s, burst and sustained dense BF16 TFLOP/s: MEASURED_PEAKS.json
     (written per pod by the benchmark driver), else the pool's earlier
@@ -513,6 +519,8 @@ def main():
     B, h1, e0, no, wdesc = W
     peaks = measured_peaks()
     fp64_peak = cublas_dgemm_peak(torch)
+    from ecgpu._lib import ECG_OPT_AUTOTUNE
+    tune_entries = ctx.tune_load(TUNE_TABLE) if os.path.exists(TUNE_TABLE) else 0
     ctx.set_system(B, h1, e0, no)
     _, T1, T2 = ctx.mp2()
     stream = torch.cuda.ExternalStream(ctx.stream())
@@ -537,6 +545,18 @@ def main():
 
     # ---- timed FP64 CCSD iterations (the value) ----
     RESTART = 8  # re-seed from MP2 amplitudes every 8 steps (outside timing)
+    if a.tune:
+        # tune every GEMM shape of an FP64 and a mixed iteration and of the
+        # (T) sweep's first batch (outside any timing), then keep the table
+        ctx.set_option(ECG_OPT_AUTOTUNE, 1)
+        for prec in (ecgpu.ECG_PREC_FP64, ecgpu.ECG_PREC_MIXED):
+            ctx.set_precision(prec)
+            restart()
+            ctx.cc_step(dc=dc)
+            ctx.pert_t()
+        ctx.set_option(ECG_OPT_AUTOTUNE, 0)
+        ctx.set_precision(ecgpu.ECG_PREC_FP64)
+        tune_entries = ctx.tune_save(a.tune)
     restart()
     for _ in range(a.warmup):
         ctx.cc_step(dc=dc)
@@ -694,7 +714,10 @@ def main():
                    "precision": "fp64",
                    "l2": "inputs larger than L2 (T2 466 MB, B 792 MB) and L2 flushed "
                          "(256 MiB write) between steps",
-                   "parallelism": f"replicas x{world}"},
+                   "parallelism": f"replicas x{world}",
+                   "gemm_tuning": f"{tune_entries} tuned GEMM shapes "
+                                  f"({os.path.relpath(TUNE_TABLE, ROOT)})" if tune_entries
+                                  else "fixed tile rules"},
         "e2e": {"value": world * a.steps / (total_e2e / 1000.0), "unit": "iter/s",
                 "h2d_bytes_per_step": 8 * (n1 + n2), "d2h_bytes_per_step": 8 * (n1 + n2)},
         "gpu_launches": launches,

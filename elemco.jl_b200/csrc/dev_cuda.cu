@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "ecg_dev.h"
+#include "ecg_tune.h"
 
 namespace ecg {
 namespace dev {
@@ -708,7 +709,114 @@ void kernel_time(int family, double* ms, int64_t* n, double* work) {
 
 void gemm_time(double* ms, int64_t* n, double* flops) { kernel_time(KT_DGEMM, ms, n, flops); }
 
+// ---- autotuner table (ecg_tune.h) ----------------------------------------
+namespace {
+std::mutex g_tune_mu;
+std::map<std::string, int> g_tune;
+std::atomic<bool> g_tuning{false};
+}  // namespace
+
+void set_tuning(bool on) { g_tuning.store(on); }
+bool tuning() { return g_tuning.load(); }
+bool stream_capturing(stream_t s) { return capturing((cudaStream_t)s); }
+
+bool tune_get(const std::string& key, int* value) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune.find(key);
+  if (it == g_tune.end()) return false;
+  *value = it->second;
+  return true;
+}
+
+void tune_put(const std::string& key, int value) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[key] = value;
+}
+
+size_t tune_size() {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  return g_tune.size();
+}
+
+std::string tune_dump() {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  std::string out;
+  for (auto& kv : g_tune) out += kv.first + " " + std::to_string(kv.second) + "\n";
+  return out;
+}
+
+int tune_parse(const std::string& text) {
+  std::map<std::string, int> add;
+  size_t pos = 0;
+  while (pos < text.size()) {
+    size_t end = text.find('\n', pos);
+    if (end == std::string::npos) end = text.size();
+    const std::string line = text.substr(pos, end - pos);
+    pos = end + 1;
+    if (line.empty() || line[0] == '#') continue;
+    const size_t sp = line.rfind(' ');
+    if (sp == std::string::npos || sp == 0) return -1;
+    char* e = nullptr;
+    const long v = std::strtol(line.c_str() + sp + 1, &e, 10);
+    if (!e || *e != '\0') return -1;
+    add[line.substr(0, sp)] = (int)v;
+  }
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  for (auto& kv : add) g_tune[kv.first] = kv.second;
+  return (int)add.size();
+}
+
+int tune_pick(stream_t s, int ncand, const std::function<int(int)>& run, const TuneOut& out) {
+  cudaStream_t st = (cudaStream_t)s;
+  void* save = nullptr;
+  const size_t bytes = (size_t)out.rows_bytes * (size_t)out.ncols;
+  if (cudaMalloc(&save, bytes ? bytes : 16) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  auto copy = [&](bool restore) {
+    if (restore)
+      return cudaMemcpy2DAsync(out.C, out.ldc_bytes, save, out.rows_bytes, out.rows_bytes,
+                               out.ncols, cudaMemcpyDeviceToDevice, st);
+    return cudaMemcpy2DAsync(save, out.rows_bytes, out.C, out.ldc_bytes, out.rows_bytes,
+                             out.ncols, cudaMemcpyDeviceToDevice, st);
+  };
+  int best = -1;
+  float best_ms = 0.f;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  if (copy(false) == cudaSuccess) {
+    for (int i = 0; i < ncand; ++i) {
+      float ms = 0.f;
+      bool ok = run(i) == 0;  // warm-up run (first use of the configuration)
+      ok = ok && copy(true) == cudaSuccess;
+      ok = ok && cudaEventRecord(a, st) == cudaSuccess;
+      ok = ok && run(i) == 0;
+      ok = ok && cudaEventRecord(b, st) == cudaSuccess;
+      ok = ok && cudaEventSynchronize(b) == cudaSuccess;
+      ok = ok && cudaEventElapsedTime(&ms, a, b) == cudaSuccess;
+      copy(true);
+      if (!ok) {
+        cudaGetLastError();
+        continue;
+      }
+      if (best < 0 || ms < best_ms) {
+        best = i;
+        best_ms = ms;
+      }
+    }
+  }
+  cudaStreamSynchronize(st);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(save);
+  return best;
+}
+
 static int gemm_launch(stream_t s, const Gemm& q);
+struct PlainChoice;
+static int plain_gemm(stream_t s, const GemmArgs& g, const Gemm& q);
 
 int gemm_strided(stream_t s, const Gemm& q) {
   if (!g_timing || q.m <= 0 || q.n <= 0 || q.batch <= 0 || q.k <= 0) return gemm_launch(s, q);
@@ -741,15 +849,23 @@ static int gemm_launch(stream_t s, const Gemm& q) {
   }
   cudaStream_t st = (cudaStream_t)s;
   if (q.k <= 0 || q.alpha == 0.0) {
+    // empty contraction: C = beta C
     if (q.beta == 1.0) return 0;
-    for (int64_t b = 0; b < q.batch; ++b)
-      for (int64_t j = 0; j < q.n; ++j)
-        for (int64_t i = 0; i < q.m; ++i) {
-          // rare path (empty contraction): scale C element-wise
-          double* p = q.C + b * q.scb + j * q.scn + i * q.scm;
-          int e = axpby(s, 1, 0.0, p, q.beta, p);
-          if (e) return e;
-        }
+    for (int64_t b = 0; b < q.batch; ++b) {
+      double* Cb = q.C + b * q.scb;
+      int e = 0;
+      if (q.scm == 1)
+        e = geam(s, q.m, q.n, 0.0, Cb, q.scn, q.beta, Cb, q.scn);
+      else if (q.scn == 1)
+        e = geam(s, q.n, q.m, 0.0, Cb, q.scm, q.beta, Cb, q.scm);
+      else
+        for (int64_t j = 0; j < q.n && !e; ++j)
+          for (int64_t i = 0; i < q.m && !e; ++i) {
+            double* p = Cb + j * q.scn + i * q.scm;
+            e = axpby(s, 1, 0.0, p, q.beta, p);
+          }
+      if (e) return e;
+    }
     return 0;
   }
   GemmArgs g{q.A, q.B, q.C, q.m, q.n, q.k, q.sam, q.sak, q.sab, q.sbk, q.sbn, q.sbb,
@@ -782,15 +898,35 @@ static int gemm_launch(stream_t s, const Gemm& q) {
         return launch_gemm<64, 64, 16, 32, 32, 3, 3, 0, GF_PTAB | GF_SEG | GF_DN>(g, nb, st);
     }
   }
-  // Split-K for GEMMs whose output covers too few tiles to fill the SMs:
-  // each z-slice writes a partial product, a fixed-order reduction sums them.
+  return plain_gemm(s, g, q);
+}
+
+// Plain GEMM configurations: tile shape (cfg 0: 64x64, warps 32x32, 3 CTAs
+// per SM; 1: 128x64, warps 64x32, 2 CTAs; 2: 64x128, warps 32x64, 2 CTAs) and
+// split-K count S (> 1: cfg 0 on K slices whose partial products a
+// fixed-order reduction sums).
+struct PlainChoice {
+  int cfg, S;
+};
+
+// The fixed rule: split K when the output covers too few 64x64 tiles to fill
+// the SMs (and K is long enough), otherwise 64x64 tiles (the best or within 2%
+// of the best configuration on every CCSD/(T) shape measured on B200).
+static PlainChoice default_plain(const Gemm& q) {
   const int64_t tiles64 = ((q.m + 63) / 64) * ((q.n + 63) / 64);
   if (q.batch == 1 && tiles64 < 148 && q.k >= 512) {
     int64_t S = std::min<int64_t>((2 * 148 + tiles64 - 1) / tiles64, q.k / 256);
-    S = std::max<int64_t>(2, std::min<int64_t>(S, 64));
-    int64_t kc = (q.k + S - 1) / S;
+    return PlainChoice{0, (int)std::max<int64_t>(2, std::min<int64_t>(S, 64))};
+  }
+  return PlainChoice{0, 1};
+}
+
+static int launch_plain(stream_t s, const GemmArgs& g, const Gemm& q, PlainChoice c) {
+  cudaStream_t st = (cudaStream_t)s;
+  if (c.S > 1 && q.batch == 1) {
+    int64_t kc = (q.k + c.S - 1) / c.S;
     kc = (kc + 15) / 16 * 16;
-    S = (q.k + kc - 1) / kc;
+    const int64_t S = (q.k + kc - 1) / kc;
     double* P = splitk_buffer(s, (size_t)S * q.m * q.n);
     if (!P) return (int)cudaErrorMemoryAllocation;
     GemmArgs h = g;
@@ -811,10 +947,41 @@ static int gemm_launch(stream_t s, const Gemm& q) {
                                                           q.C, q.scm, q.scn);
     return launched();
   }
-  // 64x64 tiles, 4 warps of 32x32, mma.m8n8k4, 3 CTAs per SM: the best or
-  // within 2% of the best measured configuration (tile sizes, m16n8k{4,8,16})
-  // on every CCSD/(T) shape on B200 (elemco.jl_b200/gemm_configs_bench.cu).
-  return launch_gemm<64, 64, 16, 32, 32, 3, 3>(g, q.batch, st);
+  switch (c.cfg) {
+    case 1: return launch_gemm<128, 64, 16, 64, 32, 3, 2>(g, q.batch, st);
+    case 2: return launch_gemm<64, 128, 16, 32, 64, 3, 2>(g, q.batch, st);
+    default: return launch_gemm<64, 64, 16, 32, 32, 3, 3>(g, q.batch, st);
+  }
+}
+
+static int plain_gemm(stream_t s, const GemmArgs& g, const Gemm& q) {
+  PlainChoice c = default_plain(q);
+  const std::string key = "dgemm " + std::to_string(q.m) + " " + std::to_string(q.n) + " " +
+                          std::to_string(q.k) + " " + std::to_string(q.batch) + " " +
+                          std::to_string(g.a_kfast) + std::to_string(g.b_nfast);
+  int enc = 0;
+  if (tune_get(key, &enc)) {
+    c = PlainChoice{enc % 4, enc / 4};
+  } else if (tuning() && q.batch == 1 && q.scm == 1 && !capturing((cudaStream_t)s)) {
+    std::vector<PlainChoice> cand = {{0, 1}, {1, 1}, {2, 1}};
+    const PlainChoice d = default_plain(q);
+    if (q.k >= 512) {
+      for (int S : {d.S, 2 * d.S, d.S / 2, 4})
+        if (S >= 2 && S <= 64 && q.k / S >= 64) {
+          bool dup = false;
+          for (auto& x : cand) dup |= (x.S == S);
+          if (!dup) cand.push_back({0, S});
+        }
+    }
+    const TuneOut out{q.C, q.m * 8, q.n, q.scn * 8};
+    const int best = tune_pick(
+        s, (int)cand.size(), [&](int i) { return launch_plain(s, g, q, cand[i]); }, out);
+    if (best >= 0) {
+      c = cand[best];
+      tune_put(key, c.S * 4 + c.cfg);
+    }
+  }
+  return launch_plain(s, g, q, c);
 }
 
 int gemm(stream_t s, char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha,

@@ -26,8 +26,11 @@
 #include <cstdint>
 #include <cstring>
 #include <mutex>
+#include <string>
+#include <vector>
 
 #include "ecg_dev.h"
+#include "ecg_tune.h"
 
 namespace ecg {
 namespace dev {
@@ -869,27 +872,17 @@ int tc_view(const TcOperand& parent, int64_t row0, int64_t rows, TcOperand* out)
   return encode_operand(enc, out, rows);
 }
 
-int tc_gemm(stream_t s, const TcGemm& g) {
-  if (g.m <= 0 || g.n <= 0) return 0;
-  int64_t k[TC_MAX_SEG];
-  const int ns = gemm_segments(g, k);
-  if (ns == 0) return (int)cudaErrorInvalidValue;
+// Launch over pre-split operands with tile width tn and split count S.
+static int tc_gemm_run(cudaStream_t st, const TcGemm& g, int ns, const TcSegs& segs, int kbt,
+                       int tn, int S) {
   const int nsl = g.A[0]->slices;
-  int tn = tile_n(g.n, nsl);
-  for (int t = 0; t < ns; ++t)
-    if (!b_map(g.B[t], tn)) tn = 128;
   TcMaps maps;
   for (int t = 0; t < TC_MAX_SEG; ++t) {
     std::memcpy(&maps.a[t], g.A[t < ns ? t : 0]->map, sizeof(CUtensorMap));
     std::memcpy(&maps.b[t], b_map(g.B[t < ns ? t : 0], tn), sizeof(CUtensorMap));
   }
-  const TcSegs segs = make_segs(ns, k);
-  const int kbt = segs.kb_end[TC_MAX_SEG - 1];
   TcOut out{g.C, g.scm, g.scn, g.dn, g.scn2, g.dm, g.scm2, g.f32 ? 1 : 0};
   const int64_t mp = pad_rows(g.m), np = (g.n + tn - 1) / tn * tn;
-  int S = 1;
-  if (!g.f32 && g.dn == 0 && g.dm == 0) S = split_count(mp / TM * (np / tn), kbt);
-  cudaStream_t st = (cudaStream_t)s;
   if (nsl == 3)
     return tn == TN_WIDE
                ? launch_tc<3, TN_WIDE>(st, maps, segs, kbt, g.m, g.n, mp, np, g.alpha, g.beta,
@@ -903,6 +896,75 @@ int tc_gemm(stream_t s, const TcGemm& g) {
              ? launch_tc<2, TN_WIDE>(st, maps, segs, kbt, g.m, g.n, mp, np, g.alpha, g.beta, out,
                                      S)
              : launch_tc<2, 128>(st, maps, segs, kbt, g.m, g.n, mp, np, g.alpha, g.beta, out, S);
+}
+
+// Split counts a plain FP64 output allows: at least enough K slices that no
+// FP32 accumulation sums more than KB_ACC k-blocks.
+static int tc_min_split(int kbt) { return (kbt + KB_ACC - 1) / KB_ACC; }
+
+int tc_gemm(stream_t s, const TcGemm& g) {
+  if (g.m <= 0 || g.n <= 0) return 0;
+  int64_t k[TC_MAX_SEG];
+  const int ns = gemm_segments(g, k);
+  if (ns == 0) return (int)cudaErrorInvalidValue;
+  const int nsl = g.A[0]->slices;
+  const TcSegs segs = make_segs(ns, k);
+  const int kbt = segs.kb_end[TC_MAX_SEG - 1];
+  const bool plain = !g.f32 && g.dn == 0 && g.dm == 0;
+  // tile widths every B operand has a descriptor for
+  auto usable = [&](int tn) {
+    for (int t = 0; t < ns; ++t)
+      if (!b_map(g.B[t], tn)) return false;
+    return true;
+  };
+  auto split_for = [&](int tn) {
+    if (!plain) return 1;
+    const int64_t np = (g.n + tn - 1) / tn * tn;
+    return split_count(pad_rows(g.m) / TM * (np / tn), kbt);
+  };
+  // the fixed rule
+  int tn = tile_n(g.n, nsl);
+  if (!usable(tn)) tn = 128;
+  int S = split_for(tn);
+  cudaStream_t st = (cudaStream_t)s;
+  const std::string key = "tc " + std::to_string(g.m) + " " + std::to_string(g.n) + " " +
+                          std::to_string(kbt) + " " + std::to_string(nsl) + " " +
+                          std::to_string(plain ? 1 : g.f32 ? 2 : 0);
+  int enc = 0;
+  if (tune_get(key, &enc)) {
+    const int t = enc % 4, tw = t == 1 ? TN_WIDE : t == 2 ? TN_XWIDE : 128;
+    if (usable(tw)) {
+      tn = tw;
+      S = plain ? std::max(enc / 4, tc_min_split(kbt)) : 1;
+    }
+  } else if (tuning() && g.dn == 0 && g.dm == 0 && g.scm == 1 && !stream_capturing(s)) {
+    struct Cand {
+      int tn, S;
+    };
+    std::vector<Cand> cand;
+    for (int tw : {128, TN_WIDE, TN_XWIDE}) {
+      if ((tw == TN_XWIDE && nsl != 2) || !usable(tw) || (tw > 128 && g.n < tw)) continue;
+      const int d = split_for(tw);
+      for (int Sx : {d, d * 2, std::max(d / 2, 1), tc_min_split(kbt)}) {
+        if (!plain && Sx != 1) continue;
+        if (plain && (Sx < tc_min_split(kbt) || Sx > kbt)) continue;
+        bool dup = false;
+        for (auto& c : cand) dup |= (c.tn == tw && c.S == Sx);
+        if (!dup) cand.push_back({tw, Sx});
+      }
+    }
+    const int64_t esz = g.f32 ? 4 : 8;
+    const TuneOut out{g.C, g.m * esz, g.n, g.scn * esz};
+    const int best = tune_pick(
+        s, (int)cand.size(),
+        [&](int i) { return tc_gemm_run(st, g, ns, segs, kbt, cand[i].tn, cand[i].S); }, out);
+    if (best >= 0) {
+      tn = cand[best].tn;
+      S = cand[best].S;
+      tune_put(key, (tn == TN_WIDE ? 1 : tn == TN_XWIDE ? 2 : 0) + 4 * S);
+    }
+  }
+  return tc_gemm_run(st, g, ns, segs, kbt, tn, S);
 }
 
 size_t tc_maps_bytes() { return sizeof(TcMaps); }
@@ -996,24 +1058,64 @@ int gemm_strided_mixed(stream_t s, const Gemm& q) {
   cudaStream_t st = (cudaStream_t)s;
   launch_split(st, q.A, m, k, q.sam, q.sak, mp, kp, NSL, As);  // A(m,k) = A[m sam + k sak]
   launch_split(st, q.B, n, k, q.sbn, q.sbk, np, kp, NSL, Bs);  // B(k,n) = B[k sbk + n sbn]
-  // B rows are padded to 128; a wider tile (tile_n) reads 160-row boxes from
-  // them (n >= 160 then; rows past np read as zero)
-  const int tn = tile_n(n, NSL);
-  const int64_t npt = (n + tn - 1) / tn * tn;
-  TcMaps maps;
-  if ((e = make_map(enc, &maps.a[0], As, mp, kp, NSL))) return e;
-  if ((e = make_map(enc, &maps.b[0], Bs, np, kp, NSL, 0, tn))) return e;
-  for (int t = 1; t < TC_MAX_SEG; ++t) {
-    maps.a[t] = maps.a[0];
-    maps.b[t] = maps.b[0];
-  }
+  // B rows are padded to 128; a wider tile reads 160-row boxes from them
+  // (n >= 160 then; rows past np read as zero)
   const TcSegs segs = make_segs(1, &k);
   const int kbt = (int)(kp / TK);
-  const int S = split_count((mp / TM) * (npt / tn), kbt);
   TcOut out{q.C, q.scm, q.scn, 0, 0, 0, 0, 0};
-  if (tn == TN_WIDE)
-    return launch_tc<NSL, TN_WIDE>(st, maps, segs, kbt, m, n, mp, npt, q.alpha, q.beta, out, S);
-  return launch_tc<NSL, 128>(st, maps, segs, kbt, m, n, mp, npt, q.alpha, q.beta, out, S);
+  auto run = [&](int tn, int S) {
+    const int64_t npt = (n + tn - 1) / tn * tn;
+    TcMaps maps;
+    int r = make_map(enc, &maps.a[0], As, mp, kp, NSL);
+    if (!r) r = make_map(enc, &maps.b[0], Bs, np, kp, NSL, 0, tn);
+    if (r) return r;
+    for (int t = 1; t < TC_MAX_SEG; ++t) {
+      maps.a[t] = maps.a[0];
+      maps.b[t] = maps.b[0];
+    }
+    if (tn == TN_WIDE)
+      return launch_tc<NSL, TN_WIDE>(st, maps, segs, kbt, m, n, mp, npt, q.alpha, q.beta, out,
+                                     S);
+    return launch_tc<NSL, 128>(st, maps, segs, kbt, m, n, mp, npt, q.alpha, q.beta, out, S);
+  };
+  auto split_for = [&](int tn) {
+    const int64_t npt = (n + tn - 1) / tn * tn;
+    return split_count((mp / TM) * (npt / tn), kbt);
+  };
+  int tn = tile_n(n, NSL);
+  int S = split_for(tn);
+  const std::string key = "tcmix " + std::to_string(m) + " " + std::to_string(n) + " " +
+                          std::to_string(kbt);
+  int code = 0;
+  if (tune_get(key, &code)) {
+    const int tw = (code % 4) == 1 && n >= TN_WIDE ? TN_WIDE : 128;
+    tn = tw;
+    S = std::max(code / 4, tc_min_split(kbt));
+  } else if (tuning() && q.scm == 1 && !stream_capturing(s)) {
+    struct Cand {
+      int tn, S;
+    };
+    std::vector<Cand> cand;
+    for (int tw : {128, TN_WIDE}) {
+      if (tw > 128 && n < tw) continue;
+      const int d = split_for(tw);
+      for (int Sx : {d, d * 2, std::max(d / 2, 1), tc_min_split(kbt)}) {
+        if (Sx < tc_min_split(kbt) || Sx > kbt) continue;
+        bool dup = false;
+        for (auto& c : cand) dup |= (c.tn == tw && c.S == Sx);
+        if (!dup) cand.push_back({tw, Sx});
+      }
+    }
+    const TuneOut to{q.C, m * 8, n, q.scn * 8};
+    const int best = tune_pick(
+        s, (int)cand.size(), [&](int i) { return run(cand[i].tn, cand[i].S); }, to);
+    if (best >= 0) {
+      tn = cand[best].tn;
+      S = cand[best].S;
+      tune_put(key, (tn == TN_WIDE ? 1 : 0) + 4 * S);
+    }
+  }
+  return run(tn, S);
 }
 
 int gemm_mixed(stream_t s, char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha,

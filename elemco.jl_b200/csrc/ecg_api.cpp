@@ -7,9 +7,12 @@
 #include <exception>
 #include <new>
 
+#include <cstdio>
+
 #include "ecg_core.h"
 #include "ecg_lambda.h"
 #include "ecg_triples.h"
+#include "ecg_tune.h"
 
 using namespace ecg;
 
@@ -153,9 +156,42 @@ int ecg_set_option(ecg_ctx* c, int32_t key, int64_t value) {
         check(dev::set_device(c->device), "cudaSetDevice");
         check(dev::set_tc_wait(c->st, (uint64_t)value), "set_tc_wait");
         break;
+      case ECG_OPT_AUTOTUNE:
+        dev::set_tuning(value != 0);
+        break;
       default:
         throw Error(ECG_ERR_ARG, "unknown option key " + std::to_string(key));
     }
+  });
+}
+
+int ecg_tune_save(ecg_ctx* c, const char* path, int64_t* entries) {
+  if (!c) return ECG_ERR_ARG;
+  return guarded(c, [&] {
+    need_ptr(path, "path");
+    FILE* f = std::fopen(path, "w");
+    if (!f) throw Error(ECG_ERR_ARG, std::string("cannot write ") + path);
+    const std::string text = dev::tune_dump();
+    const size_t w = std::fwrite(text.data(), 1, text.size(), f);
+    std::fclose(f);
+    if (w != text.size()) throw Error(ECG_ERR_ARG, std::string("short write to ") + path);
+    if (entries) *entries = (int64_t)dev::tune_size();
+  });
+}
+
+int ecg_tune_load(ecg_ctx* c, const char* path, int64_t* entries) {
+  if (!c) return ECG_ERR_ARG;
+  return guarded(c, [&] {
+    need_ptr(path, "path");
+    FILE* f = std::fopen(path, "r");
+    if (!f) throw Error(ECG_ERR_ARG, std::string("cannot read ") + path);
+    std::string text;
+    char buf[4096];
+    size_t r;
+    while ((r = std::fread(buf, 1, sizeof buf, f)) > 0) text.append(buf, r);
+    std::fclose(f);
+    if (dev::tune_parse(text) < 0) throw Error(ECG_ERR_ARG, std::string("bad tuning file ") + path);
+    if (entries) *entries = (int64_t)dev::tune_size();
   });
 }
 

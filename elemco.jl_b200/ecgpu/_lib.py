@@ -24,6 +24,7 @@ ECG_DIIS_CS = 0
 ECG_DIIS_PLAIN = 1
 ECG_OPT_TRIPLES_BATCH = 1
 ECG_OPT_TC_WAIT_NS = 2
+ECG_OPT_AUTOTUNE = 3
 ECG_KT_DGEMM = 0
 ECG_KT_TCGEMM = 1
 ECG_KT_TRIPLES = 2
@@ -71,6 +72,8 @@ SIGNATURES = {
     "ecg_set_mem_cap": (C.c_int, [_P, C.c_uint64]),
     "ecg_set_precision": (C.c_int, [_P, C.c_int]),
     "ecg_set_option": (C.c_int, [_P, C.c_int32, C.c_int64]),
+    "ecg_tune_save": (C.c_int, [_P, C.c_char_p, C.POINTER(C.c_int64)]),
+    "ecg_tune_load": (C.c_int, [_P, C.c_char_p, C.POINTER(C.c_int64)]),
     "ecg_set_system": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, _D, _D, C.c_double]),
     "ecg_fock": (C.c_int, [_P, _D, _D, _D]),
     "ecg_mp2": (C.c_int, [_P, _D, _D, _D]),

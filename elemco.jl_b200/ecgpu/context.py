@@ -50,8 +50,21 @@ class Context:
     def set_precision(self, prec=ECG_PREC_FP64):
         self._chk(self._L.ecg_set_precision(self._h, int(prec)))
 
+    def tune_save(self, path):
+        """Write the GEMM tuning table; returns its number of entries."""
+        n = C.c_int64()
+        self._chk(self._L.ecg_tune_save(self._h, str(path).encode(), C.byref(n)))
+        return n.value
+
+    def tune_load(self, path):
+        """Merge a tuning file into the table; returns its number of entries."""
+        n = C.c_int64()
+        self._chk(self._L.ecg_tune_load(self._h, str(path).encode(), C.byref(n)))
+        return n.value
+
     def set_option(self, key, value):
-        """``ecg_set_option``: ECG_OPT_TRIPLES_BATCH, ECG_OPT_TC_WAIT_NS (0 = automatic)."""
+        """``ecg_set_option``: ECG_OPT_TRIPLES_BATCH, ECG_OPT_TC_WAIT_NS,
+        ECG_OPT_AUTOTUNE (0 = automatic / off)."""
         self._chk(self._L.ecg_set_option(self._h, int(key), int(value)))
 
     def set_system(self, B, h1, e0, nocc):

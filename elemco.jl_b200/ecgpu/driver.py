@@ -87,8 +87,13 @@ class ECInfo:
         return np.array([C.T @ D @ C for D in hf.ints.dipole(origin)])
 
     def context(self):
+        """The GPU context; the packaged GEMM tuning table for B200
+        (``tuning/b200.txt``, written by the autotuner) is loaded on creation."""
         if self._ctx is None:
             self._ctx = Context(self.options["gpu"].device)
+            table = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning", "b200.txt")
+            if os.path.exists(table):
+                self._ctx.tune_load(table)
         return self._ctx
 
 

@@ -73,10 +73,28 @@ int ecg_set_precision(ecg_ctx* ctx, int prec);
  *                         waits on this context's stream (default 1 s); a wait
  *                         that runs out makes the call return ECG_ERR_TIMEOUT
  *                         and the context stays usable (the kernel's final
- *                         waits on its own copies keep the 1 s bound) */
+ *                         waits on its own copies keep the 1 s bound)
+ *  ECG_OPT_AUTOTUNE       1: GEMM shapes without an entry in the tuning table
+ *                         are tuned on first use (see ecg_tune_save); 0: the
+ *                         table's entries, else the fixed rules, are used.
+ *                         The table is process-wide (all contexts and GPUs). */
 #define ECG_OPT_TRIPLES_BATCH 1
 #define ECG_OPT_TC_WAIT_NS 2
+#define ECG_OPT_AUTOTUNE 3
 int ecg_set_option(ecg_ctx* ctx, int32_t key, int64_t value);
+
+/* GEMM autotuner table (no counterpart in the reference; the reference's
+ * contractions run through TensorOperations/BLAS).  For each GEMM shape the
+ * FP64 GEMM (tile shape 64x64 / 128x64 / 64x128, split-K count) and the
+ * tensor-core GEMM (tile width 128 / 160 / 256 columns, split-K count within
+ * the FP32 accumulation bound) can choose from several configurations; with
+ * ECG_OPT_AUTOTUNE on, the first call of a shape times each candidate on its
+ * own operands (the result is unchanged) and records the fastest.
+ * ecg_tune_save writes the table to a text file ("key value" lines),
+ * ecg_tune_load merges such a file into it; *entries (may be NULL) receives
+ * the table size afterwards. */
+int ecg_tune_save(ecg_ctx* ctx, const char* path, int64_t* entries);
+int ecg_tune_load(ecg_ctx* ctx, const char* path, int64_t* entries);
 
 /* Upload the system.  B[p,q,Q] (n x n x nq) are the density-fitting factors
  * with (pq|rs) = sum_Q B[p,q,Q] B[r,s,Q] — the `mmL` file of
