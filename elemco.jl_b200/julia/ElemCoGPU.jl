@@ -17,7 +17,8 @@ column-major layout is the library's layout.  Status codes other than 0 raise
 """
 module ElemCoGPU
 
-export GPUContext, gpu_calc_cc, gpu_calc_pertT, gpu_calc_lm_cc
+export GPUContext, gpu_calc_cc, gpu_calc_pertT, gpu_calc_lm_cc, set_option!, tune_load!, tune_save,
+       ShellArrays, int1e, int2c2e, int3c2e
 
 const libecgpu = get(ENV, "ECGPU_LIB", joinpath(@__DIR__, "..", "ecgpu", "libecgpu.so"))
 
@@ -29,7 +30,18 @@ struct CcOpts
   shiftp::Cdouble
   maxdiis::Int32
   resthr::Cdouble
+  diis_dot::Int32   # ECG_DIIS_CS = 0 (the reference's closed-shell dots), ECG_DIIS_PLAIN = 1
 end
+
+const ECG_DIIS_CS = Int32(0)
+const ECG_DIIS_PLAIN = Int32(1)
+const ECG_OPT_TRIPLES_BATCH = Int32(1)
+const ECG_OPT_TC_WAIT_NS = Int32(2)
+const ECG_OPT_AUTOTUNE = Int32(3)
+const ECG_INT_OVERLAP = Int32(0)
+const ECG_INT_KINETIC = Int32(1)
+const ECG_INT_NUCLEAR = Int32(2)
+const ECG_INT_DIPOLE = Int32(3)
 
 """
     GPUContext(device=0)
@@ -59,7 +71,105 @@ end
 function options(EC)
   cc = EC.options.cc
   d = EC.options.diis
-  return CcOpts(cc.thr, cc.conven, Int32(cc.maxit), cc.shifts, cc.shiftp, Int32(d.maxdiis), d.resthr)
+  return CcOpts(cc.thr, cc.conven, Int32(cc.maxit), cc.shifts, cc.shiftp, Int32(d.maxdiis), d.resthr,
+                ECG_DIIS_CS)
+end
+
+"""
+    set_option!(ctx, key, value)
+
+`ecg_set_option`: `ECG_OPT_TRIPLES_BATCH` (triplets per (T) batch),
+`ECG_OPT_TC_WAIT_NS` (tensor-core GEMM wait bound), `ECG_OPT_AUTOTUNE`.
+"""
+set_option!(ctx::GPUContext, key::Integer, value::Integer) =
+  check(ctx, ccall((:ecg_set_option, libecgpu), Cint, (Ptr{Cvoid}, Int32, Int64),
+                   ctx.ptr, key, value))
+
+"""
+    tune_load!(ctx, path) / tune_save(ctx, path)
+
+Merge a GEMM tuning table ("key value" lines, e.g. ecgpu/tuning/b200.txt)
+into the process-wide table, or write the table; return its size.
+"""
+function tune_load!(ctx::GPUContext, path::AbstractString)
+  n = Ref{Int64}(0)
+  check(ctx, ccall((:ecg_tune_load, libecgpu), Cint, (Ptr{Cvoid}, Cstring, Ref{Int64}), ctx.ptr, path, n))
+  return n[]
+end
+function tune_save(ctx::GPUContext, path::AbstractString)
+  n = Ref{Int64}(0)
+  check(ctx, ccall((:ecg_tune_save, libecgpu), Cint, (Ptr{Cvoid}, Cstring, Ref{Int64}), ctx.ptr, path, n))
+  return n[]
+end
+
+# Shells of an ElemCo.jl BasisSet in the plain arrays of `ecg_shells`
+# (per shell: l, primitive count, centre; exponents and coefficients of the
+# basis file, shell after shell).  `shells` yields (l, centre, exps, coefs).
+struct ShellArrays
+  l::Vector{Int32}
+  nprim::Vector{Int32}
+  centre::Vector{Cdouble}
+  exps::Vector{Cdouble}
+  coefs::Vector{Cdouble}
+end
+function ShellArrays(shells)
+  l = Int32[]; np = Int32[]; cen = Cdouble[]; ex = Cdouble[]; co = Cdouble[]
+  for (ls, c, e, k) in shells
+    push!(l, ls); push!(np, length(e)); append!(cen, c); append!(ex, e); append!(co, k)
+  end
+  return ShellArrays(l, np, cen, ex, co)
+end
+struct CShells
+  nshell::Int32
+  l::Ptr{Int32}
+  nprim::Ptr{Int32}
+  centre::Ptr{Cdouble}
+  exps::Ptr{Cdouble}
+  coefs::Ptr{Cdouble}
+end
+cshells(s::ShellArrays) = CShells(length(s.l), pointer(s.l), pointer(s.nprim), pointer(s.centre),
+                                  pointer(s.exps), pointer(s.coefs))
+function nbf(s::ShellArrays)
+  n = Ref{Int32}(0)
+  GC.@preserve s ccall((:ecg_shells_nbf, libecgpu), Cint, (Ref{CShells}, Ref{Int32}), cshells(s), n)
+  return Int(n[])
+end
+
+"""
+    int1e(ctx, kind, basis; charges, xyz, origin) -> Matrix (or 3 matrices for dipoles)
+
+Overlap, kinetic, nuclear attraction or dipole integrals over real solid
+harmonics (`ecg_int1e`; libcint int1e_ovlp/kin/nuc in src/system/integrals_2idx.jl).
+"""
+function int1e(ctx::GPUContext, kind::Integer, b::ShellArrays;
+               charges=Cdouble[], xyz=Cdouble[], origin=Cdouble[0, 0, 0])
+  n = nbf(b)
+  out = zeros(n, n, kind == ECG_INT_DIPOLE ? 3 : 1)
+  q = Vector{Cdouble}(charges); r = Vector{Cdouble}(vec(xyz)); o = Vector{Cdouble}(origin)
+  GC.@preserve b q r o out check(ctx, ccall((:ecg_int1e, libecgpu), Cint,
+      (Ptr{Cvoid}, Int32, Ref{CShells}, Int32, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}),
+      ctx.ptr, kind, cshells(b), length(q), q, r, o, out))
+  return kind == ECG_INT_DIPOLE ? out : out[:, :, 1]
+end
+
+"""
+    int2c2e(ctx, fit) / int3c2e(ctx, ao, fit)
+
+The fitting metric (P|Q) and the three-index integrals (mn|P) as `[m,n,P]`
+(`ecg_int2c2e`, `ecg_int3c2e`; eri_2e2idx / eri_2e3idx of the reference).
+"""
+function int2c2e(ctx::GPUContext, f::ShellArrays)
+  n = nbf(f)
+  out = zeros(n, n)
+  GC.@preserve f out check(ctx, ccall((:ecg_int2c2e, libecgpu), Cint,
+      (Ptr{Cvoid}, Ref{CShells}, Ptr{Cdouble}), ctx.ptr, cshells(f), out))
+  return out
+end
+function int3c2e(ctx::GPUContext, a::ShellArrays, f::ShellArrays)
+  out = zeros(nbf(a), nbf(a), nbf(f))
+  GC.@preserve a f out check(ctx, ccall((:ecg_int3c2e, libecgpu), Cint,
+      (Ptr{Cvoid}, Ref{CShells}, Ref{CShells}, Ptr{Cdouble}), ctx.ptr, cshells(a), cshells(f), out))
+  return out
 end
 
 """
@@ -143,7 +253,10 @@ end
 
 function context(EM, EC)
   ctx = get!(EC.options.gpu, :ctx) do
-    GPUContext(get(EC.options.gpu, :device, 0))
+    c = GPUContext(get(EC.options.gpu, :device, 0))
+    table = joinpath(@__DIR__, "..", "ecgpu", "tuning", "b200.txt")
+    isfile(table) && tune_load!(c, table)   # the packaged B200 GEMM tuning table
+    c
   end
   SP = EC.space
   set_system!(ctx, df_factors(EM, EC), EM.FciDumps.integ1(EC.fd), EC.fd.int0, length(SP['o']))
