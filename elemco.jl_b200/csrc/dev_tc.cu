@@ -31,6 +31,7 @@
 
 #include "ecg_dev.h"
 #include "ecg_tune.h"
+#include "tma_util.cuh"
 
 namespace ecg {
 namespace dev {
@@ -53,7 +54,13 @@ constexpr int KB_ACC = (int)(TC_ACC_K / TK);
 // argument wait_ns); the final waits for the kernel's own TMA loads and MMAs
 // in flight always keep the full second, so nothing is in flight when the CTA
 // frees its tensor memory and exits.
-constexpr unsigned long long WAIT_NS = 1000000000ull;
+using tma::WAIT_NS;
+using tma::gtime;
+using tma::mbar_expect_tx;
+using tma::mbar_init;
+using tma::mbar_wait;
+using tma::smem_u32;
+using tma::tma_load_3d;
 
 template <int NSL, int TN>
 struct TcCfg {
@@ -77,52 +84,6 @@ __host__ __device__ constexpr int pair_a(int p) { return p == 2 || p == 3 ? 1 : 
 __host__ __device__ constexpr int pair_b(int p) { return p == 1 || p == 3 ? 1 : p == 4 ? 2 : 0; }
 
 __device__ int g_tc_error = 0;
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, int count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count));
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)),
-               "r"(bytes));
-}
-
-__device__ __forceinline__ unsigned long long gtime() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
-  return t;
-}
-
-// Parity wait bounded by `limit` ns of wall time (limit 0: gives up at the
-// first try_wait that finds the phase incomplete); returns false on time-out.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
-                                          unsigned long long limit = WAIT_NS) {
-  const uint32_t a = smem_u32(bar);
-  const unsigned long long t0 = gtime();
-  for (;;) {
-    uint32_t done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(a), "r"(parity));
-    if (done) return true;
-    if (gtime() - t0 >= limit) return false;
-  }
-}
-
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar,
-                                            int x, int y, int z) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(smem_u32(dst)),
-      "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
-      : "memory");
-}
 
 // UMMA shared-memory descriptor, K-major operand in the 128-byte-swizzled
 // canonical layout: 128-byte rows, 8-row (1024-byte) groups.
@@ -522,16 +483,13 @@ __global__ void split_kernel(const double* __restrict__ src, int64_t R, int64_t 
   }
 }
 
-// Driver entry point for tensor-map encoding (no libcuda link needed).
-typedef CUresult (*EncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
-                             const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
-                             const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
-                             CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+}  // namespace
+
 EncodeFn g_encode = nullptr;
-std::mutex g_tc_mu;
+std::mutex g_encode_mu;
 
 int encode_fn(EncodeFn* out) {
-  std::lock_guard<std::mutex> lk(g_tc_mu);
+  std::lock_guard<std::mutex> lk(g_encode_mu);
   if (!g_encode) {
     cudaDriverEntryPointQueryResult q;
     void* f = nullptr;
@@ -543,6 +501,8 @@ int encode_fn(EncodeFn* out) {
   *out = g_encode;
   return 0;
 }
+
+namespace {
 
 
 // rows: extent of the map (rows past it read as zero); slice_stride in BF16
@@ -1135,11 +1095,13 @@ int tc_error(int* code) {
   int h = 0;
   cudaError_t e = cudaMemcpyFromSymbol(&h, g_tc_error, sizeof(int));
   if (e != cudaSuccess) return (int)e;
-  *code = h;
   if (h) {
     int zero = 0;
     cudaMemcpyToSymbol(g_tc_error, &zero, sizeof(int));
   }
+  int d = 0;
+  if (int r = dtma_error(&d)) return r;
+  *code = h ? h : (d ? 16 + d : 0);
   return 0;
 }
 

@@ -625,7 +625,7 @@ int ecg_diag_gemm(ecg_ctx* c, char ta, char tb, int64_t m, int64_t n, int64_t k,
     check(dev::sync(c->st), "sync");
     int tc = 0;
     check(dev::tc_error(&tc), "tc_error");
-    if (tc) throw Error(ECG_ERR_TIMEOUT, "tensor-core GEMM wait timed out (code " +
+    if (tc) throw Error(ECG_ERR_TIMEOUT, "GEMM wait timed out (code " +
                                              std::to_string(tc) + ")");
   });
 }

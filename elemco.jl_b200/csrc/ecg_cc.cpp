@@ -96,13 +96,10 @@ double scal(Ctx& c, int i) { return c.hscal[i]; }
 void sync_scalars(Ctx& c, int count) {
   check(dev::d2h(c.hscal, c.dscal, sizeof(double) * count, c.st), "d2h scalars");
   check(dev::sync(c.st), "stream sync");
-  if (c.prec == ECG_PREC_MIXED) {
-    int tc = 0;
-    check(dev::tc_error(&tc), "tc_error");
-    if (tc)
-      throw Error(ECG_ERR_TIMEOUT,
-                  "tensor-core GEMM wait timed out (code " + std::to_string(tc) + ")");
-  }
+  int tc = 0;
+  check(dev::tc_error(&tc), "tc_error");
+  if (tc)
+    throw Error(ECG_ERR_TIMEOUT, "GEMM wait timed out (code " + std::to_string(tc) + ")");
 }
 
 // --------------------------------------------------------------- setup

@@ -72,6 +72,18 @@ struct Gemm {
   const int64_t* ptab = nullptr;
 };
 int gemm_strided(stream_t s, const Gemm& g);
+// FP64 GEMM with TMA-staged operands (dev_dgemm.cu) for plain GEMMs: C with
+// unit row stride, no dn/kseg/ptab, each operand contiguous along its row
+// index or along k with its other strides even (16-byte multiples) and a
+// 16-byte-aligned base.  cfg selects the tile (0: 64x64, 1: 128x64, 2: 64x128,
+// 3: 128x128); nsplit > 1 (batch 1) cuts K into slices summed in a fixed
+// order.  Returns -1, launching nothing, when TMA cannot address an operand.
+constexpr int DTMA_CONFIGS = 4;
+bool dgemm_tma_usable(const Gemm& q);
+int dgemm_tma(stream_t s, const Gemm& q, int cfg, int nsplit);
+// Time-out code of the TMA FP64 GEMM's bounded waits since the last call
+// (0 = none); reading clears it.
+int dtma_error(int* code);
 // Split-BF16 tensor-core version of gemm_strided (batch 1, no dn/kseg).
 int gemm_strided_mixed(stream_t s, const Gemm& g);
 
@@ -237,7 +249,8 @@ int gemm_splitk_noalloc(stream_t s, char ta, char tb, int64_t m, int64_t n, int6
 
 // Split-BF16 tensor-core GEMM (tcgen05, FP32 accumulate, ~FP32 accuracy),
 // same interface as gemm().  tc_error() returns and clears the time-out code
-// of the tensor-core kernels (0 = none).
+// of the kernels with bounded mbarrier waits (0 = none; 1-4 tensor-core GEMM,
+// 17 TMA-staged FP64 GEMM).
 int gemm_mixed(stream_t s, char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha,
                const double* A, int64_t lda, const double* B, int64_t ldb, double beta,
                double* C, int64_t ldc);

@@ -462,11 +462,9 @@ void pert_triples(Ctx& c, const double* U1h, const double* U2h, double* et, doub
   std::vector<double> Eh(2 * nt);
   check(dev::d2h(Eh.data(), Et, 2 * nt * 8, s), "d2h");
   check(dev::sync(s), "sync");
-  if (mixed) {
-    int tc = 0;
-    check(dev::tc_error(&tc), "tc_error");
-    if (tc) throw Error(ECG_ERR_TIMEOUT, "tensor-core GEMM wait timed out in (T)");
-  }
+  int tc = 0;
+  check(dev::tc_error(&tc), "tc_error");
+  if (tc) throw Error(ECG_ERR_TIMEOUT, "GEMM wait timed out in (T) (code " + std::to_string(tc) + ")");
   // sum K X, and the singles / Fock term sum X Y (cc_triples.jl:143-156 / :286-294)
   double Enb3 = 0.0, Esf = 0.0;
   for (int64_t q = 0; q < nt; ++q) {

@@ -1,0 +1,100 @@
+// tma_util.cuh — mbarrier and TMA helpers shared by the sm_100a kernels
+// (the split-BF16 tensor-core GEMM and the TMA-staged FP64 GEMM).
+//
+// Every wait is bounded by wall time (%globaltimer): a kernel that gives up
+// records an error code, lets its own copies in flight finish (again
+// bounded) and returns, so a stuck wait never hangs the device.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace ecg {
+namespace dev {
+namespace tma {
+
+// Default bound on one mbarrier wait: 1 s.
+constexpr unsigned long long WAIT_NS = 1000000000ull;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+// Arrive once and add `bytes` to the transaction count of the current phase.
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)),
+               "r"(bytes));
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long gtime() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+  return t;
+}
+
+// Parity wait bounded by `limit` ns of wall time; returns false on time-out.
+// The first probe does not block (test_wait): a limit below 1 us, the
+// resolution of %globaltimer, gives up as soon as that probe finds the phase
+// incomplete.  Later probes use try_wait, which may suspend the thread for a
+// while inside the hardware.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
+                                          unsigned long long limit = WAIT_NS) {
+  const uint32_t a = smem_u32(bar);
+  {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (limit < 1000) return false;
+  }
+  const unsigned long long t0 = gtime();
+  for (;;) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (gtime() - t0 >= limit) return false;
+  }
+}
+
+// Tiled 3-D TMA load of one box at element coordinates (x, y, z) into shared
+// memory, completing on `bar` (no multicast).  x times the element size must
+// be a multiple of 16 bytes.
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar,
+                                            int x, int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(smem_u32(dst)),
+      "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
+}  // namespace tma
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda
+// link needed).
+typedef CUresult (*EncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                             const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                             const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                             CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+int encode_fn(EncodeFn* out);
+
+}  // namespace dev
+}  // namespace ecg

@@ -85,9 +85,10 @@ int ecg_set_option(ecg_ctx* ctx, int32_t key, int64_t value);
 
 /* GEMM autotuner table (no counterpart in the reference; the reference's
  * contractions run through TensorOperations/BLAS).  For each GEMM shape the
- * FP64 GEMM (tile shape 64x64 / 128x64 / 64x128, split-K count) and the
- * tensor-core GEMM (tile width 128 / 160 / 256 columns, split-K count within
- * the FP32 accumulation bound) can choose from several configurations; with
+ * FP64 GEMM (TMA-staged tiles 64x64 / 128x64 / 64x128 / 128x128 or cp.async-
+ * staged tiles 64x64 / 128x64 / 64x128, split-K count) and the tensor-core
+ * GEMM (tile width 128 / 160 / 256 columns, split-K count within the FP32
+ * accumulation bound) can choose from several configurations; with
  * ECG_OPT_AUTOTUNE on, the first call of a shape times each candidate on its
  * own operands (the result is unchanged) and records the fastest.
  * ecg_tune_save writes the table to a text file ("key value" lines),
