@@ -1383,8 +1383,9 @@ int combine(stream_t s, int64_t n, int m, const double* const* X, const double* 
 
 __global__ void ladder_pack_t_kernel(int nv, int no, const double* __restrict__ T,
                                      const int2* __restrict__ cdp, const int2* __restrict__ ijp,
-                                     double* __restrict__ Ts, double* __restrict__ Ta) {
-  const int64_t v = nv, o = no, ncdp = v * (v + 1) / 2, ncdm = v * (v - 1) / 2;
+                                     double* __restrict__ Ts, double* __restrict__ Ta,
+                                     int64_t ldp, int64_t ldm) {
+  const int64_t v = nv, o = no, ncdp = v * (v + 1) / 2;
   const int64_t nijp = o * (o + 1) / 2, total = ncdp * nijp;
   for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
        idx += (int64_t)gridDim.x * blockDim.x) {
@@ -1392,24 +1393,24 @@ __global__ void ladder_pack_t_kernel(int nv, int no, const double* __restrict__ 
     const int2 cd = cdp[k], ij = ijp[q];
     const int64_t ij0 = v * v * (ij.x + o * ij.y);
     const double x = T[cd.x + v * cd.y + ij0], y = T[cd.y + v * cd.x + ij0];
-    Ts[idx] = 0.5 * (x + y);
-    if (cd.x < cd.y && ij.x < ij.y) Ta[(k - cd.y) + ncdm * (q - ij.y)] = 0.5 * (x - y);
+    Ts[k + ldp * q] = 0.5 * (x + y);
+    if (cd.x < cd.y && ij.x < ij.y) Ta[(k - cd.y) + ldm * (q - ij.y)] = 0.5 * (x - y);
   }
 }
 
 int ladder_pack_t(stream_t s, int nv, int no, const double* T2, const int* cdp, const int* ijp,
-                  double* Ts, double* Ta) {
+                  double* Ts, double* Ta, int64_t ldp, int64_t ldm) {
   int64_t total = (int64_t)nv * (nv + 1) / 2 * ((int64_t)no * (no + 1) / 2);
   ladder_pack_t_kernel<<<grid_for(total), 256, 0, (cudaStream_t)s>>>(
-      nv, no, T2, (const int2*)cdp, (const int2*)ijp, Ts, Ta);
+      nv, no, T2, (const int2*)cdp, (const int2*)ijp, Ts, Ta, ldp, ldm);
   return launched();
 }
 
 __global__ void ladder_pack_v_kernel(int nv, int a0, int na, int npairs,
                                      const int2* __restrict__ pairs, const int2* __restrict__ cdp,
                                      const double* __restrict__ V, double* __restrict__ Vp,
-                                     double* __restrict__ Vm) {
-  const int64_t v = nv, ncdp = v * (v + 1) / 2, ncdm = v * (v - 1) / 2, total = ncdp * npairs;
+                                     double* __restrict__ Vm, int64_t ldp, int64_t ldm) {
+  const int64_t v = nv, ncdp = v * (v + 1) / 2, total = ncdp * npairs;
   const int64_t lda = v * na;  // Vblk[c + v a' + v na (d + v b'')]
   for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
        idx += (int64_t)gridDim.x * blockDim.x) {
@@ -1418,16 +1419,17 @@ __global__ void ladder_pack_v_kernel(int nv, int a0, int na, int npairs,
     const int64_t ap = ab.x - a0, bp = ab.y - a0;
     const double x = V[cd.x + v * ap + lda * (cd.y + v * bp)];
     const double y = V[cd.y + v * ap + lda * (cd.x + v * bp)];
-    Vp[idx] = (cd.x == cd.y) ? x : x + y;
-    if (cd.x < cd.y && ab.x < ab.y) Vm[(k - cd.y) + ncdm * (pr - ap - 1)] = x - y;
+    Vp[k + ldp * pr] = (cd.x == cd.y) ? x : x + y;
+    if (cd.x < cd.y && ab.x < ab.y) Vm[(k - cd.y) + ldm * (pr - ap - 1)] = x - y;
   }
 }
 
 int ladder_pack_v(stream_t s, int nv, int a0, int na, int npairs, const int* pairs,
-                  const int* cdp, const double* Vblk, double* Vp, double* Vm) {
+                  const int* cdp, const double* Vblk, double* Vp, double* Vm, int64_t ldp,
+                  int64_t ldm) {
   int64_t total = (int64_t)nv * (nv + 1) / 2 * npairs;
   ladder_pack_v_kernel<<<grid_for(total), 256, 0, (cudaStream_t)s>>>(
-      nv, a0, na, npairs, (const int2*)pairs, (const int2*)cdp, Vblk, Vp, Vm);
+      nv, a0, na, npairs, (const int2*)pairs, (const int2*)cdp, Vblk, Vp, Vm, ldp, ldm);
   return launched();
 }
 

@@ -328,19 +328,23 @@ void ladder(Ctx& c, const double* Bf, const double* BfT, const double* T2, doubl
   const int64_t o = c.no, v = c.nv, Q = c.nq;
   const int64_t ncdp = v * (v + 1) / 2, ncdm = v * (v - 1) / 2;
   const int64_t nijp = o * (o + 1) / 2, nijm = o * (o - 1) / 2;
+  // leading dimensions of the packed cd index, rounded up to even so that the
+  // TMA-staged FP64 GEMM can address the packed operands
+  const int64_t ldp = (ncdp + 1) / 2 * 2, ldm = std::max<int64_t>((ncdm + 1) / 2 * 2, 2);
   dev::stream_t s = c.st;
   const int64_t mark = c.ws.mark();
-  double* Ts = c.ws.get(ncdp * nijp);
-  double* Ta = c.ws.get(std::max<int64_t>(ncdm * nijm, 1));
-  check(dev::ladder_pack_t(s, (int)v, (int)o, T2, c.cdp, c.ijp, Ts, Ta), "ladder pack T");
+  double* Ts = c.ws.get(ldp * nijp);
+  double* Ta = c.ws.get(std::max<int64_t>(ldm * nijm, 1));
+  check(dev::ladder_pack_t(s, (int)v, (int)o, T2, c.cdp, c.ijp, Ts, Ta, ldp, ldm),
+        "ladder pack T");
   int64_t maxpp = 0, maxv = 0;
   for (auto& b : c.lblocks) {
     maxpp = std::max<int64_t>(maxpp, b.npp);
     maxv = std::max<int64_t>(maxv, v * b.na * v * (v - b.a0));
   }
   double* V = c.ws.get(maxv);
-  double* Vp = c.ws.get(ncdp * maxpp);
-  double* Vm = c.ws.get(std::max<int64_t>(ncdm * maxpp, 1));
+  double* Vp = c.ws.get(ldp * maxpp);
+  double* Vm = c.ws.get(std::max<int64_t>(ldm * maxpp, 1));
   double* Lp = c.ws.get(maxpp * nijp);
   double* Lm = c.ws.get(std::max<int64_t>(maxpp * nijm, 1));
   // Mixed precision: the operands shared by every a-block (BfT for the V
@@ -369,8 +373,8 @@ void ladder(Ctx& c, const double* Bf, const double* BfT, const double* T2, doubl
     pTa = pVp + eVp;
     pVm = pTa + eTa;
     if (mv) check(dev::tc_split(s, BfT, v * v, Q, 1, v * v, NSL, pB, &oB), "split BfT");
-    if (mp) check(dev::tc_split(s, Ts, nijp, ncdp, ncdp, 1, NSL, pTs, &oTs), "split T+");
-    if (mm) check(dev::tc_split(s, Ta, nijm, ncdm, ncdm, 1, NSL, pTa, &oTa), "split T-");
+    if (mp) check(dev::tc_split(s, Ts, nijp, ncdp, ldp, 1, NSL, pTs, &oTs), "split T+");
+    if (mm) check(dev::tc_split(s, Ta, nijm, ncdm, ldm, 1, NSL, pTa, &oTa), "split T-");
   }
   const bool fused = mp && mm;  // V+/- packed into BF16 slices directly
   const bool vf32 = fused && mv && Q <= dev::TC_ACC_K;
@@ -398,27 +402,28 @@ void ladder(Ctx& c, const double* Bf, const double* BfT, const double* T2, doubl
       check(dev::tc_bind(pVp, b.npp, ncdp, NSL, &oVp), "bind V+");
       if (b.npm > 0) check(dev::tc_bind(pVm, b.npm, ncdm, NSL, &oVm), "bind V-");
     } else {
-      check(dev::ladder_pack_v(s, (int)v, b.a0, b.na, b.npp, pairs, c.cdp, V, Vp, Vm), "pack V");
+      check(dev::ladder_pack_v(s, (int)v, b.a0, b.na, b.npp, pairs, c.cdp, V, Vp, Vm, ldp, ldm),
+            "pack V");
     }
     if (mp) {
-      if (!fused) check(dev::tc_split(s, Vp, b.npp, ncdp, ncdp, 1, NSL, pVp, &oVp), "split V+");
+      if (!fused) check(dev::tc_split(s, Vp, b.npp, ncdp, ldp, 1, NSL, pVp, &oVp), "split V+");
       dev::TcGemm g;
       g.m = b.npp; g.n = nijp; g.A[0] = &oVp; g.B[0] = &oTs;
       g.C = Lp; g.scm = 1; g.scn = b.npp;
       check(dev::tc_gemm(s, g), "gemm ladder +");
     } else {
-      check(dev::gemm(s, 'T', 'N', b.npp, nijp, ncdp, 1.0, Vp, ncdp, Ts, ncdp, 0.0, Lp, b.npp),
+      check(dev::gemm(s, 'T', 'N', b.npp, nijp, ncdp, 1.0, Vp, ldp, Ts, ldp, 0.0, Lp, b.npp),
             "gemm ladder +");
     }
     if (b.npm > 0 && nijm > 0) {
       if (mm) {
-        if (!fused) check(dev::tc_split(s, Vm, b.npm, ncdm, ncdm, 1, NSL, pVm, &oVm), "split V-");
+        if (!fused) check(dev::tc_split(s, Vm, b.npm, ncdm, ldm, 1, NSL, pVm, &oVm), "split V-");
         dev::TcGemm g;
         g.m = b.npm; g.n = nijm; g.A[0] = &oVm; g.B[0] = &oTa;
         g.C = Lm; g.scm = 1; g.scn = b.npm;
         check(dev::tc_gemm(s, g), "gemm ladder -");
       } else {
-        check(dev::gemm(s, 'T', 'N', b.npm, nijm, ncdm, 1.0, Vm, ncdm, Ta, ncdm, 0.0, Lm,
+        check(dev::gemm(s, 'T', 'N', b.npm, nijm, ncdm, 1.0, Vm, ldm, Ta, ldm, 0.0, Lm,
                         b.npm),
               "gemm ladder -");
       }

@@ -292,10 +292,13 @@ void ktime_end(stream_t s, int family, int slot, double work);
 //   ladder_pack_v: Vblk[c,a',d,b''] (a' = a-a0, b'' = b-a0) ->
 //                  Vp[cd+,pair+] = V[acbd]+V[adbc] (c<d), V[acbc] (c=d);  Vm[cd-,pair-] = V[acbd]-V[adbc]
 //   ladder_unpack: R2[a,b,i,j] += Lp+Lm, R2[b,a,i,j] += Lp-Lm, R2[a,b,j,i] += Lp-Lm, R2[b,a,j,i] += Lp+Lm
+// The packed cd index runs fastest, with leading dimensions ldp (>= v(v+1)/2)
+// for Ts / Vp and ldm (>= v(v-1)/2) for Ta / Vm (even values let TMA stage them).
 int ladder_pack_t(stream_t s, int nv, int no, const double* T2, const int* cdp, const int* ijp,
-                  double* Ts, double* Ta);
+                  double* Ts, double* Ta, int64_t ldp, int64_t ldm);
 int ladder_pack_v(stream_t s, int nv, int a0, int na, int npairs, const int* pairs,
-                  const int* cdp, const double* Vblk, double* Vp, double* Vm);
+                  const int* cdp, const double* Vblk, double* Vp, double* Vm, int64_t ldp,
+                  int64_t ldm);
 int ladder_unpack(stream_t s, int nv, int no, int a0, int npairs, const int* pairs,
                   const int* ijp, const double* Lp, const double* Lm, double* R2);
 
