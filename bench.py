@@ -712,8 +712,10 @@ def main():
         "config": {"workload": f"{a.workload} {a.method.upper()} (o={no}, v={nv}, nQ={nq}): "
                                f"{wdesc}",
                    "precision": "fp64",
-                   "l2": "inputs larger than L2 (T2 466 MB, B 792 MB) and L2 flushed "
-                         "(256 MiB write) between steps",
+                   "l2": (f"L2 flushed (256 MiB write) between steps; T2 "
+                          f"{8 * n2 / 1e6:.0f} MB, B {8 * (no + nv) ** 2 * nq / 1e6:.0f} MB "
+                          + ("(larger than the 126 MB L2)" if 8 * n2 > 126e6
+                             else "(smaller than the 126 MB L2)")),
                    "parallelism": f"replicas x{world}",
                    "gemm_tuning": f"{tune_entries} tuned GEMM shapes "
                                   f"({os.path.relpath(TUNE_TABLE, ROOT)})" if tune_entries
