@@ -13,6 +13,7 @@
 
 #include "ecg_dev.h"
 #include "ecg_tune.h"
+#include "triples_perm.h"
 
 namespace ecg {
 namespace dev {
@@ -1153,6 +1154,20 @@ int to_f32(stream_t s, int64_t n, const double* x, float* y) {
   return launched();
 }
 
+__global__ void to_f32_pairs_kernel(int64_t n, const double* __restrict__ a,
+                                    const double* __restrict__ b, float2* __restrict__ y) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = make_float2((float)a[i], (float)b[i]);
+}
+
+int to_f32_pairs(stream_t s, int64_t n, const double* a, const double* b, void* out) {
+  if (n <= 0) return 0;
+  to_f32_pairs_kernel<<<grid_for(n, 256, 148 * 16), 256, 0, (cudaStream_t)s>>>(
+      n, a, b, reinterpret_cast<float2*>(out));
+  return launched();
+}
+
 // exponent field all ones: infinity or NaN
 __global__ void nonfinite_kernel(int64_t n, const double* __restrict__ x, double* flag) {
   bool bad = false;
@@ -1470,52 +1485,6 @@ int ladder_unpack(stream_t s, int nv, int no, int a0, int npairs, const int* pai
 
 // ---------------------------------------------------------------- (T)
 //
-// Permutations s of (0,1,2) in the order (012)(021)(102)(120)(201)(210).
-__host__ __device__ constexpr int perm3(int q, int d) {
-  return q == 0   ? d
-         : q == 1 ? (d == 0 ? 0 : 3 - d)
-         : q == 2 ? (d == 2 ? 2 : 1 - d)
-         : q == 3 ? (d == 0 ? 1 : d == 1 ? 2 : 0)
-         : q == 4 ? (d == 0 ? 2 : d - 1)
-                  : 2 - d;
-}
-__host__ __device__ constexpr int perm3_index(int t0, int t1) {
-  return 2 * t0 + (t0 == 0 ? (t1 == 2) : t0 == 1 ? (t1 == 2) : (t1 == 1));
-}
-// X terms: K at (a,b,c) (a,c,b) (c,b,a) (b,a,c) (c,a,b) (b,c,a), weights 4 -2 -2 -2 1 1
-__host__ __device__ constexpr int xp(int r, int d) {
-  return r == 0   ? d
-         : r == 1 ? (d == 0 ? 0 : 3 - d)
-         : r == 2 ? 2 - d
-         : r == 3 ? (d == 2 ? 2 : 1 - d)
-         : r == 4 ? (d == 0 ? 2 : d - 1)
-                  : (d == 2 ? 0 : d + 1);
-}
-// For the ordering q of an element, the ordering that X term r reads.
-__host__ __device__ constexpr int xcomp(int q, int r) {
-  return perm3_index(perm3(q, xp(r, 0)), perm3(q, xp(r, 1)));
-}
-// Parity of ordering q: (012)(120)(201) even, (021)(102)(210) odd.  For an
-// element in ordering q the transposed orderings (weight -2) are the three of
-// the other parity and the cyclic ones (weight 1) the two others of its own,
-// so X_q = 3 k_q + (sum of k over q's parity) - 2 (sum over the other).
-__host__ __device__ constexpr int perm3_parity(int q) {
-  return ((perm3(q, 0) > perm3(q, 1)) + (perm3(q, 0) > perm3(q, 2)) + (perm3(q, 1) > perm3(q, 2))) & 1;
-}
-constexpr bool x_parity_rule() {
-  for (int q = 0; q < 6; ++q) {
-    if (xcomp(q, 0) != q) return false;
-    for (int r = 1; r < 6; ++r) {
-      const int p = xcomp(q, r);
-      if (p == q || (r <= 3) == (perm3_parity(p) == perm3_parity(q))) return false;
-    }
-  }
-  return true;
-}
-static_assert(x_parity_rule(), "X term orderings follow the parity rule");
-// Index of the ordered position pair (x, y), x != y, in [0, 6).
-__host__ __device__ constexpr int pair_index(int x, int y) { return 2 * x + (y > x ? y - 1 : y); }
-
 constexpr int TCUBE = 8;
 constexpr int TPITCH = 9;                             // padded row pitch of a staged cube
 constexpr int TCUBE_ELEMS = TCUBE * TPITCH * TPITCH;  // 648
@@ -1781,66 +1750,48 @@ __global__ void final_sum_pairs_kernel(int nparts, const double* part, double* o
   if (threadIdx.x == 0) out[q] = r;
 }
 
-static int64_t energy_grid(int nv) {
+int64_t triples_energy_grid(int nv) {
   // one resident block per SM: 128 registers a thread keep the evaluation free
   // of spills; the double-buffered loads overlap it with the next orbit
   const int64_t ntri = triples_cube_count(nv);
   return ntri < 148 ? ntri : 148;
 }
 
-int64_t triples_energy_scratch_len(int nv, int nitems) { return 2 * energy_grid(nv) * nitems; }
+int64_t triples_energy_scratch_len(int nv, int nitems) { return 2 * triples_energy_grid(nv) * nitems; }
 
 int triples_energy_batched(stream_t s, int nv, int nitems, const void* K, const void* KU,
                            int64_t kstride, bool k_f32, const double* eijk_tab, const double* ev,
                            const TriplesTerms* tt_tab, const int* tri, double* scratch,
                            double* out) {
   const int64_t ntri = triples_cube_count(nv);
-  if (nv > 1290 || nitems <= 0 || nitems > 65535 || !eijk_tab || !tt_tab)
+  // FP32 K goes to triples_energy_f32_batched (dev_energy.cu)
+  if (k_f32 || nv > 1290 || nitems <= 0 || nitems > 65535 || !eijk_tab || !tt_tab)
     return (int)cudaErrorInvalidValue;
-  const int g = (int)energy_grid(nv);
+  const int g = (int)triples_energy_grid(nv);
   static DeviceFlags attr;
   if (!attr.test()) {
     cudaError_t e = cudaFuncSetAttribute(triples_energy_kernel<double, false>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          EnergySmem<double, false>::BYTES);
     if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(triples_energy_kernel<float, false>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               EnergySmem<float, false>::BYTES);
-    if (e == cudaSuccess)
       e = cudaFuncSetAttribute(triples_energy_kernel<double, true>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                EnergySmem<double, true>::BYTES);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(triples_energy_kernel<float, true>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               EnergySmem<float, true>::BYTES);
     attr.set(e);
   }
   cudaStream_t st = (cudaStream_t)s;
   const dim3 grid((unsigned)g, (unsigned)nitems);
   // algorithmic bytes: each element of K (and of KU) read once
   const int slot = ktime_begin(s, KT_TRIPLES);
-  const double kbytes = (double)nitems * (double)nv * nv * nv * (k_f32 ? 4.0 : 8.0) *
-                        (KU ? 2.0 : 1.0);
-  if (k_f32) {
-    if (KU)
-      triples_energy_kernel<float, true><<<grid, 512, EnergySmem<float, true>::BYTES, st>>>(
-          nv, (const float*)K, (const float*)KU, kstride, eijk_tab, ev, tt_tab, tri, (int)ntri,
-          scratch);
-    else
-      triples_energy_kernel<float, false><<<grid, 512, EnergySmem<float, false>::BYTES, st>>>(
-          nv, (const float*)K, nullptr, kstride, eijk_tab, ev, tt_tab, tri, (int)ntri, scratch);
-  } else {
-    if (KU)
-      triples_energy_kernel<double, true><<<grid, 512, EnergySmem<double, true>::BYTES, st>>>(
-          nv, (const double*)K, (const double*)KU, kstride, eijk_tab, ev, tt_tab, tri,
-          (int)ntri, scratch);
-    else
-      triples_energy_kernel<double, false><<<grid, 512, EnergySmem<double, false>::BYTES, st>>>(
-          nv, (const double*)K, nullptr, kstride, eijk_tab, ev, tt_tab, tri, (int)ntri,
-          scratch);
-  }
+  const double kbytes = (double)nitems * (double)nv * nv * nv * 8.0 * (KU ? 2.0 : 1.0);
+  if (KU)
+    triples_energy_kernel<double, true><<<grid, 512, EnergySmem<double, true>::BYTES, st>>>(
+        nv, (const double*)K, (const double*)KU, kstride, eijk_tab, ev, tt_tab, tri,
+        (int)ntri, scratch);
+  else
+    triples_energy_kernel<double, false><<<grid, 512, EnergySmem<double, false>::BYTES, st>>>(
+        nv, (const double*)K, nullptr, kstride, eijk_tab, ev, tt_tab, tri, (int)ntri,
+        scratch);
   ktime_end(s, KT_TRIPLES, slot, kbytes);
   int e = launched();
   if (e) return e;

@@ -1099,9 +1099,10 @@ int tc_error(int* code) {
     int zero = 0;
     cudaMemcpyToSymbol(g_tc_error, &zero, sizeof(int));
   }
-  int d = 0;
+  int d = 0, en = 0;
   if (int r = dtma_error(&d)) return r;
-  *code = h ? h : (d ? 16 + d : 0);
+  if (int r = energy_error(&en)) return r;
+  *code = h ? h : d ? 16 + d : (en ? 32 + en : 0);
   return 0;
 }
 

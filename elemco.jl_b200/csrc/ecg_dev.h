@@ -206,6 +206,8 @@ int combine(stream_t s, int64_t n, int m, const double* const* X, const double* 
 
 // y[i] = (float)x[i]
 int to_f32(stream_t s, int64_t n, const double* x, float* y);
+// out[i] = (float(a[i]), float(b[i])) as float2 pairs (out 8-byte aligned)
+int to_f32_pairs(stream_t s, int64_t n, const double* a, const double* b, void* out);
 // *flag = 1 if any of x[0..n) is an infinity or NaN, else 0 (device double)
 int nonfinite(stream_t s, int64_t n, const double* x, double* flag);
 
@@ -229,15 +231,40 @@ struct TriplesTerms {
 };
 int64_t triples_cube_count(int nv);
 void triples_cube_table(int nv, int* tri);
-// Item b reads K + b*kstride (KU likewise), eijk_tab[b] and tt_tab[b] (device
-// tables) and writes out[2b], out[2b+1]; partial sums land in `scratch` (at
-// least triples_energy_scratch_len(nv, nitems) doubles) and are summed in a
-// fixed order.  One launch (plus one fixed-order reduction launch).
+// FP64 K: item b reads K + b*kstride (KU likewise), eijk_tab[b] and tt_tab[b]
+// (device tables) and writes out[2b], out[2b+1]; partial sums land in
+// `scratch` (at least triples_energy_scratch_len(nv, nitems) doubles) and are
+// summed in a fixed order.  One launch (plus one fixed-order reduction
+// launch).  k_f32 must be false (FP32 K: triples_energy_f32_batched).
 int64_t triples_energy_scratch_len(int nv, int nitems);
+int64_t triples_energy_grid(int nv);  // blocks per batch item of the energy kernels
 int triples_energy_batched(stream_t s, int nv, int nitems, const void* K, const void* KU,
                            int64_t kstride, bool k_f32, const double* eijk_tab, const double* ev,
                            const TriplesTerms* tt_tab, const int* tri, double* scratch,
                            double* out);
+// The same for FP32 K (and K') (dev_energy.cu).  K[a,b,c] of slot i sits at
+// K + i*kstride + a + vp*(b + v*c), vp >= v a multiple of 4 (TMA strides of
+// 16 bytes); nslots >= nitems slots at K (and KU), 16-byte aligned.  The
+// (M, N) terms are FP32 pairs per occupied pair p = x + o*y, packed by
+// triples_mn_pack: mn[p][a + vpe*b] and their transposes mt[p][b + vpe*a]
+// (vpe = v rounded up to even; triples_mn_elems float2 each).  Per item,
+// gf[r] points at the (g, f)[a] FP32 pairs of occupied index r of the triplet
+// (i, j, k) and mnpair[w] is the pair index of (j,k), (i,k), (i,j).
+struct TriplesTermsF {
+  const void* gf[3];
+  int32_t mnpair[3];
+};
+int64_t triples_mn_elems(int nv, int64_t npairs);
+int triples_mn_pack(stream_t s, int nv, int64_t npairs, const double* M, const double* N,
+                    void* mn, void* mt);
+int triples_energy_f32_batched(stream_t s, int nv, int vp, int nitems, int nslots, const float* K,
+                               const float* KU, int64_t kstride, const void* mn, const void* mt,
+                               int64_t npairs, const double* eijk_tab, const double* ev,
+                               const TriplesTermsF* tt_tab, const int* tri, double* scratch,
+                               double* out);
+// Time-out code of the FP32 energy kernel's bounded waits (0 = none); reading
+// clears it.
+int energy_error(int* code);
 
 // Split-K GEMM (column-major, device pointers) whose partial products use a
 // fixed file-scope device array instead of allocated memory; m*n must not
@@ -250,7 +277,7 @@ int gemm_splitk_noalloc(stream_t s, char ta, char tb, int64_t m, int64_t n, int6
 // Split-BF16 tensor-core GEMM (tcgen05, FP32 accumulate, ~FP32 accuracy),
 // same interface as gemm().  tc_error() returns and clears the time-out code
 // of the kernels with bounded mbarrier waits (0 = none; 1-4 tensor-core GEMM,
-// 17 TMA-staged FP64 GEMM).
+// 17 TMA-staged FP64 GEMM, 33 FP32 (T) energy kernel).
 int gemm_mixed(stream_t s, char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha,
                const double* A, int64_t lda, const double* B, int64_t ldb, double beta,
                double* C, int64_t ldc);

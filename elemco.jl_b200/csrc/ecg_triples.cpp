@@ -51,15 +51,25 @@ struct PermW {
   int64_t scm, scn, dn, scn2;
 };
 
-// n = b' + v c' in the [b,c,d] layout, n = c' + v b' in the [c,b,d] layout
-void perm_table(int i, int j, int k, int64_t v, PermW* P) {
-  const int64_t v2 = v * v;
-  P[0] = {i, j, k, false, 1, v, 0, 0};    // W^{ijk} -> K[a',b',c'] = a' + v n
-  P[1] = {j, i, k, false, v, 1, v, v2};   // W^{jik} -> K[b',a',c'] = v a' + b' + v^2 c'
-  P[2] = {i, k, j, true, 1, v, 0, 0};     // W^{ikj} -> K[a',c',b'] = a' + v n
-  P[3] = {k, j, i, true, v2, 1, 0, 0};    // W^{kji} -> K[c',b',a'] = v^2 a' + n
-  P[4] = {j, k, i, true, v, 1, v, v2};    // W^{jki} -> K[c',a',b'] = v a' + c' + v^2 b'
-  P[5] = {k, i, j, false, v2, 1, 0, 0};   // W^{kij} -> K[b',c',a'] = v^2 a' + n
+// n = b' + v c' in the [b,c,d] layout, n = c' + v b' in the [c,b,d] layout.
+// K[a,b,c] sits at a + vp b + vp v c (vp >= v: the padded pitch of the a
+// index; vp = v for FP64 K, a multiple of 4 for FP32 K so that the energy
+// kernel's TMA copies start on 16 bytes).
+void perm_table(int i, int j, int k, int64_t v, int64_t vp, PermW* P) {
+  const int64_t pv = vp * v;
+  P[1] = {j, i, k, false, vp, 1, v, pv};   // W^{jik} -> K[b',a',c'] = vp a' + b' + vp v c'
+  P[4] = {j, k, i, true, vp, 1, v, pv};    // W^{jki} -> K[c',a',b'] = vp a' + c' + vp v b'
+  if (vp == v) {  // unpadded: the column index n maps with one stride
+    P[0] = {i, j, k, false, 1, v, 0, 0};   // W^{ijk} -> K[a',b',c'] = a' + v n
+    P[2] = {i, k, j, true, 1, v, 0, 0};    // W^{ikj} -> K[a',c',b'] = a' + v n
+    P[3] = {k, j, i, true, pv, 1, 0, 0};   // W^{kji} -> K[c',b',a'] = v^2 a' + n
+    P[5] = {k, i, j, false, pv, 1, 0, 0};  // W^{kij} -> K[b',c',a'] = v^2 a' + n
+  } else {
+    P[0] = {i, j, k, false, 1, vp, v, pv};  // K[a',b',c'] = a' + vp b' + vp v c'
+    P[2] = {i, k, j, true, 1, vp, v, pv};   // K[a',c',b'] = a' + vp c' + vp v b'
+    P[3] = {k, j, i, true, pv, 1, v, vp};   // K[c',b',a'] = c' + vp b' + vp v a'
+    P[5] = {k, i, j, false, pv, 1, v, vp};  // K[b',c',a'] = b' + vp c' + vp v a'
+  }
 }
 
 // BF16 operands of one amplitude tensor (T2 or covariant U2).
@@ -128,7 +138,7 @@ struct KTables {
 constexpr int kGemmsFP64 = 9, kGemmsMixed = 3;
 
 void fill_tables(Ctx& c, const TriplesOps& ops, const SplitAmps* Sp, const std::vector<Trip>& tr,
-                 int NB, int64_t kstride, KTables& kt) {
+                 int NB, int64_t kstride, int64_t vp, KTables& kt) {
   const int64_t o = c.no, v = c.nv, v2 = v * v, v3 = v2 * v, o2 = o * o;
   const int64_t nt = (int64_t)tr.size();
   auto on = [&](int y, int z) { return o * y + o2 * v * z; };
@@ -138,7 +148,7 @@ void fill_tables(Ctx& c, const TriplesOps& ops, const SplitAmps* Sp, const std::
       const int i = tr[t].i, j = tr[t].j, k = tr[t].k;
       const int64_t offC = (t % NB) * kstride;
       PermW P[6];
-      perm_table(i, j, k, v, P);
+      perm_table(i, j, k, v, vp, P);
       auto put = [&](int q, int64_t a, int64_t b, int64_t a1, int64_t b1) {
         int64_t* e = kt.ptab.data() + (q * nt + t) * 5;
         e[0] = a; e[1] = b; e[2] = offC; e[3] = a1; e[4] = b1;
@@ -156,7 +166,7 @@ void fill_tables(Ctx& c, const TriplesOps& ops, const SplitAmps* Sp, const std::
   for (int64_t t = 0; t < nt; ++t) {
     const int i = tr[t].i, j = tr[t].j, k = tr[t].k;
     PermW P[6];
-    perm_table(i, j, k, v, P);
+    perm_table(i, j, k, v, vp, P);
     // ovoo pairs (A of both segments, B of both segments) in the order of
     // the vvvo pairs they share K's index map with
     const dev::TcOperand* ovoo[3][4] = {
@@ -196,11 +206,12 @@ void upload_tables(Ctx& c, KTables& kt) {
 // K^{ijk} = P[W] for triplets t0 .. t0+nb-1 into K slots 0 .. nb-1 (FP64 or
 // FP32), one launch per GEMM kind.
 void build_K_batch(Ctx& c, const TriplesOps& ops, const double* T, const SplitAmps* Sp,
-                   const KTables& kt, int64_t nt, int64_t t0, int nb, void* K, int64_t kstride) {
+                   const KTables& kt, int64_t nt, int64_t t0, int nb, void* K, int64_t kstride,
+                   int64_t vp) {
   const int64_t o = c.no, v = c.nv, v2 = v * v, o2 = o * o;
   dev::stream_t s = c.st;
   PermW P[6];
-  perm_table(0, 0, 0, v, P);  // output maps and layouts do not depend on i, j, k
+  perm_table(0, 0, 0, v, vp, P);  // output maps and layouts do not depend on i, j, k
   if (!ops.mixed) {
     auto tab = [&](int q) { return kt.ptab_d + (q * nt + t0) * 5; };
     for (int q = 0; q < 6; ++q) {
@@ -360,7 +371,8 @@ void pert_triples(Ctx& c, const double* U1h, const double* U2h, double* et, doub
   }
   // batches of NB triplets, one K slot each, within a 4 GiB budget
   const int64_t esz = mixed ? 4 : 8;
-  const int64_t kstride = (v3 + 31) / 32 * 32;
+  const int64_t vp = mixed ? (v + 3) / 4 * 4 : v;  // K's a pitch (see perm_table)
+  const int64_t kstride = (vp * v2 + 31) / 32 * 32;
   const int64_t per = kstride * esz * (lam ? 2 : 1);
   int64_t nbmax = std::min<int64_t>({256, nt, ((int64_t)4 << 30) / per});
   if (c.triples_batch > 0) nbmax = std::min(nbmax, c.triples_batch);
@@ -368,10 +380,10 @@ void pert_triples(Ctx& c, const double* U1h, const double* U2h, double* et, doub
   void* K = c.alloc((NB * kstride * esz + 7) / 8, "(T) K slots");
   void* KU = lam ? (void*)c.alloc((NB * kstride * esz + 7) / 8, "(T) K(Lambda) slots") : nullptr;
   KTables KT, KUt;
-  fill_tables(c, ops, &ST, tr, NB, kstride, KT);
+  fill_tables(c, ops, &ST, tr, NB, kstride, vp, KT);
   upload_tables(c, KT);
   if (lam) {
-    fill_tables(c, ops, &SU, tr, NB, kstride, KUt);
+    fill_tables(c, ops, &SU, tr, NB, kstride, vp, KUt);
     upload_tables(c, KUt);
   }
 
@@ -393,42 +405,57 @@ void pert_triples(Ctx& c, const double* U1h, const double* U2h, double* et, doub
   check(dev::h2d(gf, gh.data(), v * o * 8, s), "h2d");
   check(dev::h2d(gf + v * o, fh.data(), v * o * 8, s), "h2d");
   const double* Nsrc = lam ? U2c : c.T2();
-  // the energy kernel reads g, f, M and N in K's precision: FP32 copies in
-  // mixed precision (they enter only the singles/Fock term sum X Y)
-  const void* gfe = gf;
-  const void* Me = c.Kvvoo;
-  const void* Ne = Nsrc;
-  if (mixed) {
-    const int64_t n2 = v2 * o * o;
-    float* t32 = reinterpret_cast<float*>(c.alloc((2 * v * o + 2 * n2 + 1) / 2, "(T) FP32 terms"));
-    check(dev::to_f32(s, 2 * v * o, gf, t32), "FP32 g, f");
-    check(dev::to_f32(s, n2, c.Kvvoo, t32 + 2 * v * o), "FP32 <ij|ab>");
-    check(dev::to_f32(s, n2, Nsrc, t32 + 2 * v * o + n2), "FP32 amplitudes");
-    gfe = t32;
-    Me = t32 + 2 * v * o;
-    Ne = t32 + 2 * v * o + n2;
-  }
-  auto at = [&](const void* p, int64_t off) {
-    return static_cast<const void*>(static_cast<const char*>(p) + esz * off);
-  };
-  auto M = [&](int x, int y) { return at(Me, v2 * (x + o * y)); };
-  auto N = [&](int x, int y) { return at(Ne, v2 * (x + o * y)); };
-  std::vector<dev::TriplesTerms> terms(nt);
   std::vector<double> eijk(nt);
-  for (int64_t t = 0; t < nt; ++t) {
-    const int i = tr[t].i, j = tr[t].j, k = tr[t].k;
-    dev::TriplesTerms& tt = terms[t];
-    tt.g[0] = at(gfe, v * i); tt.g[1] = at(gfe, v * j); tt.g[2] = at(gfe, v * k);
-    tt.f[0] = at(gfe, v * (o + i)); tt.f[1] = at(gfe, v * (o + j)); tt.f[2] = at(gfe, v * (o + k));
-    tt.M[0] = M(j, k); tt.M[1] = M(i, k); tt.M[2] = M(i, j);
-    tt.N[0] = N(j, k); tt.N[1] = N(i, k); tt.N[2] = N(i, j);
-    eijk[t] = tr[t].eijk;
-  }
-  auto* terms_d = reinterpret_cast<dev::TriplesTerms*>(
-      c.alloc((int64_t)((nt * sizeof(dev::TriplesTerms) + 7) / 8), "(T) energy terms"));
+  for (int64_t t = 0; t < nt; ++t) eijk[t] = tr[t].eijk;
   double* eijk_d = c.alloc(nt, "(T) denominators");
-  check(dev::h2d(terms_d, terms.data(), nt * sizeof(dev::TriplesTerms), s), "h2d");
   check(dev::h2d(eijk_d, eijk.data(), nt * 8, s), "h2d");
+  // energy terms per triplet.  FP64: g, f, M = <ij|ab>, N = T2 (or U2c) as
+  // separate arrays.  Mixed precision: FP32 copies interleaved in pairs,
+  // (g, f)[a] per occupied index and (M, N)[a + v b] per occupied pair, which
+  // the FP32 energy kernel stages with one 8-byte copy per position (they
+  // enter only the singles/Fock term sum X Y).
+  dev::TriplesTerms* terms_d = nullptr;
+  dev::TriplesTermsF* termsf_d = nullptr;
+  float* MNp = nullptr;
+  float* MNt = nullptr;
+  if (mixed) {
+    float* GF = reinterpret_cast<float*>(c.alloc(v * o, "(T) FP32 (g, f)"));  // float2 [occ][a]
+    const int64_t mne = dev::triples_mn_elems((int)v, o * o);
+    MNp = reinterpret_cast<float*>(c.alloc(mne, "(T) FP32 (M, N)"));
+    MNt = reinterpret_cast<float*>(c.alloc(mne, "(T) FP32 (M, N) transposed"));
+    check(dev::to_f32_pairs(s, v * o, gf, gf + v * o, GF), "FP32 (g, f)");
+    check(dev::triples_mn_pack(s, (int)v, o * o, c.Kvvoo, Nsrc, MNp, MNt),
+          "FP32 (<ij|ab>, amplitudes)");
+    auto gfp = [&](int x) { return static_cast<const void*>(GF + 2 * v * x); };
+    std::vector<dev::TriplesTermsF> terms(nt);
+    for (int64_t t = 0; t < nt; ++t) {
+      const int i = tr[t].i, j = tr[t].j, k = tr[t].k;
+      dev::TriplesTermsF& tt = terms[t];
+      tt.gf[0] = gfp(i); tt.gf[1] = gfp(j); tt.gf[2] = gfp(k);
+      tt.mnpair[0] = (int32_t)(j + o * k);
+      tt.mnpair[1] = (int32_t)(i + o * k);
+      tt.mnpair[2] = (int32_t)(i + o * j);
+    }
+    termsf_d = reinterpret_cast<dev::TriplesTermsF*>(
+        c.alloc((int64_t)((nt * sizeof(dev::TriplesTermsF) + 7) / 8), "(T) energy terms"));
+    check(dev::h2d(termsf_d, terms.data(), nt * sizeof(dev::TriplesTermsF), s), "h2d");
+  } else {
+    auto at = [&](const double* p, int64_t off) { return static_cast<const void*>(p + off); };
+    auto M = [&](int x, int y) { return at(c.Kvvoo, v2 * (x + o * y)); };
+    auto N = [&](int x, int y) { return at(Nsrc, v2 * (x + o * y)); };
+    std::vector<dev::TriplesTerms> terms(nt);
+    for (int64_t t = 0; t < nt; ++t) {
+      const int i = tr[t].i, j = tr[t].j, k = tr[t].k;
+      dev::TriplesTerms& tt = terms[t];
+      tt.g[0] = at(gf, v * i); tt.g[1] = at(gf, v * j); tt.g[2] = at(gf, v * k);
+      tt.f[0] = at(gf, v * (o + i)); tt.f[1] = at(gf, v * (o + j)); tt.f[2] = at(gf, v * (o + k));
+      tt.M[0] = M(j, k); tt.M[1] = M(i, k); tt.M[2] = M(i, j);
+      tt.N[0] = N(j, k); tt.N[1] = N(i, k); tt.N[2] = N(i, j);
+    }
+    terms_d = reinterpret_cast<dev::TriplesTerms*>(
+        c.alloc((int64_t)((nt * sizeof(dev::TriplesTerms) + 7) / 8), "(T) energy terms"));
+    check(dev::h2d(terms_d, terms.data(), nt * sizeof(dev::TriplesTerms), s), "h2d");
+  }
   const int64_t ncube = dev::triples_cube_count((int)v);
   std::vector<int> trih(3 * ncube);
   dev::triples_cube_table((int)v, trih.data());
@@ -445,11 +472,19 @@ void pert_triples(Ctx& c, const double* U1h, const double* U2h, double* et, doub
       if (bi == 1) check(dev::graph_capture_begin(s), "graph capture");
       const int64_t t0 = bi * NB;
       const int nb = (int)std::min<int64_t>(NB, nt - t0);
-      build_K_batch(c, ops, c.T2(), &ST, KT, nt, t0, nb, K, kstride);
-      if (lam) build_K_batch(c, ops, U2c, &SU, KUt, nt, t0, nb, KU, kstride);
-      check(dev::triples_energy_batched(s, (int)v, nb, K, KU, kstride, mixed, eijk_d + t0,
-                                        c.eps + o, terms_d + t0, tri, part, Et + 2 * t0),
-            "triples energy");
+      build_K_batch(c, ops, c.T2(), &ST, KT, nt, t0, nb, K, kstride, vp);
+      if (lam) build_K_batch(c, ops, U2c, &SU, KUt, nt, t0, nb, KU, kstride, vp);
+      if (mixed)
+        check(dev::triples_energy_f32_batched(s, (int)v, (int)vp, nb, NB,
+                                              static_cast<const float*>(K),
+                                              static_cast<const float*>(KU), kstride, MNp, MNt,
+                                              o * o, eijk_d + t0, c.eps + o, termsf_d + t0, tri,
+                                              part, Et + 2 * t0),
+              "triples energy");
+      else
+        check(dev::triples_energy_batched(s, (int)v, nb, K, KU, kstride, false, eijk_d + t0,
+                                          c.eps + o, terms_d + t0, tri, part, Et + 2 * t0),
+              "triples energy");
     }
     if (nbatch > 1) {
       int64_t nodes = 0;
