@@ -66,7 +66,7 @@ struct EnergyWarpSmem {
   static constexpr int E_OFF = VEC_OFF + 3 * 3 * 8 * 8;     // (g,f): [pos][occ][l] float2
   static constexpr int BAR_OFF = E_OFF + 32 * 4;            // orbital energies [pos][l]
   static constexpr int BYTES = (BAR_OFF + 8 + 127) / 128 * 128;
-  static constexpr int WARPS = HAS_U ? 6 : 10;
+  static constexpr int WARPS = HAS_U ? 6 : 8;
   static constexpr int THREADS = 32 * WARPS;
   static constexpr int SMEM = WARPS * BYTES + 128;  // + alignment of the base
   // bytes one orbit's TMA boxes deliver (out-of-range elements included)
@@ -200,7 +200,7 @@ __global__ void __launch_bounds__(EnergyWarpSmem<HAS_U>::THREADS, 1)
       kb[q] = q * EC_CUBE + cube_coef(q, 0) * l0lo + cube_coef(q, 1) * l1lo +
               cube_coef(q, 2) * l2lo;
     float ek = 0.0f, ey = 0.0f;
-#pragma unroll 1
+#pragma unroll
     for (int ia = 0; ia < 2; ++ia) {
       const int l0 = l0lo + 4 * ia;
       const float e0 = (float)(eijk - (double)pe[l0]);
@@ -219,7 +219,7 @@ __global__ void __launch_bounds__(EnergyWarpSmem<HAS_U>::THREADS, 1)
           m01[w] = mn[(w * 6 + 0) * 64 + l0 + 8 * l1];
           m10[w] = mn[(w * 6 + 2) * 64 + l0 + 8 * l1];
         }
-#pragma unroll 2
+#pragma unroll
         for (int ic = 0; ic < 4; ++ic) {
           const int l2 = l2lo + 2 * ic;
           const float dinv = __fdividef(1.0f, e01 - pe[16 + l2]);
