@@ -496,23 +496,45 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, BK, WM, WN, STAGES>::THREADS, 
       else
         coff[j][h] = col * g.scn;
     }
+  if (g.beta == 0.0) {
+#pragma unroll
+    for (int i = 0; i < MT; ++i)
+#pragma unroll
+      for (int rr = 0; rr < NACC / 2; ++rr) {
+        const int64_t row = m0 + wm0 + i * RH + 8 * rr + gq;
+        if (row >= g.m) continue;
+#pragma unroll
+        for (int j = 0; j < NTL; ++j)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int64_t col = n0 + wn0 + j * 8 + 2 * tq + h;
+            if (col < g.n) C[row * g.scm + coff[j][h]] = g.alpha * acc[i][j][2 * rr + h];
+          }
+      }
+    return;
+  }
+  // read-modify-write: per fragment row, all C values are loaded before any
+  // store (the compiler cannot prove the stores disjoint from later loads)
 #pragma unroll
   for (int i = 0; i < MT; ++i)
 #pragma unroll
     for (int rr = 0; rr < NACC / 2; ++rr) {
       const int64_t row = m0 + wm0 + i * RH + 8 * rr + gq;
       if (row >= g.m) continue;
+      double cv[NTL][2];
+#pragma unroll
+      for (int j = 0; j < NTL; ++j)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int64_t col = n0 + wn0 + j * 8 + 2 * tq + h;
+          cv[j][h] = col < g.n ? g.beta * C[row * g.scm + coff[j][h]] : 0.0;
+        }
 #pragma unroll
       for (int j = 0; j < NTL; ++j) {
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-          int64_t col = n0 + wn0 + j * 8 + 2 * tq + h;
-          if (col < g.n) {
-            double* cp = C + row * g.scm + coff[j][h];
-            double v = g.alpha * acc[i][j][2 * rr + h];
-            if (g.beta != 0.0) v += g.beta * *cp;
-            *cp = v;
-          }
+          const int64_t col = n0 + wn0 + j * 8 + 2 * tq + h;
+          if (col < g.n) C[row * g.scm + coff[j][h]] = g.alpha * acc[i][j][2 * rr + h] + cv[j][h];
         }
       }
     }
@@ -873,6 +895,10 @@ static int gemm_launch(stream_t s, const Gemm& q) {
              q.scm, q.scn, q.scb, q.alpha, q.beta, (q.sam != 1 && q.sak == 1) ? 1 : 0,
              (q.sbk != 1 && q.sbn == 1) ? 1 : 0, 0};
   const int flags = (q.kseg > 0 ? GF_SEG : 0) | (q.dn > 0 ? GF_DN : 0) | (q.ptab ? GF_PTAB : 0);
+  if (q.mapped_tma && (flags & ~GF_DN) == 0 && dgemm_tma_usable_mapped(q)) {
+    const int e = dgemm_tma(s, q, 0, 1);
+    if (e != -1) return e;
+  }
   if (flags) {
     if ((!q.ptab && q.batch != 1) || (q.kseg > 0 && (q.kseg >= q.k || !q.A1 || !q.B1)))
       return (int)cudaErrorInvalidValue;

@@ -1,7 +1,8 @@
 // dev_dgemm.cu — FP64 GEMM with TMA-staged operands (sm_100a).
 //
-// C(m,n) = alpha * A(m,k) B(k,n) + beta * C with C column-major (unit row
-// stride), batched (3-D tensor maps, one batch item per grid z) or split over
+// C(m,n) = alpha * A(m,k) B(k,n) + beta * C with C addressed through a row
+// stride and a column map (plain column stride, or a split column index as the
+// (T) K builds use), batched (3-D tensor maps, one batch item per grid z) or split over
 // K (grid z = K slice, partial products into the stream's split-K buffer,
 // summed in a fixed order by splitk_reduce).  tcgen05 has no FP64 kind, so the
 // products run on the FP64 MMA pipe (mma.sync m8n8k4 f64).  What the Tensor
@@ -64,9 +65,12 @@ struct DCfg {
 };
 
 struct DOut {
-  double* C;  // element (i, j) of grid-z item z at C + i + j*scn + z*scb
+  // element (i, j) of grid-z item z at C + z*scb + i*scm + colmap(j), colmap(j)
+  // = (j % dn)*scn + (j / dn)*scn2 (dn = 0: j*scn)
+  double* C;
   int64_t m, n, scn, scb;
   double alpha, beta;
+  int64_t scm = 1, dn = 0, scn2 = 0;
 };
 
 __device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
@@ -127,7 +131,11 @@ __device__ __forceinline__ int frag_row(int w0, int rb, int g) {
     return w0 + 16 * (rb >> 1) + jmap(g, rb & 1);
 }
 
-template <int BM, int BN, int WM, int WN, int STAGES, int MINB, bool AKF, bool BKF>
+// RMW2: read-modify-write epilogue that loads a group of C values before
+// storing any (the (T) K builds, whose beta = 1 GEMMs spend most of their
+// epilogue waiting on those loads); the CCSD GEMMs run faster with the
+// one-by-one epilogue, so it is a separate instantiation.
+template <int BM, int BN, int WM, int WN, int STAGES, int MINB, bool AKF, bool BKF, bool RMW2>
 __global__ void __launch_bounds__(DCfg<BM, BN, WM, WN, STAGES>::THREADS, MINB)
     dgemm_tma_kernel(const __grid_constant__ CUtensorMap ma, const __grid_constant__ CUtensorMap mb,
                      DOut out, int64_t k, int64_t kslice, int split,
@@ -247,22 +255,65 @@ __global__ void __launch_bounds__(DCfg<BM, BN, WM, WN, STAGES>::THREADS, MINB)
   }
 
   double* C = out.C + (int64_t)z * out.scb;
+  int64_t coff[NTL][2];
 #pragma unroll
-  for (int i = 0; i < MT; ++i) {
-    const int64_t row = m0 + frag_row<AKF>(wm0, i, g);
-    if (row >= out.m) continue;
+  for (int j = 0; j < NTL; ++j)
 #pragma unroll
-    for (int j = 0; j < NTL; ++j)
+    for (int h = 0; h < 2; ++h) {
+      const int64_t col = n0 + frag_row<BKF>(wn0, j, 2 * t4 + h);
+      coff[j][h] = col >= out.n ? -1
+                   : out.dn > 0 ? (col % out.dn) * out.scn + (col / out.dn) * out.scn2
+                                : col * out.scn;
+    }
+  if (!RMW2 || out.beta == 0.0) {
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int64_t col = n0 + frag_row<BKF>(wn0, j, 2 * t4 + h);
-        if (col < out.n) {
-          double* cp = C + row + col * out.scn;
-          double v = out.alpha * acc[i][j][h];
-          if (out.beta != 0.0) v += out.beta * *cp;
-          *cp = v;
+    for (int i = 0; i < MT; ++i) {
+      const int64_t row = m0 + frag_row<AKF>(wm0, i, g);
+      if (row >= out.m) continue;
+      double* Cr = C + row * out.scm;
+#pragma unroll
+      for (int j = 0; j < NTL; ++j)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          if (coff[j][h] >= 0) {
+            double* cp = Cr + coff[j][h];
+            double v = out.alpha * acc[i][j][h];
+            if (out.beta != 0.0) v += out.beta * *cp;
+            *cp = v;
+          }
         }
-      }
+    }
+    return;
+  }
+  // read-modify-write: ER rows of fragments at a time (16 C values a lane)
+  // are all loaded before any store, so the loads overlap instead of waiting
+  // one by one behind stores the compiler cannot prove disjoint
+  constexpr int ER = NTL > 4 ? 1 : 2;
+#pragma unroll
+  for (int i0 = 0; i0 < MT; i0 += ER) {
+    double cv[ER][NTL][2];
+#pragma unroll
+    for (int ii = 0; ii < ER; ++ii) {
+      const int64_t row = m0 + frag_row<AKF>(wm0, i0 + ii, g);
+      const double* Cr = C + row * out.scm;
+#pragma unroll
+      for (int j = 0; j < NTL; ++j)
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+          cv[ii][j][h] = (row < out.m && coff[j][h] >= 0) ? Cr[coff[j][h]] : 0.0;
+    }
+#pragma unroll
+    for (int ii = 0; ii < ER; ++ii) {
+      const int64_t row = m0 + frag_row<AKF>(wm0, i0 + ii, g);
+      if (row >= out.m) continue;
+      double* Cr = C + row * out.scm;
+#pragma unroll
+      for (int j = 0; j < NTL; ++j)
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+          if (coff[j][h] >= 0)
+            Cr[coff[j][h]] = out.alpha * acc[i0 + ii][j][h] + out.beta * cv[ii][j][h];
+    }
   }
 }
 
@@ -310,11 +361,12 @@ bool operand_map(CUtensorMap* m, bool* kfast, const double* X, int64_t ni, int64
   return false;
 }
 
-template <int BM, int BN, int WM, int WN, int STAGES, int MINB, bool AKF, bool BKF>
+template <int BM, int BN, int WM, int WN, int STAGES, int MINB, bool AKF, bool BKF,
+          bool RMW2 = false>
 int launch_dtma(cudaStream_t st, const CUtensorMap& ma, const CUtensorMap& mb, const DOut& out,
                 int64_t k, int64_t kslice, int nz, int split) {
   using Cfg = DCfg<BM, BN, WM, WN, STAGES>;
-  auto kern = dgemm_tma_kernel<BM, BN, WM, WN, STAGES, MINB, AKF, BKF>;
+  auto kern = dgemm_tma_kernel<BM, BN, WM, WN, STAGES, MINB, AKF, BKF, RMW2>;
   // cudaFuncSetAttribute acts on the current device only: one flag per device
   static std::atomic<bool> done[128] = {};
   int d = 0;
@@ -355,13 +407,22 @@ DtmaLaunch pick(int cfg) {
     default: return launch_dtma<64, 64, 32, 32, 4, 3, AKF, BKF>;
   }
 }
+// The (T) K builds' configuration: 64x64 with the grouped read-modify-write.
+template <bool AKF, bool BKF>
+DtmaLaunch pick_rmw() {
+  return launch_dtma<64, 64, 32, 32, 4, 3, AKF, BKF, true>;
+}
 constexpr int CFG_BM[DTMA_CONFIGS] = {64, 128, 64, 128};
 constexpr int CFG_BN[DTMA_CONFIGS] = {64, 64, 128, 128};
 
 }  // namespace
 
 bool dgemm_tma_usable(const Gemm& q) {
-  if (q.dn || q.kseg || q.ptab || q.scm != 1 || q.m <= 0 || q.n <= 0 || q.k <= 0) return false;
+  return q.scm == 1 && q.dn == 0 && dgemm_tma_usable_mapped(q);
+}
+
+bool dgemm_tma_usable_mapped(const Gemm& q) {
+  if (q.kseg || q.ptab || q.m <= 0 || q.n <= 0 || q.k <= 0 || q.dn < 0) return false;
   if (q.m >= ((int64_t)1 << 31) || q.n >= ((int64_t)1 << 31) || q.k >= ((int64_t)1 << 31))
     return false;
   CUtensorMap m;
@@ -373,7 +434,8 @@ bool dgemm_tma_usable(const Gemm& q) {
 int dgemm_tma(stream_t s, const Gemm& q, int cfg, int nsplit) {
   if (cfg < 0 || cfg >= DTMA_CONFIGS) return (int)cudaErrorInvalidValue;
   cudaStream_t st = (cudaStream_t)s;
-  if (nsplit > 1 && q.batch != 1) return (int)cudaErrorInvalidValue;
+  // the split-K reduction writes C through plain strides only
+  if (nsplit > 1 && (q.batch != 1 || q.dn > 0)) return (int)cudaErrorInvalidValue;
   CUtensorMap ma, mb;
   bool akf = false, bkf = false;
   if (!operand_map(&ma, &akf, q.A, q.m, q.k, q.sam, q.sak, q.batch, q.sab, CFG_BM[cfg]) ||
@@ -381,8 +443,11 @@ int dgemm_tma(stream_t s, const Gemm& q, int cfg, int nsplit) {
     return -1;
   DtmaLaunch f = akf ? (bkf ? pick<true, true>(cfg) : pick<true, false>(cfg))
                      : (bkf ? pick<false, true>(cfg) : pick<false, false>(cfg));
+  if (q.mapped_tma && cfg == 0)
+    f = akf ? (bkf ? pick_rmw<true, true>() : pick_rmw<true, false>())
+            : (bkf ? pick_rmw<false, true>() : pick_rmw<false, false>());
   if (nsplit <= 1) {
-    DOut o{q.C, q.m, q.n, q.scn, q.scb, q.alpha, q.beta};
+    DOut o{q.C, q.m, q.n, q.scn, q.scb, q.alpha, q.beta, q.scm, q.dn, q.scn2};
     return f(st, ma, mb, o, q.k, q.k, (int)q.batch, 0);
   }
   int64_t kc = (q.k + nsplit - 1) / nsplit;

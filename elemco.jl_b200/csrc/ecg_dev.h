@@ -70,16 +70,23 @@ struct Gemm {
   const double* B1 = nullptr;
   int64_t sbk1 = 0;
   const int64_t* ptab = nullptr;
+  // run on the TMA-staged kernel whenever it can address the operands, also
+  // with a row stride or column map (the (T) K builds; other callers keep
+  // the dispatcher's choice)
+  bool mapped_tma = false;
 };
 int gemm_strided(stream_t s, const Gemm& g);
-// FP64 GEMM with TMA-staged operands (dev_dgemm.cu) for plain GEMMs: C with
-// unit row stride, no dn/kseg/ptab, each operand contiguous along its row
-// index or along k with its other strides even (16-byte multiples) and a
-// 16-byte-aligned base.  cfg selects the tile (0: 64x64, 1: 128x64, 2: 64x128,
+// FP64 GEMM with TMA-staged operands (dev_dgemm.cu): no kseg/ptab (C through
+// scm and scn or the dn/scn2 column map; no K split with dn), each operand
+// contiguous along its row index or along k with its other strides even
+// (16-byte multiples) and a 16-byte-aligned base.  cfg selects the tile (0: 64x64, 1: 128x64, 2: 64x128,
 // 3: 128x128); nsplit > 1 (batch 1) cuts K into slices summed in a fixed
 // order.  Returns -1, launching nothing, when TMA cannot address an operand.
+// dgemm_tma_usable: the cases the plain-GEMM dispatcher sends to it (C with
+// unit row stride, no column map); dgemm_tma_usable_mapped: all it accepts.
 constexpr int DTMA_CONFIGS = 4;
 bool dgemm_tma_usable(const Gemm& q);
+bool dgemm_tma_usable_mapped(const Gemm& q);
 int dgemm_tma(stream_t s, const Gemm& q, int cfg, int nsplit);
 // Time-out code of the TMA FP64 GEMM's bounded waits since the last call
 // (0 = none); reading clears it.

@@ -214,15 +214,23 @@ void build_K_batch(Ctx& c, const TriplesOps& ops, const double* T, const SplitAm
   perm_table(0, 0, 0, v, vp, P);  // output maps and layouts do not depend on i, j, k
   if (!ops.mixed) {
     auto tab = [&](int q) { return kt.ptab_d + (q * nt + t0) * 5; };
-    for (int q = 0; q < 6; ++q) {
-      dev::Gemm g;
-      g.m = v; g.n = v2; g.k = v; g.batch = nb; g.alpha = 1.0; g.beta = q ? 1.0 : 0.0;
-      g.A = T; g.sam = 1; g.sak = v;
-      g.B = P[q].l2 ? ops.V2 : ops.V1; g.sbk = v2; g.sbn = 1;
-      g.C = (double*)K; g.scm = P[q].scm; g.scn = P[q].scn; g.dn = P[q].dn; g.scn2 = P[q].scn2;
-      g.ptab = tab(q);
-      check(dev::gemm_strided(s, g), "W vvvo");
-    }
+    // The vvvo GEMMs (M = v, N = v^2, K = v): one GEMM per triplet, its
+    // operands placed from the host copy of the offset table; each fills the
+    // GPU by itself (v/64 x v^2/64 tiles) and runs on the TMA-staged kernel
+    // through K's index map.  Per K element the six contributions still add in
+    // the order q = 0..5.
+    for (int q = 0; q < 6; ++q)
+      for (int it = 0; it < nb; ++it) {
+        const int64_t* e = kt.ptab.data() + (q * nt + t0 + it) * 5;
+        dev::Gemm g;
+        g.m = v; g.n = v2; g.k = v; g.batch = 1; g.alpha = 1.0; g.beta = q ? 1.0 : 0.0;
+        g.A = T + e[0]; g.sam = 1; g.sak = v;
+        g.B = (P[q].l2 ? ops.V2 : ops.V1) + e[1]; g.sbk = v2; g.sbn = 1;
+        g.C = (double*)K + e[2];
+        g.scm = P[q].scm; g.scn = P[q].scn; g.dn = P[q].dn; g.scn2 = P[q].scn2;
+        g.mapped_tma = true;
+        check(dev::gemm_strided(s, g), "W vvvo");
+      }
     dev::Gemm g;
     g.k = 2 * o; g.kseg = o; g.alpha = -1.0; g.beta = 1.0; g.C = (double*)K; g.batch = nb;
     // (1) rows (a,b), columns c
