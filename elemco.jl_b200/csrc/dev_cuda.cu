@@ -1005,13 +1005,19 @@ static int plain_gemm(stream_t s, const GemmArgs& g, const Gemm& q) {
       for (int t = 0; t < DTMA_CONFIGS; ++t) cand.push_back({CFG_TMA + t, 1});
     const PlainChoice d = default_plain(q, false);
     if (q.batch == 1 && q.k >= 512) {
-      for (int S : {d.S, 2 * d.S, d.S / 2, 4})
+      // split counts around the rule's and the small ones that round the
+      // CTA count up to whole waves; long contractions also try the
+      // 128x128 TMA tile split
+      for (int S : {d.S, 2 * d.S, d.S / 2, 2, 3, 4, 6, 8, 12, 16})
         if (S >= 2 && S <= 64 && q.k / S >= 64) {
-          bool dup = false;
-          for (auto& x : cand) dup |= (x.S == S);
-          if (dup) continue;
-          cand.push_back({0, S});
-          if (tma) cand.push_back({CFG_TMA, S});
+          auto add = [&](int cfg) {
+            for (auto& x : cand)
+              if (x.S == S && x.cfg == cfg) return;
+            cand.push_back({cfg, S});
+          };
+          add(0);
+          if (tma) add(CFG_TMA);
+          if (tma && q.k >= 4096) add(CFG_TMA + 3);
         }
     }
     // tune_pick restores the output region it is given: the m x n columns of
