@@ -352,7 +352,10 @@ void ladder(Ctx& c, const double* Bf, const double* BfT, const double* T2, doubl
   // per call, each block reads row ranges of them; the per-block V+/- are
   // packed straight into BF16 slices (one pass over V, written in FP32 by the
   // tensor cores, which accumulate it in FP32).  Which GEMMs go to the tensor
-  // cores follows gemm_prec's size rule.
+  // cores follows gemm_prec's size rule but not its length rule: the V build
+  // contracts over the auxiliary index and still runs mixed (measured on
+  // (H2O)6/cc-pVTZ, the whole mixed ladder moves the mixed-product fixed
+  // point by -4 uEh, the other short contractions by +10).
   const double big = 67108864.0;
   const bool mv = c.mixed_active && (double)(v * c.lblocks[0].na) * (double)(v * v) * Q >= big;
   const bool mp = c.mixed_active && (double)maxpp * nijp * ncdp >= big;
