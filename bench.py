@@ -610,7 +610,8 @@ def main():
     rl_dgemm = {"bound": "tensor", "achieved": F / gemm_s / 1e12, "peak": fp64_peak,
                 "unit": "TFLOP/s", "frac": F / gemm_s / 1e12 / fp64_peak,
                 "traffic": traffic_of(f"dgemm_{a.workload}_{a.method}"),
-                "kernel": "dgemm_kernel (FP64 mma.sync, the DMMA pipe), all GEMMs of a step",
+                "kernel": "dgemm_tma_kernel and dgemm_kernel (FP64 mma.sync m8n8k4 on the DMMA pipe; "
+                          "TMA-staged or cp.async operands, per-shape tuned), all GEMMs of a step",
                 "algorithmic_flops_per_step": F, "gemm_ms_per_step": gms / R,
                 "gemm_launches_per_step": glaunch / R,
                 "executed_gemm_tflops": gflops / R / gemm_s / 1e12,
@@ -698,7 +699,8 @@ def main():
     rl_energy = {"bound": "hbm", "achieved": e_ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                  "frac": e_ach / peaks["hbm_gbs"] if e_ach else None,
                  "traffic": traffic_of(f"triples_energy_{a.workload}"),
-                 "kernel": "triples_energy_kernel (FP32 K of mixed (T)), first batch",
+                 "kernel": "triples_energy_f32_kernel (FP32 K of mixed (T), one warp per orbit, TMA-staged "
+                           "cubes), first batch",
                  "bytes_per_launch": ebytes / max(elaunch, 1), "ms_per_launch":
                  ems / max(elaunch, 1), "work": "bytes of K read once per element",
                  "peak_source": "hbm_gbs, " + peaks["source"]}

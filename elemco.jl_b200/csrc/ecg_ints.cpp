@@ -119,21 +119,34 @@ std::vector<double> sph_transform(const Basis& B) {
   return T;
 }
 
-// out (ns x ns) = T X T^T for X (nc x nc), host, small.
-void transform2(const std::vector<double>& T, int ns, int nc, const double* X, double* out) {
-  std::vector<double> Y((size_t)ns * nc, 0.0);  // Y = T X
-  for (int j = 0; j < nc; ++j)
-    for (int k = 0; k < nc; ++k) {
-      const double x = X[k + (size_t)nc * j];
-      if (x == 0.0) continue;
-      for (int i = 0; i < ns; ++i) Y[i + (size_t)ns * j] += T[i + (size_t)ns * k] * x;
-    }
-  for (int j = 0; j < ns; ++j)
-    for (int i = 0; i < ns; ++i) {
-      double acc = 0.0;
-      for (int k = 0; k < nc; ++k) acc += Y[i + (size_t)ns * k] * T[j + (size_t)ns * k];
-      out[i + (size_t)ns * j] = acc;
-    }
+// out (ns x ns) = T X T^T for X (nc x nc) on the host, T = sph_transform(B):
+// T is block diagonal (shell by shell), so each product runs over one shell's
+// Cartesian components only (O(nc * sum_s ns_s nc_s) instead of O(ns nc^2)).
+void transform2(const Basis& B, const std::vector<double>& T, const double* X, double* out) {
+  const int64_t ns = B.nsph, nc = B.ncart;
+  std::vector<double> Y((size_t)ns * nc);  // Y = T X
+  int64_t c0 = 0;
+  for (size_t s = 0; s < B.sh.size(); ++s) {
+    const int64_t l = B.sh[s].l, ncs = ncart((int)l), r0 = B.sph_off[s];
+    for (int64_t j = 0; j < nc; ++j)
+      for (int64_t i = 0; i < 2 * l + 1; ++i) {
+        double acc = 0.0;
+        for (int64_t k = 0; k < ncs; ++k) acc += T[(r0 + i) + ns * (c0 + k)] * X[(c0 + k) + nc * j];
+        Y[(r0 + i) + ns * j] = acc;
+      }
+    c0 += ncs;
+  }
+  c0 = 0;
+  for (size_t s = 0; s < B.sh.size(); ++s) {
+    const int64_t l = B.sh[s].l, ncs = ncart((int)l), r0 = B.sph_off[s];
+    for (int64_t j = 0; j < 2 * l + 1; ++j)
+      for (int64_t i = 0; i < ns; ++i) {
+        double acc = 0.0;
+        for (int64_t k = 0; k < ncs; ++k) acc += Y[i + ns * (c0 + k)] * T[(r0 + j) + ns * (c0 + k)];
+        out[i + ns * (r0 + j)] = acc;
+      }
+    c0 += ncs;
+  }
 }
 
 // Device copies of shells and primitives (released by the caller's scope).
@@ -189,7 +202,7 @@ void one_electron(Ctx& c, const Basis& B, int kind, int natom, const double* Z,
   const std::vector<double> T = sph_transform(B);
   out.assign(ncomp * ns * ns, 0.0);
   for (int q = 0; q < ncomp; ++q)
-    transform2(T, (int)ns, (int)nc, cart.data() + q * nc * nc, out.data() + q * ns * ns);
+    transform2(B, T, cart.data() + q * nc * nc, out.data() + q * ns * ns);
 }
 
 // 1 / sqrt of the spherical self-overlaps
@@ -216,7 +229,65 @@ void check_ltot(const Basis& a, const Basis* b, const Basis& c) {
                              "l above " + std::to_string(dev::INT_LTOT) + ")");
 }
 
+// (mn|P) of ao x ao x fit on the device, spherical and normalised, as
+// Z[m + nao*(n + nao*P)] in an allocation of c's stack (with the
+// intermediates below it: the caller's scope releases them all).
+double* int3c2e_device(Ctx& c, const ecg_shells* ao, const ecg_shells* fit, int64_t* nao,
+                       int64_t* naux) {
+  const Basis A = make_basis(ao, 0, 0);
+  // P0: the fitting basis on its own (normalisation, transform); P: the same
+  // shells with primitive offsets past A's, for the kernel's joint arrays
+  const Basis P0 = make_basis(fit, 0, 0);
+  const Basis P = make_basis(fit, (int)A.ex.size(), 0);
+  check_ltot(A, &A, P);
+  const std::vector<double> dA = norms(c, A), dP = norms(c, P0);
+  std::vector<double> TA = sph_transform(A), TP = sph_transform(P0);
+  for (int64_t k = 0; k < A.ncart; ++k)
+    for (int64_t i = 0; i < A.nsph; ++i) TA[i + A.nsph * k] *= dA[i];
+  for (int64_t k = 0; k < P.ncart; ++k)
+    for (int64_t i = 0; i < P.nsph; ++i) TP[i + P.nsph * k] *= dP[i];
+  const int64_t na = A.ncart, np = P.ncart, sa = A.nsph, sp = P.nsph;
+  std::vector<double> ex(A.ex), co(A.co);
+  ex.insert(ex.end(), P.ex.begin(), P.ex.end());
+  co.insert(co.end(), P.co.begin(), P.co.end());
+  DevBasis dao = upload(c, A.sh, ex, co);
+  DevBasis daux = upload(c, P.sh, {}, {});
+  double* X = c.alloc(na * na * np, "int3c cart");
+  check(dev::memset0(X, na * na * np * 8, c.st), "memset");
+  check(dev::int3c2e_cart(c.st, dao.sh, (int)A.sh.size(), daux.sh, (int)P.sh.size(), dao.ex,
+                          dao.co, na, X),
+        "int3c2e");
+  double* dTA = c.alloc(sa * na, "TA");
+  double* dTP = c.alloc(sp * np, "TP");
+  check(dev::h2d(dTA, TA.data(), TA.size() * 8, c.st), "h2d");
+  check(dev::h2d(dTP, TP.data(), TP.size() * 8, c.st), "h2d");
+  // Y1[m,n,P] = sum_Pc X[m,n,Pc] TP[P,Pc]
+  double* Y1 = c.alloc(na * na * sp, "int3c 1");
+  check(dev::gemm(c.st, 'N', 'T', na * na, sp, np, 1.0, X, na * na, dTP, sp, 0.0, Y1, na * na),
+        "gemm P");
+  // Y2[m,n',P] = sum_n Y1[m,n,P] TA[n',n]  (batched over P)
+  double* Y2 = c.alloc(na * sa * sp, "int3c 2");
+  check(dev::gemm(c.st, 'N', 'T', na, sa, na, 1.0, Y1, na, dTA, sa, 0.0, Y2, na, sp, na * na, 0,
+                  na * sa),
+        "gemm n");
+  // Z[m',n',P] = sum_m TA[m',m] Y2[m,n',P]
+  double* Z = c.alloc(sa * sa * sp, "int3c 3");
+  check(dev::gemm(c.st, 'N', 'N', sa, sa * sp, na, 1.0, dTA, sa, Y2, na, 0.0, Z, sa), "gemm m");
+  *nao = sa;
+  *naux = sp;
+  return Z;
+}
+
+
 }  // namespace
+
+// Density-fitted three-index factors held on the device between calls.
+struct ecg_df {
+  ecg_ctx* ctx = nullptr;
+  double* aal = nullptr;  // AAL[m + n*(m' + n*L)], n = nao
+  size_t bytes = 0;
+  int64_t n = 0, nL = 0;
+};
 
 extern "C" {
 
@@ -279,11 +350,12 @@ int ecg_int2c2e(ecg_ctx* ctx, const ecg_shells* fit, double* out) {
     }
     const std::vector<double> T = sph_transform(P);
     const std::vector<double> d = norms(*c, P);
-    transform2(T, (int)ns, (int)nc, cart.data(), out);
+    transform2(P, T, cart.data(), out);
     for (int64_t j = 0; j < ns; ++j)
       for (int64_t i = 0; i < ns; ++i) out[i + ns * j] *= d[i] * d[j];
   });
 }
+
 
 int ecg_int3c2e(ecg_ctx* ctx, const ecg_shells* ao, const ecg_shells* fit, double* out) {
   Ctx* c = ctx;
@@ -291,49 +363,135 @@ int ecg_int3c2e(ecg_ctx* ctx, const ecg_shells* ao, const ecg_shells* fit, doubl
   return guarded(c, [&] {
     if (!out) throw Error(ECG_ERR_ARG, "NULL output");
     check(dev::set_device(c->device), "cudaSetDevice");
-    const Basis A = make_basis(ao, 0, 0);
-    // P0: the fitting basis on its own (normalisation, transform); P: the same
-    // shells with primitive offsets past A's, for the kernel's joint arrays
-    const Basis P0 = make_basis(fit, 0, 0);
-    const Basis P = make_basis(fit, (int)A.ex.size(), 0);
-    check_ltot(A, &A, P);
-    const std::vector<double> dA = norms(*c, A), dP = norms(*c, P0);
-    std::vector<double> TA = sph_transform(A), TP = sph_transform(P0);
-    for (int64_t k = 0; k < A.ncart; ++k)
-      for (int64_t i = 0; i < A.nsph; ++i) TA[i + A.nsph * k] *= dA[i];
-    for (int64_t k = 0; k < P.ncart; ++k)
-      for (int64_t i = 0; i < P.nsph; ++i) TP[i + P.nsph * k] *= dP[i];
-    const int64_t na = A.ncart, np = P.ncart, sa = A.nsph, sp = P.nsph;
     Scope scope{*c, c->allocs.size()};
-    std::vector<double> ex(A.ex), co(A.co);
-    ex.insert(ex.end(), P.ex.begin(), P.ex.end());
-    co.insert(co.end(), P.co.begin(), P.co.end());
-    DevBasis dao = upload(*c, A.sh, ex, co);
-    DevBasis daux = upload(*c, P.sh, {}, {});
-    double* X = c->alloc(na * na * np, "int3c cart");
-    check(dev::memset0(X, na * na * np * 8, c->st), "memset");
-    check(dev::int3c2e_cart(c->st, dao.sh, (int)A.sh.size(), daux.sh, (int)P.sh.size(), dao.ex,
-                            dao.co, na, X),
-          "int3c2e");
-    double* dTA = c->alloc(sa * na, "TA");
-    double* dTP = c->alloc(sp * np, "TP");
-    check(dev::h2d(dTA, TA.data(), TA.size() * 8, c->st), "h2d");
-    check(dev::h2d(dTP, TP.data(), TP.size() * 8, c->st), "h2d");
-    // Y1[m,n,P] = sum_Pc X[m,n,Pc] TP[P,Pc]
-    double* Y1 = c->alloc(na * na * sp, "int3c 1");
-    check(dev::gemm(c->st, 'N', 'T', na * na, sp, np, 1.0, X, na * na, dTP, sp, 0.0, Y1, na * na),
-          "gemm P");
-    // Y2[m,n',P] = sum_n Y1[m,n,P] TA[n',n]  (batched over P)
-    double* Y2 = c->alloc(na * sa * sp, "int3c 2");
-    check(dev::gemm(c->st, 'N', 'T', na, sa, na, 1.0, Y1, na, dTA, sa, 0.0, Y2, na, sp, na * na,
-                    0, na * sa),
-          "gemm n");
-    // Z[m',n',P] = sum_m TA[m',m] Y2[m,n',P]
-    double* Z = c->alloc(sa * sa * sp, "int3c 3");
-    check(dev::gemm(c->st, 'N', 'N', sa, sa * sp, na, 1.0, dTA, sa, Y2, na, 0.0, Z, sa), "gemm m");
-    check(dev::d2h(out, Z, sa * sa * sp * 8, c->st), "d2h");
+    int64_t n = 0, naux = 0;
+    const double* Z = int3c2e_device(*c, ao, fit, &n, &naux);
+    check(dev::d2h(out, Z, n * n * naux * 8, c->st), "d2h");
     check(dev::sync(c->st), "sync");
   });
+}
+
+int ecg_df_create(ecg_ctx* ctx, const ecg_shells* ao, const ecg_shells* fit, const double* M,
+                  int64_t nL, ecg_df** out) {
+  Ctx* c = ctx;
+  if (!c || !out) return ECG_ERR_ARG;
+  *out = nullptr;
+  ecg_df* d = new (std::nothrow) ecg_df();
+  if (!d) return ECG_ERR_OOM;
+  d->ctx = ctx;
+  const int st = guarded(c, [&] {
+    if (!M) throw Error(ECG_ERR_ARG, "NULL fitting matrix");
+    if (nL <= 0) throw Error(ECG_ERR_ARG, "nL must be positive");
+    int32_t nao = 0, naux = 0;
+    if (ecg_shells_nbf(ao, &nao) != ECG_OK || ecg_shells_nbf(fit, &naux) != ECG_OK)
+      throw Error(ECG_ERR_ARG, "invalid basis");
+    if (nL > naux) throw Error(ECG_ERR_ARG, "nL exceeds the fitting basis");
+    check(dev::set_device(c->device), "cudaSetDevice");
+    d->n = nao;
+    d->nL = nL;
+    d->bytes = (size_t)std::max<int64_t>((int64_t)nao * nao * nL, 1) * 8;
+    if (c->memcap && c->memused + d->bytes > c->memcap)
+      throw Error(ECG_ERR_OOM, "device memory cap exceeded allocating the DF factors");
+    d->aal = (double*)dev::dmalloc(d->bytes);
+    if (!d->aal) throw Error(ECG_ERR_OOM, "cudaMalloc failed for the DF factors");
+    c->memused += d->bytes;
+    Scope scope{*c, c->allocs.size()};
+    int64_t n = 0, np = 0;
+    const double* Z = int3c2e_device(*c, ao, fit, &n, &np);
+    double* dM = c->alloc(np * nL, "fitting matrix");
+    check(dev::h2d(dM, M, np * nL * 8, c->st), "h2d");
+    // AAL[mn, L] = sum_P (mn|P) M[P, L]
+    check(dev::gemm(c->st, 'N', 'N', n * n, nL, np, 1.0, Z, n * n, dM, np, 0.0, d->aal, n * n),
+          "gemm AAL");
+    check(dev::sync(c->st), "sync");
+  });
+  if (st != ECG_OK) {
+    ecg_df_destroy(d);
+    return st;
+  }
+  *out = d;
+  return ECG_OK;
+}
+
+int ecg_df_fock(ecg_df* d, const double* h, const double* Cocc, int64_t nocc, double* F) {
+  if (!d) return ECG_ERR_ARG;
+  Ctx* c = d->ctx;
+  return guarded(c, [&] {
+    if (!h || !F || (nocc > 0 && !Cocc)) throw Error(ECG_ERR_ARG, "NULL argument");
+    if (nocc < 0 || nocc > d->n) throw Error(ECG_ERR_ARG, "nocc out of range");
+    check(dev::set_device(c->device), "cudaSetDevice");
+    const int64_t n = d->n, nL = d->nL;
+    Scope scope{*c, c->allocs.size()};
+    double* dF = c->alloc(n * n, "Fock");
+    check(dev::h2d(dF, h, n * n * 8, c->st), "h2d");
+    if (nocc > 0) {
+      double* dC = c->alloc(n * nocc, "occupied orbitals");
+      double* Ct = c->alloc(n * nocc, "occupied orbitals^T");
+      double* Y = c->alloc(nocc * n * nL, "LoA");
+      double* Yp = c->alloc(nocc * n * nL, "LoA permuted");
+      double* cL = c->alloc(nL, "cL");
+      check(dev::h2d(dC, Cocc, n * nocc * 8, c->st), "h2d");
+      // Y[j, nu, L] = sum_mu C[mu, j] AAL[mu, nu, L]
+      check(dev::gemm(c->st, 'T', 'N', nocc, n * nL, n, 1.0, dC, n, d->aal, n, 0.0, Y, nocc),
+            "gemm LoA");
+      // cL[L] = sum_{j, nu} Y[j, nu, L] C[nu, j]
+      const int64_t d2[2] = {n, nocc};
+      const int p2[2] = {1, 0};
+      check(dev::permute(c->st, 2, d2, p2, 1.0, dC, 0.0, Ct), "permute C");
+      check(dev::gemm(c->st, 'T', 'N', nL, 1, nocc * n, 1.0, Y, nocc * n, Ct, nocc * n, 0.0, cL,
+                      nL),
+            "gemm cL");
+      // F += 2 sum_L AAL[mu, nu, L] cL[L]
+      check(dev::gemm(c->st, 'N', 'N', n * n, 1, nL, 2.0, d->aal, n * n, cL, nL, 1.0, dF, n * n),
+            "gemm J");
+      // F -= sum_{L, j} Y[j, mu, L] Y[j, nu, L], over Yp[j, L, nu]
+      const int64_t d3[3] = {nocc, n, nL};
+      const int p3[3] = {0, 2, 1};
+      check(dev::permute(c->st, 3, d3, p3, 1.0, Y, 0.0, Yp), "permute LoA");
+      check(dev::gemm(c->st, 'T', 'N', n, n, nocc * nL, -1.0, Yp, nocc * nL, Yp, nocc * nL, 1.0,
+                      dF, n),
+            "gemm K");
+    }
+    check(dev::d2h(F, dF, n * n * 8, c->st), "d2h");
+    check(dev::sync(c->st), "sync");
+  });
+}
+
+int ecg_df_mo(ecg_df* d, const double* C, int64_t nmo, double* B) {
+  if (!d) return ECG_ERR_ARG;
+  Ctx* c = d->ctx;
+  return guarded(c, [&] {
+    if (!C || !B) throw Error(ECG_ERR_ARG, "NULL argument");
+    if (nmo <= 0) throw Error(ECG_ERR_ARG, "nmo must be positive");
+    check(dev::set_device(c->device), "cudaSetDevice");
+    const int64_t n = d->n, nL = d->nL;
+    Scope scope{*c, c->allocs.size()};
+    double* dC = c->alloc(n * nmo, "orbitals");
+    double* T1 = c->alloc(nmo * n * nL, "mAL");
+    double* dB = c->alloc(nmo * nmo * nL, "mmL");
+    check(dev::h2d(dC, C, n * nmo * 8, c->st), "h2d");
+    // T1[p, nu, L] = sum_mu C[mu, p] AAL[mu, nu, L]
+    check(dev::gemm(c->st, 'T', 'N', nmo, n * nL, n, 1.0, dC, n, d->aal, n, 0.0, T1, nmo),
+          "gemm mAL");
+    // B[p, q, L] = sum_nu T1[p, nu, L] C[nu, q], batched over L
+    check(dev::gemm(c->st, 'N', 'N', nmo, nmo, n, 1.0, T1, nmo, dC, n, 0.0, dB, nmo, nL, nmo * n,
+                    0, nmo * nmo),
+          "gemm mmL");
+    check(dev::d2h(B, dB, nmo * nmo * nL * 8, c->st), "d2h");
+    check(dev::sync(c->st), "sync");
+  });
+}
+
+int ecg_df_destroy(ecg_df* d) {
+  if (!d) return ECG_OK;
+  if (d->aal) {
+    Ctx* c = d->ctx;
+    if (c->st) dev::sync(c->st);
+    dev::dfree(d->aal);
+    c->memused -= d->bytes;
+  }
+  delete d;
+  return ECG_OK;
 }
 
 }  // extern "C"

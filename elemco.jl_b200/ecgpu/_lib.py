@@ -108,6 +108,10 @@ SIGNATURES = {
     "ecg_int1e": (C.c_int, [_P, C.c_int32, _S, C.c_int32, _D, _D, _D, _D]),
     "ecg_int2c2e": (C.c_int, [_P, _S, _D]),
     "ecg_int3c2e": (C.c_int, [_P, _S, _S, _D]),
+    "ecg_df_create": (C.c_int, [_P, _S, _S, _D, C.c_int64, C.POINTER(_P)]),
+    "ecg_df_fock": (C.c_int, [_P, _D, _D, C.c_int64, _D]),
+    "ecg_df_mo": (C.c_int, [_P, _D, C.c_int64, _D]),
+    "ecg_df_destroy": (C.c_int, [_P]),
     "ecg_gemm_noalloc": (C.c_int, [C.c_char, C.c_char, C.c_int64, C.c_int64, C.c_int64,
                                    C.c_double, _P, C.c_int64, _P, C.c_int64, C.c_double, _P,
                                    C.c_int64, _P, C.POINTER(C.c_int32)]),

@@ -4,6 +4,7 @@ Arrays are numpy float64 in the reference's index order and Fortran (column-
 major) layout, exactly what the Julia ``ccall`` glue passes.
 """
 import ctypes as C
+import weakref
 
 import numpy as np
 
@@ -20,10 +21,13 @@ class Context:
         if st:
             raise ECGError(st, self._L.ecg_last_error(None).decode())
         self._h = h
+        self._handles = weakref.WeakSet()  # device handles to release before the context
         self.no = self.nv = self.nq = 0
 
     def close(self):
         if getattr(self, "_h", None):
+            for obj in list(self._handles):
+                obj.close()
             self._L.ecg_destroy(self._h)
             self._h = None
 
@@ -252,6 +256,10 @@ class Context:
         self._chk(self._L.ecg_int3c2e(self._h, C.byref(sa), C.byref(sf), dptr(out)))
         return out
 
+    def df_factors(self, ao, fit, M):
+        """:class:`DFFactors` AAL[m,n,L] = sum_P (mn|P) M[P,L] held on the device."""
+        return DFFactors(self, ao, fit, M)
+
     def diag_gemm(self, ta, tb, alpha, A, B, beta, Cm):
         A, B = as_f(A), as_f(B)
         Cm = as_f(Cm).copy(order="F")
@@ -292,3 +300,61 @@ class Diis:
         if self._h:
             self._ctx._L.ecg_diis_destroy(self._h)
             self._h = None
+
+
+class DFFactors:
+    """Density-fitted three-index factors on the device (``ecg_df_*``):
+    AAL[m,n,L] = sum_P (mn|P) M[P,L] for an AO basis and a fitting basis
+    (:class:`ecgpu.basis.ShellArrays`), M (naux x nL) with M M^T = (P|Q)^-1."""
+
+    def __init__(self, ctx, ao, fit, M):
+        M = as_f(M)
+        if M.shape[0] != fit.nbf:
+            raise ValueError("M must have one row per fitting function")
+        h = C.c_void_p()
+        sa, sf = ao.struct(), fit.struct()
+        ctx._chk(ctx._L.ecg_df_create(ctx._h, C.byref(sa), C.byref(sf), dptr(M), M.shape[1],
+                                      C.byref(h)))
+        self._ctx, self._h = ctx, h
+        self.nao, self.nL = ao.nbf, M.shape[1]
+        ctx._handles.add(self)
+
+    def _handle(self):
+        if not self._h:
+            raise ValueError("DF factors already released")
+        return self._h
+
+    def fock(self, h, Cocc):
+        """F = h + 2 J - K (closed shell) from the occupied orbitals Cocc (n x nocc)."""
+        n = self.nao
+        h = as_f(h)
+        Cocc = as_f(np.reshape(Cocc, (n, -1)))
+        F = fvec((n, n))
+        self._ctx._chk(self._ctx._L.ecg_df_fock(self._handle(), dptr(h), dptr(Cocc),
+                                                Cocc.shape[1], dptr(F)))
+        return F
+
+    def mo(self, Cmo):
+        """B[p,q,L] = sum_{m,n} C[m,p] AAL[m,n,L] C[n,q], F-ordered (nmo, nmo, nL)."""
+        Cmo = as_f(Cmo)
+        nmo = Cmo.shape[1]
+        B = fvec((nmo, nmo, self.nL))
+        self._ctx._chk(self._ctx._L.ecg_df_mo(self._handle(), dptr(Cmo), nmo, dptr(B)))
+        return B
+
+    def close(self):
+        if self._h:
+            self._ctx._L.ecg_df_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

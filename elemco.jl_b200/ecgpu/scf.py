@@ -20,8 +20,11 @@
   ``int0 = E_nuc + sum_occ h_ii + sum_core F_ii - sum_active-occ int1_ii``.
 
 The Gaussian integrals (overlap, kinetic, nuclear attraction, (P|Q), (mn|P))
-come from libecgpu's GPU integral engine.  The fitting metric's inverse
-square root is the pivoted Cholesky of ``sqrtinvchol``
+come from libecgpu's GPU integral engine.  The fitted factors
+AAL[m,n,L] = sum_P (mn|P) M[P,L] stay on the device (``ecg_df_*``), where the
+Fock builds and the MO transform run; the host keeps the n x n matrices
+(the generalized eigenproblem, DIIS on the Fock matrix).  The fitting
+metric's inverse square root is the pivoted Cholesky of ``sqrtinvchol``
 (src/tools/tensortools.jl:377-389, tolerance ``cholesky.thred`` 1e-6).
 """
 import math
@@ -79,12 +82,12 @@ class AOIntegrals:
         self.enuc = mol.nuclear_repulsion()
 
     def fitted(self, fit, thred=1e-6):
-        """AAL[m, n, L] = sum_P (mn|P) M[P, L] with M M^T = (P|Q)^{-1}."""
+        """Device factors (:class:`ecgpu.context.DFFactors`)
+        AAL[m, n, L] = sum_P (mn|P) M[P, L] with M M^T = (P|Q)^{-1}
+        (generate_AO_DF_integrals, src/integrals/dftools.jl:28-84)."""
         fb = Bm.shells(Bm.load(fit, self.library), self.mol.symbols, self.mol.xyz)
         M = sqrtinvchol(self.ctx.int2c2e(fb), thred)
-        B3 = self.ctx.int3c2e(self.ao, fb)
-        n = self.ao.nbf
-        return (B3.reshape(n * n, -1, order="F") @ M).reshape(n, n, -1, order="F")
+        return self.ctx.df_factors(self.ao, fb, M)
 
     def dipole(self, origin=(0.0, 0.0, 0.0)):
         return self.ctx.int1e(ECG_INT_DIPOLE, self.ao, origin=origin)
@@ -92,14 +95,8 @@ class AOIntegrals:
 
 def df_fock(h, AAL, Cocc):
     """gen_dffock closed shell (src/scf/fockfactory.jl:202-245):
-    F = h + 2 J - K with DF factors AAL[m, n, L]."""
-    n, nL = AAL.shape[0], AAL.shape[2]
-    LoA = np.einsum("mnL,mj->Ljn", AAL, Cocc, optimize=True)   # [L, j, n]
-    cL = np.einsum("Ljn,nj->L", LoA, Cocc, optimize=True)
-    X = LoA.reshape(-1, n)
-    F = h - X.T @ X
-    F += 2.0 * (AAL.reshape(n * n, nL, order="F") @ cL).reshape(n, n, order="F")
-    return F
+    F = h + 2 J - K with the device DF factors AAL (ecg_df_fock)."""
+    return AAL.fock(h, Cocc)
 
 
 class _Diis:
@@ -174,6 +171,7 @@ def _atomic_density(ctx, sym, ao, jkfit, thred, library, maxit=100):
         SDF = ints.S @ D @ F
         F = diis.perform(F, SDF - SDF.T)
         eps, C = _geneig(F, ints.S)
+    AAL.close()
     return D
 
 
@@ -262,18 +260,18 @@ def dfints(hf, mpfit="cc-pvdz-mpfit", jkfit="cc-pvtz-jkfit", ncore=None, thred=1
     nc = mol.ncore() if ncore is None else int(ncore)
     act = C[:, nc:]
     n = act.shape[1]
-    # mpfit factors of the active orbitals
+    # mpfit factors of the active orbitals (generate_3idx_integrals,
+    # src/integrals/dftools.jl:92-136), on the device
     AAL = ints.fitted(mpfit, thred)
-    nao, nL = AAL.shape[0], AAL.shape[2]
-    tmp = (act.T @ AAL.reshape(nao, nao * nL, order="F")).reshape(n, nao, nL, order="F")
-    B = np.einsum("pnL,nq->pqL", tmp, act, optimize=True)
-    B = np.asfortranarray(B)
-    # Fock matrix of the active space from the mpfit integrals
-    no = nocc - nc
-    o = slice(0, no)
-    J = np.einsum("pqL,iiL->pq", B, B[o, o, :], optimize=True)
-    K = np.einsum("piL,iqL->pq", B[:, o, :], B[o, :, :], optimize=True)
-    f_mp = 2.0 * J - K
+    try:
+        B = AAL.mo(act)
+        # Fock matrix of the active space from the mpfit integrals,
+        # 2 J - K over the active occupied orbitals, in the AO basis on the
+        # device, then transformed
+        no = nocc - nc
+        f_mp = act.T @ AAL.fock(np.zeros_like(ints.h), act[:, :no]) @ act
+    finally:
+        AAL.close()
     # jkfit DF-HF Fock matrix of the orbitals (all occupied, core included)
     Fjk = C.T @ df_fock(ints.h, hf.AAL, C[:, :nocc]) @ C
     int1 = Fjk[nc:, nc:] - f_mp

@@ -279,6 +279,30 @@ int ecg_int2c2e(ecg_ctx* ctx, const ecg_shells* fit, double* out);
  * eri_2e3idx (src/system/integrals_2e3idx.jl:108-158, libcint int3c2e). */
 int ecg_int3c2e(ecg_ctx* ctx, const ecg_shells* ao, const ecg_shells* fit, double* out);
 
+/* Density-fitted three-index factors kept on the device between calls:
+ * AAL[m,n,L] = sum_P (mn|P) M[P,L], M (naux x nL, column-major) with
+ * M M^T = (P|Q)^{-1} on the span kept (the caller's pivoted Cholesky of
+ * ecg_int2c2e).  The reference's generate_AO_DF_integrals
+ * (src/integrals/dftools.jl:28-84), which the reference writes to a file
+ * `AAL`; here the factors stay in HBM (n^2 nL doubles, counted against the
+ * context's memory cap) for the Fock builds of DF-HF and the MO transform.
+ * The handle belongs to its context: destroy it before the context. */
+typedef struct ecg_df ecg_df;
+int ecg_df_create(ecg_ctx* ctx, const ecg_shells* ao, const ecg_shells* fit, const double* M,
+                  int64_t nL, ecg_df** out);
+/* Closed-shell DF Fock matrix in the AO basis, F = h + 2 J - K
+ * (n x n, column-major) from the occupied orbitals Cocc (n x nocc):
+ * LoA[L,j,n] = sum_m AAL[m,n,L] C[m,j], J = AAL . (sum LoA[L,j,n] C[n,j]),
+ * K[m,n] = sum_{L,j} LoA[L,j,m] LoA[L,j,n] — the reference's gen_dffock
+ * (src/scf/fockfactory.jl:202-245), which recomputes (mn|P) in batches for
+ * every build.  nocc = 0 returns h. */
+int ecg_df_fock(ecg_df* df, const double* h, const double* Cocc, int64_t nocc, double* F);
+/* MO three-index factors B[p,q,L] = sum_{m,n} C[m,p] AAL[m,n,L] C[n,q]
+ * (nmo x nmo x nL, column-major) of the orbitals C (n x nmo): the reference's
+ * generate_3idx_integrals (src/integrals/dftools.jl:92-136, file `mmL`). */
+int ecg_df_mo(ecg_df* df, const double* C, int64_t nmo, double* B);
+int ecg_df_destroy(ecg_df* df);
+
 /* ------------------------------------------------------------------------
  * Allocation-free entry point (no counterpart in the reference).
  *

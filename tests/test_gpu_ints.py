@@ -86,6 +86,50 @@ def test_water_cc_pvdz_shapes(ictx):
     assert np.abs(B[:n, :n, :1] - Bo).max() < 1e-11
 
 
+def test_df_factors_fock_and_mo_match_oracle(ictx):
+    """Device DF factors (ecg_df_create) against the numpy restatement
+    (oracle/dfhf.py) on the engine's own (mn|P): the closed-shell Fock build
+    F = h + 2J - K (gen_dffock) and the MO transform (generate_3idx_integrals)
+    to 1e-12 relative, with a rank-reduced M (nL < naux); nocc = 0 gives h."""
+    from oracle import dfhf as O
+    ao, _ = _shells([(0, 3), (1, 2), (2, 1), (0, 1), (1, 1), (3, 1)], 4)
+    fit, _ = _shells([(0, 1), (1, 1), (2, 1), (3, 1), (0, 2), (1, 1), (2, 1)], 5)
+    rng = np.random.default_rng(6)
+    n, naux = ao.nbf, fit.nbf
+    M = rng.standard_normal((naux, naux - 3))
+    AALo = O.df_factors(ictx.int3c2e(ao, fit), M)
+    h = rng.standard_normal((n, n))
+    h = h + h.T
+    Cocc = rng.standard_normal((n, 5))
+    C = rng.standard_normal((n, n - 2))
+    with ictx.df_factors(ao, fit, M) as df:
+        F = df.fock(h, Cocc)
+        Fo = O.df_fock(h, AALo, Cocc)
+        assert np.abs(F - Fo).max() < 1e-12 * np.abs(Fo).max()
+        assert np.abs(df.fock(h, np.zeros((n, 0))) - h).max() == 0.0
+        B = df.mo(C)
+        Bo = O.df_mo(AALo, C)
+        assert B.shape == (n - 2, n - 2, naux - 3)
+        assert np.abs(B - Bo).max() < 1e-12 * np.abs(Bo).max()
+
+
+def test_df_factors_handle_lifetime():
+    """A DF handle released by its context's close() raises on use; an
+    out-of-range nocc and a wrong M shape are argument errors."""
+    import ecgpu
+    ao, _ = _shells([(0, 2), (1, 1)], 7)
+    fit, _ = _shells([(0, 1), (1, 1), (2, 1)], 8)
+    c = ecgpu.Context(0)
+    df = c.df_factors(ao, fit, np.eye(fit.nbf))
+    with pytest.raises(ecgpu.ECGError):
+        df.fock(np.zeros((ao.nbf, ao.nbf)), np.zeros((ao.nbf, ao.nbf + 1)))
+    with pytest.raises(ValueError):
+        c.df_factors(ao, fit, np.eye(fit.nbf + 1))
+    c.close()
+    with pytest.raises(ValueError):
+        df.mo(np.eye(ao.nbf))
+
+
 def test_df_hf_chain_reproduces_reference_pins(gold):
     """@dfhf with cc-pVDZ / cc-pVTZ-JKFIT on the test/df_hf.jl water, then
     @dfints (frozen O 1s, cc-pVDZ-MPFIT) and ccdriver at the reference's CC
