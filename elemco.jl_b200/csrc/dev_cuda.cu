@@ -562,20 +562,32 @@ static unsigned grid_for(int64_t n, int threads = 256, int64_t cap = 148 * 16);
 // C = alpha sum_z P[z] + beta C, the partials (FP64, or FP32 for the
 // tensor-core GEMM, whose partials are FP32 accumulations) summed in FP64 in
 // slice order.
-template <typename PT>
+// IT: index type of the element loop (32-bit unsigned whenever m * n allows).
+template <typename PT, typename IT>
 __global__ void splitk_reduce_kernel(int64_t m, int64_t n, int S, const PT* __restrict__ P,
                                      double alpha, double beta, double* C, int64_t scm,
                                      int64_t scn) {
   const int64_t total = m * n;
-  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
-       idx += (int64_t)gridDim.x * blockDim.x) {
+  const IT tot = (IT)total, mi = (IT)m;
+  for (IT idx = blockIdx.x * (IT)blockDim.x + threadIdx.x; idx < tot;
+       idx += (IT)gridDim.x * blockDim.x) {
     double acc = 0.0;
-    for (int z = 0; z < S; ++z) acc += (double)P[z * total + idx];
-    double* c = C + (idx % m) * scm + (idx / m) * scn;
+    for (int z = 0; z < S; ++z) acc += (double)P[z * total + (int64_t)idx];
+    double* c = C + (int64_t)(idx % mi) * scm + (int64_t)(idx / mi) * scn;
     double v = alpha * acc;
     if (beta != 0.0) v += beta * *c;
     *c = v;
   }
+}
+
+template <typename PT>
+void launch_reduce(cudaStream_t st, int64_t m, int64_t n, int S, const PT* P, double alpha,
+                   double beta, double* C, int64_t scm, int64_t scn) {
+  const unsigned g = grid_for(m * n);
+  if (m * n < ((int64_t)1 << 32) - 256 * 148 * 16)
+    splitk_reduce_kernel<PT, uint32_t><<<g, 256, 0, st>>>(m, n, S, P, alpha, beta, C, scm, scn);
+  else
+    splitk_reduce_kernel<PT, uint64_t><<<g, 256, 0, st>>>(m, n, S, P, alpha, beta, C, scm, scn);
 }
 
 // ---- split-K GEMM without any allocation --------------------------------
@@ -647,23 +659,20 @@ int gemm_splitk_noalloc(stream_t s, char ta, char tb, int64_t m, int64_t n, int6
   cudaStream_t st = (cudaStream_t)s;
   e = launch_gemm<64, 64, 16, 32, 32, 3, 3>(h, S, st);
   if (e) return e;
-  splitk_reduce_kernel<<<grid_for(m * n), 256, 0, st>>>(m, n, (int)S, P, alpha, beta, C, ldcm,
-                                                        ldcn);
+  launch_reduce(st, m, n, (int)S, P, alpha, beta, C, ldcm, ldcn);
   if (nsplit) *nsplit = (int)S;
   return launched();
 }
 
 int splitk_reduce(stream_t s, int64_t m, int64_t n, int S, const double* P, double alpha,
                   double beta, double* C, int64_t scm, int64_t scn) {
-  splitk_reduce_kernel<<<grid_for(m * n), 256, 0, (cudaStream_t)s>>>(m, n, S, P, alpha, beta, C,
-                                                                     scm, scn);
+  launch_reduce((cudaStream_t)s, m, n, S, P, alpha, beta, C, scm, scn);
   return launched();
 }
 
 int splitk_reduce_f32(stream_t s, int64_t m, int64_t n, int S, const float* P, double alpha,
                       double beta, double* C, int64_t scm, int64_t scn) {
-  splitk_reduce_kernel<<<grid_for(m * n), 256, 0, (cudaStream_t)s>>>(m, n, S, P, alpha, beta, C,
-                                                                     scm, scn);
+  launch_reduce((cudaStream_t)s, m, n, S, P, alpha, beta, C, scm, scn);
   return launched();
 }
 
@@ -978,9 +987,7 @@ static int launch_plain(stream_t s, const GemmArgs& g, const Gemm& q, PlainChoic
     h.beta = 0.0;
     int e = launch_gemm<64, 64, 16, 32, 32, 3, 3>(h, S, st);
     if (e) return e;
-    int64_t total = q.m * q.n;
-    splitk_reduce_kernel<<<grid_for(total), 256, 0, st>>>(q.m, q.n, (int)S, P, q.alpha, q.beta,
-                                                          q.C, q.scm, q.scn);
+    launch_reduce(st, q.m, q.n, (int)S, P, q.alpha, q.beta, q.C, q.scm, q.scn);
     return launched();
   }
   switch (c.cfg) {
@@ -1063,17 +1070,26 @@ struct PermArgs {
   double* out;
 };
 
+// Index arithmetic of the permutation kernels runs in IT (32-bit unsigned
+// whenever the element count allows it: a 64-bit division by a run-time value
+// costs several times the instructions of a 32-bit one, and at a few divisions
+// per element it, not memory, bounded these kernels); offsets stay 64-bit.
+
 // Plain elementwise permutation (out-fastest index also drives the input
 // fastest or the tensor is small): one thread per output element.
+template <typename IT>
 __global__ void permute_plain_kernel(PermArgs p) {
-  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < p.total;
-       idx += (int64_t)gridDim.x * blockDim.x) {
-    int64_t r = idx, off = 0;
+  const IT total = (IT)p.total;
+  for (IT idx = blockIdx.x * (IT)blockDim.x + threadIdx.x; idx < total;
+       idx += (IT)gridDim.x * blockDim.x) {
+    IT r = idx;
+    int64_t off = 0;
 #pragma unroll 8
     for (int d = 0; d < p.nd; ++d) {
-      int64_t x = r % p.odim[d];
-      r /= p.odim[d];
-      off += x * p.istr[d];
+      const IT od = (IT)p.odim[d];
+      const IT x = r % od;
+      r /= od;
+      off += (int64_t)x * p.istr[d];
     }
     double v = p.alpha * p.in[off];
     if (p.beta != 0.0) v += p.beta * p.out[idx];
@@ -1081,25 +1097,56 @@ __global__ void permute_plain_kernel(PermArgs p) {
   }
 }
 
+// Permutation that keeps the fastest index (out dim 0 = in dim 0, stride 1 on
+// both sides): one warp per row of out dim 0, the row's offsets computed once
+// and its elements copied with coalesced loads and stores.
+template <typename IT>
+__global__ void permute_rows_kernel(PermArgs p) {
+  const IT rows = (IT)(p.total / p.odim[0]);
+  const int64_t n0 = p.odim[0];
+  const int lane = threadIdx.x & 31;
+  const IT nwarp = (IT)gridDim.x * (blockDim.x >> 5);
+  for (IT row = blockIdx.x * (IT)(blockDim.x >> 5) + (threadIdx.x >> 5); row < rows;
+       row += nwarp) {
+    IT r = row;
+    int64_t ioff = 0;
+    for (int d = 1; d < p.nd; ++d) {
+      const IT od = (IT)p.odim[d];
+      const IT x = r % od;
+      r /= od;
+      ioff += (int64_t)x * p.istr[d];
+    }
+    const double* in = p.in + ioff;
+    double* out = p.out + (int64_t)row * n0;
+    for (int64_t x = lane; x < n0; x += 32) {
+      double v = p.alpha * in[x];
+      if (p.beta != 0.0) v += p.beta * out[x];
+      out[x] = v;
+    }
+  }
+}
+
 // Tiled permutation: 32x32 tiles spanning out dim 0 (written contiguously)
 // and out dim q (read contiguously); all other dims enumerate tiles.
-__global__ void permute_tiled_kernel(PermArgs p, int64_t tiles0, int64_t tilesq, int64_t rest) {
+template <typename IT>
+__global__ void permute_tiled_kernel(PermArgs p, IT tiles0, IT tilesq, IT rest) {
   __shared__ double tile[32][33];
-  const int64_t ntile = tiles0 * tilesq * rest;
+  const IT ntile = tiles0 * tilesq * rest;
   const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
-  for (int64_t t = blockIdx.x; t < ntile; t += gridDim.x) {
-    int64_t t0 = t % tiles0;
-    int64_t tq = (t / tiles0) % tilesq;
-    int64_t r = t / (tiles0 * tilesq);
+  for (IT t = blockIdx.x; t < ntile; t += gridDim.x) {
+    const IT t0 = t % tiles0;
+    const IT tq = (t / tiles0) % tilesq;
+    IT r = t / (tiles0 * tilesq);
     int64_t ibase = 0, obase = 0;
     for (int d = 1; d < p.nd; ++d) {
       if (d == p.q) continue;
-      int64_t x = r % p.odim[d];
-      r /= p.odim[d];
-      ibase += x * p.istr[d];
-      obase += x * p.ostr[d];
+      const IT od = (IT)p.odim[d];
+      const IT x = r % od;
+      r /= od;
+      ibase += (int64_t)x * p.istr[d];
+      obase += (int64_t)x * p.ostr[d];
     }
-    const int64_t x0b = t0 * 32, xqb = tq * 32;
+    const int64_t x0b = (int64_t)t0 * 32, xqb = (int64_t)tq * 32;
     // read: contiguous along q (input fastest)
     for (int j = ty; j < 32; j += 8) {
       int64_t x0 = x0b + j, xq = xqb + tx;
@@ -1142,16 +1189,34 @@ int permute(stream_t s, int nd, const int64_t* in_dims, const int* perm, double 
   p.in = in;
   p.out = out;
   cudaStream_t st = (cudaStream_t)s;
-  if (p.q == 0 || p.odim[0] < 8 || p.odim[p.q] < 8) {
+  // 32-bit index arithmetic while every index (element, row, tile) fits
+  const bool small = p.total < ((int64_t)1 << 32) - 256 * 148 * 16;
+  if (p.q == 0 && p.odim[0] >= 32) {
+    const int64_t rows = p.total / p.odim[0];
+    int64_t blocks = (rows + 7) / 8;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    if (small)
+      permute_rows_kernel<uint32_t><<<(unsigned)blocks, 256, 0, st>>>(p);
+    else
+      permute_rows_kernel<uint64_t><<<(unsigned)blocks, 256, 0, st>>>(p);
+  } else if (p.q == 0 || p.odim[0] < 8 || p.odim[p.q] < 8) {
     int64_t blocks = (p.total + 255) / 256;
     if (blocks > 148 * 16) blocks = 148 * 16;
-    permute_plain_kernel<<<(unsigned)blocks, 256, 0, st>>>(p);
+    if (small)
+      permute_plain_kernel<uint32_t><<<(unsigned)blocks, 256, 0, st>>>(p);
+    else
+      permute_plain_kernel<uint64_t><<<(unsigned)blocks, 256, 0, st>>>(p);
   } else {
     int64_t t0 = (p.odim[0] + 31) / 32, tq = (p.odim[p.q] + 31) / 32;
     int64_t rest = p.total / (p.odim[0] * p.odim[p.q]);
     int64_t blocks = t0 * tq * rest;
     if (blocks > 148 * 32) blocks = 148 * 32;
-    permute_tiled_kernel<<<(unsigned)blocks, dim3(32, 8), 0, st>>>(p, t0, tq, rest);
+    if (small)
+      permute_tiled_kernel<uint32_t><<<(unsigned)blocks, dim3(32, 8), 0, st>>>(
+          p, (uint32_t)t0, (uint32_t)tq, (uint32_t)rest);
+    else
+      permute_tiled_kernel<uint64_t><<<(unsigned)blocks, dim3(32, 8), 0, st>>>(
+          p, (uint64_t)t0, (uint64_t)tq, (uint64_t)rest);
   }
   return launched();
 }
@@ -1314,17 +1379,38 @@ __global__ void dot_partial_kernel(int64_t n, const double* x, const double* y, 
   if (threadIdx.x == 0) part[blockIdx.x] = r;
 }
 
+// Partial sums of <X|Y> and <X^T|Y> (X^T[a,b,i,j] = X[b,a,i,j]) over 32 x 32
+// tiles of each (a,b) slice: the block reads the tile of X and Y and the
+// mirrored tile of X, all coalesced, and takes the transposed elements from
+// shared memory.  Tiles go to blocks in a fixed order, so the sums are
+// deterministic.
 __global__ void cs_dot_partial_kernel(int nv, int no, const double* X, const double* Y,
                                       double* part) {
   __shared__ double sh[32];
-  const int64_t vv = (int64_t)nv * nv, n = vv * no * no;
+  __shared__ double xt[32][33];
+  const int64_t vv = (int64_t)nv * nv;
+  const uint32_t T = (uint32_t)(nv + 31) / 32, ntile = T * T * (uint32_t)no * (uint32_t)no;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
   double d = 0.0, ex = 0.0;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    int64_t a = i % nv, b = (i / nv) % nv, ij = i / vv;
-    double y = Y[i];
-    d += X[i] * y;
-    ex += X[b + a * nv + ij * vv] * y;
+  for (uint32_t t = blockIdx.x; t < ntile; t += gridDim.x) {
+    const uint32_t ta = t % T, tb = (t / T) % T, ij = t / (T * T);
+    const double* Xs = X + ij * vv;
+    const double* Ys = Y + ij * vv;
+    const int a0 = ta * 32, b0 = tb * 32;
+    // xt[j][tx] = X[b0 + tx, a0 + j]
+    for (int j = ty; j < 32; j += 8)
+      if (b0 + tx < nv && a0 + j < nv) xt[j][tx] = Xs[(b0 + tx) + (int64_t)nv * (a0 + j)];
+    __syncthreads();
+    for (int j = ty; j < 32; j += 8) {
+      const int a = a0 + tx, b = b0 + j;
+      if (a < nv && b < nv) {
+        const int64_t i = a + (int64_t)nv * b;
+        const double y = Ys[i];
+        d += Xs[i] * y;
+        ex += xt[tx][j] * y;  // X[b, a]
+      }
+    }
+    __syncthreads();
   }
   double r0 = block_sum(d, sh);
   double r1 = block_sum(ex, sh);
@@ -1356,6 +1442,9 @@ int dot(stream_t s, int64_t n, const double* x, const double* y, double* scratch
 int cs_dot(stream_t s, int nv, int no, const double* X, const double* Y, double* scratch,
            double* out) {
   cudaStream_t st = (cudaStream_t)s;
+  const uint64_t T = ((uint64_t)nv + 31) / 32;
+  if (T * T * (uint64_t)no * (uint64_t)no >= ((uint64_t)1 << 32) - RED_BLOCKS)
+    return (int)cudaErrorInvalidValue;  // tile index beyond 32 bits
   cs_dot_partial_kernel<<<RED_BLOCKS, 256, 0, st>>>(nv, no, X, Y, scratch);
   int e = launched();
   if (e) return e;
@@ -1453,14 +1542,18 @@ int ladder_pack_t(stream_t s, int nv, int no, const double* T2, const int* cdp, 
   return launched();
 }
 
+// IT: index type of the element loop (32-bit unsigned whenever ncdp * npairs
+// allows: its division by ncdp is the kernel's only per-element division).
+template <typename IT>
 __global__ void ladder_pack_v_kernel(int nv, int a0, int na, int npairs,
                                      const int2* __restrict__ pairs, const int2* __restrict__ cdp,
                                      const double* __restrict__ V, double* __restrict__ Vp,
                                      double* __restrict__ Vm, int64_t ldp, int64_t ldm) {
-  const int64_t v = nv, ncdp = v * (v + 1) / 2, total = ncdp * npairs;
+  const int64_t v = nv;
+  const IT ncdp = (IT)(v * (v + 1) / 2), total = ncdp * (IT)npairs;
   const int64_t lda = v * na;  // Vblk[c + v a' + v na (d + v b'')]
-  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
-       idx += (int64_t)gridDim.x * blockDim.x) {
+  for (IT idx = blockIdx.x * (IT)blockDim.x + threadIdx.x; idx < total;
+       idx += (IT)gridDim.x * blockDim.x) {
     const int64_t k = idx % ncdp, pr = idx / ncdp;
     const int2 cd = cdp[k], ab = pairs[pr];
     const int64_t ap = ab.x - a0, bp = ab.y - a0;
@@ -1475,8 +1568,12 @@ int ladder_pack_v(stream_t s, int nv, int a0, int na, int npairs, const int* pai
                   const int* cdp, const double* Vblk, double* Vp, double* Vm, int64_t ldp,
                   int64_t ldm) {
   int64_t total = (int64_t)nv * (nv + 1) / 2 * npairs;
-  ladder_pack_v_kernel<<<grid_for(total), 256, 0, (cudaStream_t)s>>>(
-      nv, a0, na, npairs, (const int2*)pairs, (const int2*)cdp, Vblk, Vp, Vm, ldp, ldm);
+  if (total < ((int64_t)1 << 32) - 256 * 148 * 16)
+    ladder_pack_v_kernel<uint32_t><<<grid_for(total), 256, 0, (cudaStream_t)s>>>(
+        nv, a0, na, npairs, (const int2*)pairs, (const int2*)cdp, Vblk, Vp, Vm, ldp, ldm);
+  else
+    ladder_pack_v_kernel<uint64_t><<<grid_for(total), 256, 0, (cudaStream_t)s>>>(
+        nv, a0, na, npairs, (const int2*)pairs, (const int2*)cdp, Vblk, Vp, Vm, ldp, ldm);
   return launched();
 }
 

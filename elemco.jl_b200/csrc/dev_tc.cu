@@ -453,10 +453,13 @@ __global__ void split_kernel(const double* __restrict__ src, int64_t R, int64_t 
                              int64_t sk, int64_t Rp, int64_t Kp, int nsl,
                              __nv_bfloat16* __restrict__ dst) {
   __shared__ double tile[32][33];
-  const int64_t tk = (Kp + 31) / 32, tr = (Rp + 31) / 32, ntile = tk * tr;
+  // tile indices in 32 bits (an operand whose BF16 slices fit in device
+  // memory has fewer than 2^25 tiles): one 64-bit division per tile would
+  // cost more instructions than its 1024 elements
+  const uint32_t tk = (uint32_t)((Kp + 31) / 32), ntile = tk * (uint32_t)((Rp + 31) / 32);
   const bool rfast = (sr == 1);
-  for (int64_t t = blockIdx.x; t < ntile; t += gridDim.x) {
-    const int64_t r0 = (t / tk) * 32, k0 = (t % tk) * 32;
+  for (uint32_t t = blockIdx.x; t < ntile; t += gridDim.x) {
+    const int64_t r0 = (int64_t)(t / tk) * 32, k0 = (int64_t)(t % tk) * 32;
     for (int j = threadIdx.y; j < 32; j += 8) {
       int64_t r, k;
       if (rfast) { r = r0 + threadIdx.x; k = k0 + j; } else { r = r0 + j; k = k0 + threadIdx.x; }
@@ -763,7 +766,9 @@ __device__ __forceinline__ void put_slices3(__nv_bfloat16* dst, int64_t sl, int6
 // diagonal) at k, and for a < b and c < d row pr - a' - 1 of the
 // antisymmetric operand gets X[c,d] - X[d,c] at k - d = d(d-1)/2 + c; the K
 // padding of both is written as zeros.
-template <typename VT>
+// IT: index type of the element loop (32-bit unsigned whenever kp_p * npairs
+// allows: its division by kp_p is the kernel's only per-element division).
+template <typename VT, typename IT>
 __global__ void ladder_pack_split_kernel(int nv, int a0, int na, int npairs,
                                          const int2* __restrict__ pairs,
                                          const int2* __restrict__ cdp, const VT* __restrict__ V,
@@ -771,10 +776,11 @@ __global__ void ladder_pack_split_kernel(int nv, int a0, int na, int npairs,
                                          __nv_bfloat16* __restrict__ Vp,
                                          __nv_bfloat16* __restrict__ Vm) {
   const int64_t v = nv, lda = v * na, ncdp = v * (v + 1) / 2, ncdm = v * (v - 1) / 2;
-  const int64_t total = kp_p * npairs, mpad = kp_m - ncdm;
-  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
-       idx += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t k = idx % kp_p, pr = idx / kp_p;
+  const int64_t mpad = kp_m - ncdm;
+  const IT total = (IT)kp_p * (IT)npairs, kpi = (IT)kp_p;
+  for (IT idx = blockIdx.x * (IT)blockDim.x + threadIdx.x; idx < total;
+       idx += (IT)gridDim.x * blockDim.x) {
+    const int64_t k = idx % kpi, pr = idx / kpi;
     const int2 ab = pairs[pr];
     const int64_t ap = ab.x - a0, bp = ab.y - a0;
     const bool minus = ab.x < ab.y;
@@ -807,14 +813,16 @@ int ladder_pack_v_split(stream_t s, int nv, int a0, int na, int npairs, const in
   const int64_t total = kp_p * npairs;
   const unsigned g = (unsigned)std::min<int64_t>((total + 255) / 256, 148 * 16);
   cudaStream_t st = (cudaStream_t)s;
-  if (v_f32)
-    ladder_pack_split_kernel<float><<<g, 256, 0, st>>>(
-        nv, a0, na, npairs, (const int2*)pairs, (const int2*)cdp, (const float*)V, kp_p, sl_p,
-        kp_m, sl_m, (__nv_bfloat16*)Vp, (__nv_bfloat16*)Vm);
-  else
-    ladder_pack_split_kernel<double><<<g, 256, 0, st>>>(
-        nv, a0, na, npairs, (const int2*)pairs, (const int2*)cdp, (const double*)V, kp_p, sl_p,
-        kp_m, sl_m, (__nv_bfloat16*)Vp, (__nv_bfloat16*)Vm);
+  const bool small = total < ((int64_t)1 << 32) - 256 * 148 * 16;
+#define ECG_PACK_SPLIT(VT, IT)                                                                \
+  ladder_pack_split_kernel<VT, IT><<<g, 256, 0, st>>>(                                        \
+      nv, a0, na, npairs, (const int2*)pairs, (const int2*)cdp, (const VT*)V, kp_p, sl_p, kp_m, \
+      sl_m, (__nv_bfloat16*)Vp, (__nv_bfloat16*)Vm)
+  if (v_f32 && small) ECG_PACK_SPLIT(float, uint32_t);
+  else if (v_f32) ECG_PACK_SPLIT(float, uint64_t);
+  else if (small) ECG_PACK_SPLIT(double, uint32_t);
+  else ECG_PACK_SPLIT(double, uint64_t);
+#undef ECG_PACK_SPLIT
   note_launches(1);
   return (int)cudaGetLastError();
 }

@@ -18,7 +18,7 @@ column-major layout is the library's layout.  Status codes other than 0 raise
 module ElemCoGPU
 
 export GPUContext, gpu_calc_cc, gpu_calc_pertT, gpu_calc_lm_cc, set_option!, tune_load!, tune_save,
-       ShellArrays, int1e, int2c2e, int3c2e
+       ShellArrays, int1e, int2c2e, int3c2e, DFFactors, df_fock, df_mo, release!
 
 const libecgpu = get(ENV, "ECGPU_LIB", joinpath(@__DIR__, "..", "ecgpu", "libecgpu.so"))
 
@@ -170,6 +170,65 @@ function int3c2e(ctx::GPUContext, a::ShellArrays, f::ShellArrays)
   GC.@preserve a f out check(ctx, ccall((:ecg_int3c2e, libecgpu), Cint,
       (Ptr{Cvoid}, Ref{CShells}, Ref{CShells}, Ptr{Cdouble}), ctx.ptr, cshells(a), cshells(f), out))
   return out
+end
+
+"""
+    DFFactors(ctx, ao, fit, M)
+
+Density-fitted factors `AAL[m,n,L] = sum_P (mn|P) M[P,L]` kept on the device
+(`ecg_df_create`; generate_AO_DF_integrals, src/integrals/dftools.jl:28-84),
+`M` with `M M' = (P|Q)^-1` (the pivoted Cholesky of `int2c2e`).  Release with
+`release!` before the context.
+"""
+mutable struct DFFactors
+  ptr::Ptr{Cvoid}
+  ctx::GPUContext
+  nao::Int
+  nL::Int
+end
+function DFFactors(ctx::GPUContext, a::ShellArrays, f::ShellArrays, M::Matrix{Float64})
+  @assert size(M, 1) == nbf(f)
+  h = Ref{Ptr{Cvoid}}(C_NULL)
+  GC.@preserve a f M check(ctx, ccall((:ecg_df_create, libecgpu), Cint,
+      (Ptr{Cvoid}, Ref{CShells}, Ref{CShells}, Ptr{Cdouble}, Int64, Ref{Ptr{Cvoid}}),
+      ctx.ptr, cshells(a), cshells(f), M, size(M, 2), h))
+  return DFFactors(h[], ctx, nbf(a), size(M, 2))
+end
+
+"""
+    df_fock(df, h, Cocc)
+
+Closed-shell Fock matrix `h + 2J - K` from the occupied orbitals (`ecg_df_fock`;
+gen_dffock, src/scf/fockfactory.jl:202-245).
+"""
+function df_fock(df::DFFactors, h::Matrix{Float64}, Cocc::Matrix{Float64})
+  F = zeros(df.nao, df.nao)
+  GC.@preserve h Cocc F check(df.ctx, ccall((:ecg_df_fock, libecgpu), Cint,
+      (Ptr{Cvoid}, Ptr{Cdouble}, Ptr{Cdouble}, Int64, Ptr{Cdouble}),
+      df.ptr, h, Cocc, size(Cocc, 2), F))
+  return F
+end
+
+"""
+    df_mo(df, C)
+
+MO three-index factors `B[p,q,L]` (`ecg_df_mo`; generate_3idx_integrals,
+src/integrals/dftools.jl:92-136, the `mmL` file).
+"""
+function df_mo(df::DFFactors, C::Matrix{Float64})
+  nmo = size(C, 2)
+  B = zeros(nmo, nmo, df.nL)
+  GC.@preserve C B check(df.ctx, ccall((:ecg_df_mo, libecgpu), Cint,
+      (Ptr{Cvoid}, Ptr{Cdouble}, Int64, Ptr{Cdouble}), df.ptr, C, nmo, B))
+  return B
+end
+
+function release!(df::DFFactors)
+  if df.ptr != C_NULL
+    ccall((:ecg_df_destroy, libecgpu), Cint, (Ptr{Cvoid},), df.ptr)
+    df.ptr = C_NULL
+  end
+  return nothing
 end
 
 """

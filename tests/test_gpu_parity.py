@@ -37,7 +37,8 @@ def test_gemm_kernel(ctx, ta, tb, m, n, k):
 
 @pytest.mark.parametrize("shape,perm", [((5, 7, 3, 4), (1, 0, 3, 2)), ((40, 33, 9), (2, 0, 1)),
                                         ((64, 64, 8, 8), (0, 3, 1, 2)), ((3, 70, 50), (0, 2, 1)),
-                                        ((100,), (0,))])
+                                        ((100,), (0,)), ((40, 6, 5, 7), (0, 2, 3, 1)),
+                                        ((33, 8, 65), (2, 1, 0))])
 def test_permute_kernel(ctx, shape, perm):
     rng = np.random.default_rng(1)
     x = np.asfortranarray(rng.standard_normal(shape))
