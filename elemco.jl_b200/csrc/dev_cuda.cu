@@ -1147,15 +1147,22 @@ __global__ void permute_tiled_kernel(PermArgs p, IT tiles0, IT tilesq, IT rest) 
       obase += (int64_t)x * p.ostr[d];
     }
     const int64_t x0b = (int64_t)t0 * 32, xqb = (int64_t)tq * 32;
-    // read: contiguous along q (input fastest)
-    for (int j = ty; j < 32; j += 8) {
-      int64_t x0 = x0b + j, xq = xqb + tx;
-      if (x0 < p.odim[0] && xq < p.odim[p.q])
-        tile[j][tx] = p.in[ibase + x0 * p.istr[0] + xq * p.istr[p.q]];
+    // read: contiguous along q (input fastest); the four loads of a thread
+    // are issued before any of them is used
+    double ld[4];
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      const int64_t x0 = x0b + ty + 8 * jj, xq = xqb + tx;
+      ld[jj] = (x0 < p.odim[0] && xq < p.odim[p.q])
+                   ? p.in[ibase + x0 * p.istr[0] + xq * p.istr[p.q]] : 0.0;
     }
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) tile[ty + 8 * jj][tx] = ld[jj];
     __syncthreads();
-    for (int j = ty; j < 32; j += 8) {
-      int64_t x0 = x0b + tx, xq = xqb + j;
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      const int j = ty + 8 * jj;
+      const int64_t x0 = x0b + tx, xq = xqb + j;
       if (x0 < p.odim[0] && xq < p.odim[p.q]) {
         int64_t o = obase + x0 + xq * p.ostr[p.q];
         double v = p.alpha * tile[tx][j];
@@ -1397,18 +1404,25 @@ __global__ void cs_dot_partial_kernel(int nv, int no, const double* X, const dou
     const double* Xs = X + ij * vv;
     const double* Ys = Y + ij * vv;
     const int a0 = ta * 32, b0 = tb * 32;
-    // xt[j][tx] = X[b0 + tx, a0 + j]
-    for (int j = ty; j < 32; j += 8)
-      if (b0 + tx < nv && a0 + j < nv) xt[j][tx] = Xs[(b0 + tx) + (int64_t)nv * (a0 + j)];
+    // all twelve loads of a thread are issued before any of them is used:
+    // xt[j][tx] = X[b0 + tx, a0 + j], and X, Y at (a0 + tx, b0 + j)
+    double rt[4], rx[4], ry[4];
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      const int j = ty + 8 * jj, a = a0 + tx, b = b0 + j;
+      rt[jj] = (b0 + tx < nv && a0 + j < nv) ? Xs[(b0 + tx) + (int64_t)nv * (a0 + j)] : 0.0;
+      const bool in = a < nv && b < nv;
+      const int64_t i = a + (int64_t)nv * b;
+      rx[jj] = in ? Xs[i] : 0.0;
+      ry[jj] = in ? Ys[i] : 0.0;
+    }
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) xt[ty + 8 * jj][tx] = rt[jj];
     __syncthreads();
-    for (int j = ty; j < 32; j += 8) {
-      const int a = a0 + tx, b = b0 + j;
-      if (a < nv && b < nv) {
-        const int64_t i = a + (int64_t)nv * b;
-        const double y = Ys[i];
-        d += Xs[i] * y;
-        ex += xt[tx][j] * y;  // X[b, a]
-      }
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      d += rx[jj] * ry[jj];
+      ex += xt[tx][ty + 8 * jj] * ry[jj];  // X[b, a]
     }
     __syncthreads();
   }

@@ -460,12 +460,20 @@ __global__ void split_kernel(const double* __restrict__ src, int64_t R, int64_t 
   const bool rfast = (sr == 1);
   for (uint32_t t = blockIdx.x; t < ntile; t += gridDim.x) {
     const int64_t r0 = (int64_t)(t / tk) * 32, k0 = (int64_t)(t % tk) * 32;
-    for (int j = threadIdx.y; j < 32; j += 8) {
+    // the four loads of a thread are issued before any of them is used
+    double xs[4];
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      const int j = threadIdx.y + 8 * jj;
       int64_t r, k;
       if (rfast) { r = r0 + threadIdx.x; k = k0 + j; } else { r = r0 + j; k = k0 + threadIdx.x; }
-      double x = (r < R && k < K) ? src[r * sr + k * sk] : 0.0;
-      if (rfast) tile[j][threadIdx.x] = x;   // tile[k][r]
-      else tile[threadIdx.x][j] = x;         // tile[k][r]
+      xs[jj] = (r < R && k < K) ? src[r * sr + k * sk] : 0.0;
+    }
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      const int j = threadIdx.y + 8 * jj;
+      if (rfast) tile[j][threadIdx.x] = xs[jj];   // tile[k][r]
+      else tile[threadIdx.x][j] = xs[jj];         // tile[k][r]
     }
     __syncthreads();
     for (int j = threadIdx.y; j < 32; j += 8) {
