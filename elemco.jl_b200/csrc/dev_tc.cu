@@ -161,19 +161,23 @@ struct TcOut {
 
 // Epilogue of one 16-column chunk: this lane's row (offset rowoff), columns
 // col0 .. col0+15.  Read-modify-write loads are all issued before the stores.
+// FP32 output with beta 0 or 1 and an alpha that FP32 holds exactly is
+// updated in FP32 (one rounding, as the FP64 expression rounded to FP32
+// gives): the FP64 route costs three conversions per element, which bounded
+// the epilogue of the (T) GEMMs.  Column arithmetic is 32-bit (N < 2^31).
 template <typename CT>
 __device__ __forceinline__ void epi_chunk(CT* __restrict__ C, int64_t rowoff, const uint32_t* r,
                                           int64_t col0, int64_t N, const TcOut& out,
-                                          double alpha, double beta) {
+                                          double alpha, double beta, bool f32math) {
   int64_t off[16];
   if (out.dn == 0) {
     const int64_t b = rowoff + col0 * out.scn;
 #pragma unroll
     for (int j = 0; j < 16; ++j) off[j] = b + j * out.scn;
   } else {
-    const int64_t nq = col0 / out.dn;
-    int64_t nr = col0 - nq * out.dn;
-    int64_t coff = nr * out.scn + nq * out.scn2;
+    const uint32_t dn = (uint32_t)out.dn, nq = (uint32_t)col0 / dn;
+    int64_t nr = (uint32_t)col0 - nq * dn;
+    int64_t coff = nr * out.scn + (int64_t)nq * out.scn2;
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
       off[j] = rowoff + coff;
@@ -185,7 +189,21 @@ __device__ __forceinline__ void epi_chunk(CT* __restrict__ C, int64_t rowoff, co
       }
     }
   }
-  if (beta != 0.0) {
+  if (sizeof(CT) == 4 && f32math) {
+    const float a = (float)alpha;
+    if (beta != 0.0) {  // beta == 1
+      CT old[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) old[j] = (col0 + j < N) ? C[off[j]] : (CT)0;
+#pragma unroll
+      for (int j = 0; j < 16; ++j)
+        if (col0 + j < N) C[off[j]] = (CT)fmaf(a, __uint_as_float(r[j]), (float)old[j]);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 16; ++j)
+        if (col0 + j < N) C[off[j]] = (CT)(a * __uint_as_float(r[j]));
+    }
+  } else if (beta != 0.0) {
     CT old[16];
 #pragma unroll
     for (int j = 0; j < 16; ++j) old[j] = (col0 + j < N) ? C[off[j]] : (CT)0;
@@ -208,7 +226,7 @@ __device__ __forceinline__ void prefetch_cols(const CT* C, int64_t rowoff, int64
                                               int64_t N, const TcOut& out) {
   int64_t nq = 0, nr = col0;
   if (out.dn > 0) {
-    nq = col0 / out.dn;
+    nq = (uint32_t)col0 / (uint32_t)out.dn;
     nr = col0 - nq * out.dn;
   }
   int64_t coff = nr * out.scn + nq * out.scn2;
@@ -379,6 +397,7 @@ __global__ void __launch_bounds__(THREADS_TC, 1)
     // epilogue warps 2..9: TMEM lane quarter q = warp % 4, column half hw
     const int q = warp & 3, hw = (warp - 2) >> 2;
     const uint32_t lane_base = (uint32_t)(q * 32) << 16;
+    const bool f32math = (beta == 0.0 || beta == 1.0) && (double)(float)alpha == alpha;
     int64_t lt = 0;
     for (int64_t it = blockIdx.x; it < items; it += gridDim.x, ++lt) {
       int mt, nt, z;
@@ -426,9 +445,9 @@ __global__ void __launch_bounds__(THREADS_TC, 1)
         if (row < M) {
           const int64_t col0 = (int64_t)nt * TN + c;
           if (out.f32)
-            epi_chunk((float*)out.C, rowoff, r, col0, N, out, alpha, beta);
+            epi_chunk((float*)out.C, rowoff, r, col0, N, out, alpha, beta, f32math);
           else
-            epi_chunk((double*)out.C, rowoff, r, col0, N, out, alpha, beta);
+            epi_chunk((double*)out.C, rowoff, r, col0, N, out, alpha, beta, false);
         }
       }
       asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
@@ -776,6 +795,8 @@ __device__ __forceinline__ void put_slices3(__nv_bfloat16* dst, int64_t sl, int6
 // padding of both is written as zeros.
 // IT: index type of the element loop (32-bit unsigned whenever kp_p * npairs
 // allows: its division by kp_p is the kernel's only per-element division).
+// Each thread takes U elements per pass (U * blockDim apart, coalesced) and
+// issues all their loads before it stores anything.
 template <typename VT, typename IT>
 __global__ void ladder_pack_split_kernel(int nv, int a0, int na, int npairs,
                                          const int2* __restrict__ pairs,
@@ -783,26 +804,44 @@ __global__ void ladder_pack_split_kernel(int nv, int a0, int na, int npairs,
                                          int64_t kp_p, int64_t sl_p, int64_t kp_m, int64_t sl_m,
                                          __nv_bfloat16* __restrict__ Vp,
                                          __nv_bfloat16* __restrict__ Vm) {
+  constexpr int U = 4;
   const int64_t v = nv, lda = v * na, ncdp = v * (v + 1) / 2, ncdm = v * (v - 1) / 2;
   const int64_t mpad = kp_m - ncdm;
   const IT total = (IT)kp_p * (IT)npairs, kpi = (IT)kp_p;
-  for (IT idx = blockIdx.x * (IT)blockDim.x + threadIdx.x; idx < total;
-       idx += (IT)gridDim.x * blockDim.x) {
-    const int64_t k = idx % kpi, pr = idx / kpi;
-    const int2 ab = pairs[pr];
-    const int64_t ap = ab.x - a0, bp = ab.y - a0;
-    const bool minus = ab.x < ab.y;
-    __nv_bfloat16* om = minus ? Vm + (pr - ap - 1) * kp_m : Vm;
-    if (k < ncdp) {
-      const int2 cd = cdp[k];
-      const double x = (double)V[cd.x + v * ap + lda * (cd.y + v * bp)];
-      const double y = (double)V[cd.y + v * ap + lda * (cd.x + v * bp)];
-      put_slices3(Vp + pr * kp_p, sl_p, k, cd.x == cd.y ? x : x + y);
-      if (minus && cd.x < cd.y) put_slices3(om, sl_m, k - cd.y, x - y);
-    } else {
-      put_slices3(Vp + pr * kp_p, sl_p, k, 0.0);
+  const IT step = (IT)gridDim.x * blockDim.x * U;
+  for (IT base = blockIdx.x * (IT)blockDim.x * U + threadIdx.x; base < total; base += step) {
+    int64_t k[U], pr[U];
+    int2 cd[U], ab[U];
+    double x[U], y[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const IT idx = base + (IT)u * blockDim.x;
+      const IT id = idx < total ? idx : 0;
+      k[u] = id % kpi;
+      pr[u] = id / kpi;
+      cd[u] = cdp[k[u] < ncdp ? k[u] : 0];
+      ab[u] = pairs[pr[u]];
     }
-    if (minus && k < mpad) put_slices3(om, sl_m, ncdm + k, 0.0);
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t ap = ab[u].x - a0, bp = ab[u].y - a0;
+      x[u] = k[u] < ncdp ? (double)V[cd[u].x + v * ap + lda * (cd[u].y + v * bp)] : 0.0;
+      y[u] = k[u] < ncdp ? (double)V[cd[u].y + v * ap + lda * (cd[u].x + v * bp)] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (base + (IT)u * blockDim.x >= total) break;
+      const int64_t ap = ab[u].x - a0;
+      const bool minus = ab[u].x < ab[u].y;
+      __nv_bfloat16* om = minus ? Vm + (pr[u] - ap - 1) * kp_m : Vm;
+      if (k[u] < ncdp) {
+        put_slices3(Vp + pr[u] * kp_p, sl_p, k[u], cd[u].x == cd[u].y ? x[u] : x[u] + y[u]);
+        if (minus && cd[u].x < cd[u].y) put_slices3(om, sl_m, k[u] - cd[u].y, x[u] - y[u]);
+      } else {
+        put_slices3(Vp + pr[u] * kp_p, sl_p, k[u], 0.0);
+      }
+      if (minus && k[u] < mpad) put_slices3(om, sl_m, ncdm + k[u], 0.0);
+    }
   }
 }
 
@@ -819,9 +858,9 @@ int ladder_pack_v_split(stream_t s, int nv, int a0, int na, int npairs, const in
   const int64_t sl_m = npm > 0 ? pad_rows(npm) * kp_m : 0;
   if (kp_m - v * (v - 1) / 2 > kp_p) return (int)cudaErrorInvalidValue;
   const int64_t total = kp_p * npairs;
-  const unsigned g = (unsigned)std::min<int64_t>((total + 255) / 256, 148 * 16);
+  const unsigned g = (unsigned)std::min<int64_t>((total + 1023) / 1024, 148 * 16);
   cudaStream_t st = (cudaStream_t)s;
-  const bool small = total < ((int64_t)1 << 32) - 256 * 148 * 16;
+  const bool small = total < ((int64_t)1 << 32) - 4 * 256 * 148 * 16;
 #define ECG_PACK_SPLIT(VT, IT)                                                                \
   ladder_pack_split_kernel<VT, IT><<<g, 256, 0, st>>>(                                        \
       nv, a0, na, npairs, (const int2*)pairs, (const int2*)cdp, (const VT*)V, kp_p, sl_p, kp_m, \
