@@ -218,29 +218,6 @@ __device__ __forceinline__ void epi_chunk(CT* __restrict__ C, int64_t rowoff, co
   }
 }
 
-// L2 prefetch of the C elements (row offset rowoff, columns col0 .. col0+n-1)
-// that a read-modify-write epilogue will load, issued while the MMAs of the
-// tile still run.
-template <typename CT>
-__device__ __forceinline__ void prefetch_cols(const CT* C, int64_t rowoff, int64_t col0, int n,
-                                              int64_t N, const TcOut& out) {
-  int64_t nq = 0, nr = col0;
-  if (out.dn > 0) {
-    nq = (uint32_t)col0 / (uint32_t)out.dn;
-    nr = col0 - nq * out.dn;
-  }
-  int64_t coff = nr * out.scn + nq * out.scn2;
-  for (int j = 0; j < n && col0 + j < N; ++j) {
-    asm volatile("prefetch.global.L2 [%0];\n" ::"l"(C + rowoff + coff));
-    ++nr;
-    coff += out.scn;
-    if (out.dn > 0 && nr == out.dn) {
-      nr = 0;
-      coff += out.scn2 - out.dn * out.scn;
-    }
-  }
-}
-
 template <int NSL, int TN>
 __global__ void __launch_bounds__(THREADS_TC, 1)
     mgemm_bf16_kernel(const __grid_constant__ TcMaps maps, TcOut out, int64_t M, int64_t N,
@@ -410,13 +387,6 @@ __global__ void __launch_bounds__(THREADS_TC, 1)
         rowoff += (row - mq * out.dm) * out.scm + mq * out.scm2;
       } else {
         rowoff += row * out.scm;
-      }
-      if (beta != 0.0 && row < M) {
-        const int64_t col0 = (int64_t)nt * TN + hw * (TN / 2);
-        if (out.f32)
-          prefetch_cols((const float*)out.C, rowoff, col0, TN / 2, N, out);
-        else
-          prefetch_cols((const double*)out.C, rowoff, col0, TN / 2, N, out);
       }
       // every lane waits; the warp goes on only if all lanes saw the
       // accumulator ready and no time-out was recorded, so the warp-wide
