@@ -76,7 +76,7 @@ void Ctx::free_all() {
   if (st) dev::sync(st);
   for (auto& a : allocs) dev::dfree(a.first);
   allocs.clear();
-  memused = 0;
+  memused = handle_bytes;  // handles keep their memory across systems
   if (hscal) dev::hfree_pinned(hscal);
   hscal = nullptr;
   have_system = false;

@@ -30,6 +30,7 @@ struct Ctx {
   dev::stream_t st = nullptr;
   std::string err;
   uint64_t memcap = 0, memused = 0;
+  uint64_t handle_bytes = 0;  // device memory of handles (DF factors), part of memused
   std::vector<std::pair<void*, size_t>> allocs;
   uint64_t generation = 0;  // bumped whenever free_all() releases the system's buffers
   int prec = ECG_PREC_FP64;

@@ -395,6 +395,7 @@ int ecg_df_create(ecg_ctx* ctx, const ecg_shells* ao, const ecg_shells* fit, con
     d->aal = (double*)dev::dmalloc(d->bytes);
     if (!d->aal) throw Error(ECG_ERR_OOM, "cudaMalloc failed for the DF factors");
     c->memused += d->bytes;
+    c->handle_bytes += d->bytes;
     Scope scope{*c, c->allocs.size()};
     int64_t n = 0, np = 0;
     const double* Z = int3c2e_device(*c, ao, fit, &n, &np);
@@ -489,6 +490,7 @@ int ecg_df_destroy(ecg_df* d) {
     if (c->st) dev::sync(c->st);
     dev::dfree(d->aal);
     c->memused -= d->bytes;
+    c->handle_bytes -= d->bytes;
   }
   delete d;
   return ECG_OK;

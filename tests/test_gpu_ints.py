@@ -130,6 +130,30 @@ def test_df_factors_handle_lifetime():
         df.mo(np.eye(ao.nbf))
 
 
+def test_df_factors_memory_accounting_across_systems():
+    """DF factors count against the context's memory cap and keep their
+    memory across ecg_set_system (which frees the system's buffers): under a
+    cap, systems can be set before and after the factors are released, and
+    factors that would exceed the cap are refused with ECG_ERR_OOM."""
+    import ecgpu
+    from ecgpu._lib import ECG_ERR_OOM
+    from ecgpu.synthetic import make_system
+    ao, _ = _shells([(0, 3), (1, 2), (2, 1)], 9)
+    fit, _ = _shells([(0, 1), (1, 1), (2, 1), (0, 2)], 10)
+    B, h1, e0, _ = make_system(3, 12, 40)
+    with ecgpu.Context(0) as c:
+        c.set_mem_cap(64 << 20)
+        df = c.df_factors(ao, fit, np.eye(fit.nbf))
+        c.set_system(B, h1, e0, 3)
+        df.close()
+        c.set_system(B, h1, e0, 3)
+        c.mp2()
+        big = _shells([(4, 1)] * 30, 11)[0]
+        with pytest.raises(ecgpu.ECGError) as e:
+            c.df_factors(big, big, np.eye(big.nbf))  # 270^3 doubles > the cap
+        assert e.value.code == ECG_ERR_OOM
+
+
 def test_df_hf_chain_reproduces_reference_pins(gold):
     """@dfhf with cc-pVDZ / cc-pVTZ-JKFIT on the test/df_hf.jl water, then
     @dfints (frozen O 1s, cc-pVDZ-MPFIT) and ccdriver at the reference's CC
