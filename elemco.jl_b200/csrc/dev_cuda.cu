@@ -1558,45 +1558,23 @@ int ladder_pack_t(stream_t s, int nv, int no, const double* T2, const int* cdp, 
 
 // IT: index type of the element loop (32-bit unsigned whenever ncdp * npairs
 // allows: its division by ncdp is the kernel's only per-element division).
-// Each thread takes U elements per pass (U * blockDim apart, coalesced) and
-// issues all their loads before it stores anything.
 template <typename IT>
 __global__ void ladder_pack_v_kernel(int nv, int a0, int na, int npairs,
                                      const int2* __restrict__ pairs, const int2* __restrict__ cdp,
                                      const double* __restrict__ V, double* __restrict__ Vp,
                                      double* __restrict__ Vm, int64_t ldp, int64_t ldm) {
-  constexpr int U = 4;
   const int64_t v = nv;
   const IT ncdp = (IT)(v * (v + 1) / 2), total = ncdp * (IT)npairs;
   const int64_t lda = v * na;  // Vblk[c + v a' + v na (d + v b'')]
-  const IT step = (IT)gridDim.x * blockDim.x * U;
-  for (IT base = blockIdx.x * (IT)blockDim.x * U + threadIdx.x; base < total; base += step) {
-    int64_t k[U], pr[U];
-    int2 cd[U], ab[U];
-    double x[U], y[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const IT idx = base + (IT)u * blockDim.x;
-      const IT id = idx < total ? idx : 0;
-      k[u] = id % ncdp;
-      pr[u] = id / ncdp;
-      cd[u] = cdp[k[u]];
-      ab[u] = pairs[pr[u]];
-    }
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int64_t ap = ab[u].x - a0, bp = ab[u].y - a0;
-      x[u] = V[cd[u].x + v * ap + lda * (cd[u].y + v * bp)];
-      y[u] = V[cd[u].y + v * ap + lda * (cd[u].x + v * bp)];
-    }
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      if (base + (IT)u * blockDim.x >= total) break;
-      const int64_t ap = ab[u].x - a0;
-      Vp[k[u] + ldp * pr[u]] = (cd[u].x == cd[u].y) ? x[u] : x[u] + y[u];
-      if (cd[u].x < cd[u].y && ab[u].x < ab[u].y)
-        Vm[(k[u] - cd[u].y) + ldm * (pr[u] - ap - 1)] = x[u] - y[u];
-    }
+  for (IT idx = blockIdx.x * (IT)blockDim.x + threadIdx.x; idx < total;
+       idx += (IT)gridDim.x * blockDim.x) {
+    const int64_t k = idx % ncdp, pr = idx / ncdp;
+    const int2 cd = cdp[k], ab = pairs[pr];
+    const int64_t ap = ab.x - a0, bp = ab.y - a0;
+    const double x = V[cd.x + v * ap + lda * (cd.y + v * bp)];
+    const double y = V[cd.y + v * ap + lda * (cd.x + v * bp)];
+    Vp[k + ldp * pr] = (cd.x == cd.y) ? x : x + y;
+    if (cd.x < cd.y && ab.x < ab.y) Vm[(k - cd.y) + ldm * (pr - ap - 1)] = x - y;
   }
 }
 
@@ -1604,12 +1582,11 @@ int ladder_pack_v(stream_t s, int nv, int a0, int na, int npairs, const int* pai
                   const int* cdp, const double* Vblk, double* Vp, double* Vm, int64_t ldp,
                   int64_t ldm) {
   int64_t total = (int64_t)nv * (nv + 1) / 2 * npairs;
-  const unsigned g = grid_for((total + 3) / 4);
-  if (total < ((int64_t)1 << 32) - 4 * 256 * 148 * 16)
-    ladder_pack_v_kernel<uint32_t><<<g, 256, 0, (cudaStream_t)s>>>(
+  if (total < ((int64_t)1 << 32) - 256 * 148 * 16)
+    ladder_pack_v_kernel<uint32_t><<<grid_for(total), 256, 0, (cudaStream_t)s>>>(
         nv, a0, na, npairs, (const int2*)pairs, (const int2*)cdp, Vblk, Vp, Vm, ldp, ldm);
   else
-    ladder_pack_v_kernel<uint64_t><<<g, 256, 0, (cudaStream_t)s>>>(
+    ladder_pack_v_kernel<uint64_t><<<grid_for(total), 256, 0, (cudaStream_t)s>>>(
         nv, a0, na, npairs, (const int2*)pairs, (const int2*)cdp, Vblk, Vp, Vm, ldp, ldm);
   return launched();
 }

@@ -765,8 +765,6 @@ __device__ __forceinline__ void put_slices3(__nv_bfloat16* dst, int64_t sl, int6
 // padding of both is written as zeros.
 // IT: index type of the element loop (32-bit unsigned whenever kp_p * npairs
 // allows: its division by kp_p is the kernel's only per-element division).
-// Each thread takes U elements per pass (U * blockDim apart, coalesced) and
-// issues all their loads before it stores anything.
 template <typename VT, typename IT>
 __global__ void ladder_pack_split_kernel(int nv, int a0, int na, int npairs,
                                          const int2* __restrict__ pairs,
@@ -774,44 +772,26 @@ __global__ void ladder_pack_split_kernel(int nv, int a0, int na, int npairs,
                                          int64_t kp_p, int64_t sl_p, int64_t kp_m, int64_t sl_m,
                                          __nv_bfloat16* __restrict__ Vp,
                                          __nv_bfloat16* __restrict__ Vm) {
-  constexpr int U = 4;
   const int64_t v = nv, lda = v * na, ncdp = v * (v + 1) / 2, ncdm = v * (v - 1) / 2;
   const int64_t mpad = kp_m - ncdm;
   const IT total = (IT)kp_p * (IT)npairs, kpi = (IT)kp_p;
-  const IT step = (IT)gridDim.x * blockDim.x * U;
-  for (IT base = blockIdx.x * (IT)blockDim.x * U + threadIdx.x; base < total; base += step) {
-    int64_t k[U], pr[U];
-    int2 cd[U], ab[U];
-    double x[U], y[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const IT idx = base + (IT)u * blockDim.x;
-      const IT id = idx < total ? idx : 0;
-      k[u] = id % kpi;
-      pr[u] = id / kpi;
-      cd[u] = cdp[k[u] < ncdp ? k[u] : 0];
-      ab[u] = pairs[pr[u]];
+  for (IT idx = blockIdx.x * (IT)blockDim.x + threadIdx.x; idx < total;
+       idx += (IT)gridDim.x * blockDim.x) {
+    const int64_t k = idx % kpi, pr = idx / kpi;
+    const int2 ab = pairs[pr];
+    const int64_t ap = ab.x - a0, bp = ab.y - a0;
+    const bool minus = ab.x < ab.y;
+    __nv_bfloat16* om = minus ? Vm + (pr - ap - 1) * kp_m : Vm;
+    if (k < ncdp) {
+      const int2 cd = cdp[k];
+      const double x = (double)V[cd.x + v * ap + lda * (cd.y + v * bp)];
+      const double y = (double)V[cd.y + v * ap + lda * (cd.x + v * bp)];
+      put_slices3(Vp + pr * kp_p, sl_p, k, cd.x == cd.y ? x : x + y);
+      if (minus && cd.x < cd.y) put_slices3(om, sl_m, k - cd.y, x - y);
+    } else {
+      put_slices3(Vp + pr * kp_p, sl_p, k, 0.0);
     }
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int64_t ap = ab[u].x - a0, bp = ab[u].y - a0;
-      x[u] = k[u] < ncdp ? (double)V[cd[u].x + v * ap + lda * (cd[u].y + v * bp)] : 0.0;
-      y[u] = k[u] < ncdp ? (double)V[cd[u].y + v * ap + lda * (cd[u].x + v * bp)] : 0.0;
-    }
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      if (base + (IT)u * blockDim.x >= total) break;
-      const int64_t ap = ab[u].x - a0;
-      const bool minus = ab[u].x < ab[u].y;
-      __nv_bfloat16* om = minus ? Vm + (pr[u] - ap - 1) * kp_m : Vm;
-      if (k[u] < ncdp) {
-        put_slices3(Vp + pr[u] * kp_p, sl_p, k[u], cd[u].x == cd[u].y ? x[u] : x[u] + y[u]);
-        if (minus && cd[u].x < cd[u].y) put_slices3(om, sl_m, k[u] - cd[u].y, x[u] - y[u]);
-      } else {
-        put_slices3(Vp + pr[u] * kp_p, sl_p, k[u], 0.0);
-      }
-      if (minus && k[u] < mpad) put_slices3(om, sl_m, ncdm + k[u], 0.0);
-    }
+    if (minus && k < mpad) put_slices3(om, sl_m, ncdm + k, 0.0);
   }
 }
 
@@ -828,9 +808,9 @@ int ladder_pack_v_split(stream_t s, int nv, int a0, int na, int npairs, const in
   const int64_t sl_m = npm > 0 ? pad_rows(npm) * kp_m : 0;
   if (kp_m - v * (v - 1) / 2 > kp_p) return (int)cudaErrorInvalidValue;
   const int64_t total = kp_p * npairs;
-  const unsigned g = (unsigned)std::min<int64_t>((total + 1023) / 1024, 148 * 16);
+  const unsigned g = (unsigned)std::min<int64_t>((total + 255) / 256, 148 * 16);
   cudaStream_t st = (cudaStream_t)s;
-  const bool small = total < ((int64_t)1 << 32) - 4 * 256 * 148 * 16;
+  const bool small = total < ((int64_t)1 << 32) - 256 * 148 * 16;
 #define ECG_PACK_SPLIT(VT, IT)                                                                \
   ladder_pack_split_kernel<VT, IT><<<g, 256, 0, st>>>(                                        \
       nv, a0, na, npairs, (const int2*)pairs, (const int2*)cdp, (const VT*)V, kp_p, sl_p, kp_m, \
