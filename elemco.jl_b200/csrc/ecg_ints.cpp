@@ -1,6 +1,8 @@
 // ecg_ints.cpp — C ABI of the integral engine (declared in include/ecgpu.h):
 // shells from the caller's plain arrays, Cartesian integrals on the GPU
-// (dev_ints.cu), transformation to real solid harmonics and normalisation.
+// (dev_ints.cu), transformation to real solid harmonics and normalisation;
+// and the density-fitted factors kept on the device (ecg_df_*) for the DF-HF
+// Fock builds and the MO transform of the CC integrals.
 //
 // Contraction coefficients are those of the basis-set files, which multiply
 // normalised primitives: the engine uses c_k a_k^{(2l+3)/4} (the l-dependent
@@ -278,7 +280,6 @@ double* int3c2e_device(Ctx& c, const ecg_shells* ao, const ecg_shells* fit, int6
   return Z;
 }
 
-
 }  // namespace
 
 // Density-fitted three-index factors held on the device between calls.
@@ -355,7 +356,6 @@ int ecg_int2c2e(ecg_ctx* ctx, const ecg_shells* fit, double* out) {
       for (int64_t i = 0; i < ns; ++i) out[i + ns * j] *= d[i] * d[j];
   });
 }
-
 
 int ecg_int3c2e(ecg_ctx* ctx, const ecg_shells* ao, const ecg_shells* fit, double* out) {
   Ctx* c = ctx;
