@@ -1556,8 +1556,9 @@ int ladder_pack_t(stream_t s, int nv, int no, const double* T2, const int* cdp, 
   return launched();
 }
 
-// IT: index type of the element loop (32-bit unsigned whenever ncdp * npairs
-// allows: its division by ncdp is the kernel's only per-element division).
+// One thread per element; the tiled kernel below replaces it wherever its
+// tile count fits 32 bits (always, for blocks that fit in device memory).
+// IT: index type of the element loop.
 template <typename IT>
 __global__ void ladder_pack_v_kernel(int nv, int a0, int na, int npairs,
                                      const int2* __restrict__ pairs, const int2* __restrict__ cdp,
@@ -1578,16 +1579,77 @@ __global__ void ladder_pack_v_kernel(int nv, int a0, int na, int npairs,
   }
 }
 
+// Upper-triangle tile id -> (tile row tc, tile column td), tc <= td, in the
+// order id = td (td + 1) / 2 + tc.
+__device__ __forceinline__ void tri_tile(uint32_t id, uint32_t& tc, uint32_t& td) {
+  uint32_t t = (uint32_t)((sqrtf(8.0f * (float)id + 1.0f) - 1.0f) * 0.5f);
+  while (t * (t + 1) / 2 > id) --t;
+  while ((t + 1) * (t + 2) / 2 <= id) ++t;
+  td = t;
+  tc = id - t * (t + 1) / 2;
+}
+
+// The same packing by 32 x 32 tiles of (c, d), c0 <= d0, one pair (a, b) per
+// tile: X[c,d] = V[c + v a' + lda (d + v b')] is read along c, the mirrored
+// X[d,c] along d into shared memory, so every load and store is coalesced
+// (the element kernel gathers X[d,c] with stride lda).  Block 32 x 8.
+__global__ void ladder_pack_v_tiled_kernel(int nv, int a0, int na, int npairs,
+                                           const int2* __restrict__ pairs,
+                                           const double* __restrict__ V,
+                                           double* __restrict__ Vp, double* __restrict__ Vm,
+                                           int64_t ldp, int64_t ldm) {
+  __shared__ double ys[32][33];
+  const int v = nv;
+  const int64_t lda = (int64_t)v * na;
+  const uint32_t T = (uint32_t)(v + 31) / 32, NT = T * (T + 1) / 2;
+  const uint32_t total = NT * (uint32_t)npairs;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  for (uint32_t t = blockIdx.x; t < total; t += gridDim.x) {
+    const uint32_t pr = t / NT;
+    uint32_t tc, td;
+    tri_tile(t - pr * NT, tc, td);
+    const int c0 = (int)tc * 32, d0 = (int)td * 32;
+    const int2 ab = pairs[pr];
+    const int64_t ap = ab.x - a0, bp = ab.y - a0;
+    const double* X = V + v * ap + lda * v * bp;  // X[c,d] = X[c + lda d]
+    double xr[4], yr[4];
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      const int d = d0 + ty + 8 * jj, c = c0 + tx;
+      xr[jj] = (d < v && c <= d) ? X[c + lda * d] : 0.0;
+      const int cm = c0 + ty + 8 * jj, dm = d0 + tx;  // X[dm, cm] for (c, d) = (cm, dm)
+      yr[jj] = (cm < v && dm < v) ? X[dm + lda * cm] : 0.0;
+    }
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) ys[ty + 8 * jj][tx] = yr[jj];  // ys[c - c0][d - d0]
+    __syncthreads();
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      const int d = d0 + ty + 8 * jj, c = c0 + tx;
+      if (d < v && c <= d) {
+        const double x = xr[jj], y = ys[tx][ty + 8 * jj];
+        const int64_t k = (int64_t)d * (d + 1) / 2 + c;
+        Vp[k + ldp * pr] = (c == d) ? x : x + y;
+        if (c < d && ab.x < ab.y) Vm[(k - d) + ldm * ((int64_t)pr - ap - 1)] = x - y;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 int ladder_pack_v(stream_t s, int nv, int a0, int na, int npairs, const int* pairs,
                   const int* cdp, const double* Vblk, double* Vp, double* Vm, int64_t ldp,
                   int64_t ldm) {
-  int64_t total = (int64_t)nv * (nv + 1) / 2 * npairs;
-  if (total < ((int64_t)1 << 32) - 256 * 148 * 16)
-    ladder_pack_v_kernel<uint32_t><<<grid_for(total), 256, 0, (cudaStream_t)s>>>(
-        nv, a0, na, npairs, (const int2*)pairs, (const int2*)cdp, Vblk, Vp, Vm, ldp, ldm);
-  else
+  const int64_t T = (nv + 31) / 32, tiles = T * (T + 1) / 2 * npairs;
+  if (tiles < ((int64_t)1 << 32) - 148 * 16) {
+    const unsigned g = (unsigned)std::min<int64_t>(tiles, 148 * 16);
+    ladder_pack_v_tiled_kernel<<<g, dim3(32, 8), 0, (cudaStream_t)s>>>(
+        nv, a0, na, npairs, (const int2*)pairs, Vblk, Vp, Vm, ldp, ldm);
+  } else {
+    const int64_t total = (int64_t)nv * (nv + 1) / 2 * npairs;
     ladder_pack_v_kernel<uint64_t><<<grid_for(total), 256, 0, (cudaStream_t)s>>>(
         nv, a0, na, npairs, (const int2*)pairs, (const int2*)cdp, Vblk, Vp, Vm, ldp, ldm);
+  }
   return launched();
 }
 

@@ -763,8 +763,9 @@ __device__ __forceinline__ void put_slices3(__nv_bfloat16* dst, int64_t sl, int6
 // diagonal) at k, and for a < b and c < d row pr - a' - 1 of the
 // antisymmetric operand gets X[c,d] - X[d,c] at k - d = d(d-1)/2 + c; the K
 // padding of both is written as zeros.
-// IT: index type of the element loop (32-bit unsigned whenever kp_p * npairs
-// allows: its division by kp_p is the kernel's only per-element division).
+// One thread per element; the tiled kernel below replaces it wherever its
+// tile count fits 32 bits (always, for blocks that fit in device memory).
+// IT: index type of the element loop.
 template <typename VT, typename IT>
 __global__ void ladder_pack_split_kernel(int nv, int a0, int na, int npairs,
                                          const int2* __restrict__ pairs,
@@ -795,6 +796,77 @@ __global__ void ladder_pack_split_kernel(int nv, int a0, int na, int npairs,
   }
 }
 
+// Upper-triangle tile id -> (tile row tc, tile column td), tc <= td, in the
+// order id = td (td + 1) / 2 + tc.
+__device__ __forceinline__ void tri_tile(uint32_t id, uint32_t& tc, uint32_t& td) {
+  uint32_t t = (uint32_t)((sqrtf(8.0f * (float)id + 1.0f) - 1.0f) * 0.5f);
+  while (t * (t + 1) / 2 > id) --t;
+  while ((t + 1) * (t + 2) / 2 <= id) ++t;
+  td = t;
+  tc = id - t * (t + 1) / 2;
+}
+
+// ladder_pack_split_kernel by 32 x 32 tiles of (c, d), c0 <= d0, one pair
+// (a, b) per tile: X[c,d] read along c, the mirrored X[d,c] along d into
+// shared memory, so every load and store is coalesced.  The block of a pair's
+// first tile also writes the zero padding of its rows (k >= ncdp of V+,
+// k >= ncdm of V-).  Block 32 x 8.
+template <typename VT>
+__global__ void ladder_pack_split_tiled_kernel(int nv, int a0, int na, int npairs,
+                                               const int2* __restrict__ pairs,
+                                               const VT* __restrict__ V, int64_t kp_p,
+                                               int64_t sl_p, int64_t kp_m, int64_t sl_m,
+                                               __nv_bfloat16* __restrict__ Vp,
+                                               __nv_bfloat16* __restrict__ Vm) {
+  __shared__ double ys[32][33];
+  const int v = nv;
+  const int64_t lda = (int64_t)v * na, ncdp = (int64_t)v * (v + 1) / 2;
+  const int64_t ncdm = (int64_t)v * (v - 1) / 2;
+  const uint32_t T = (uint32_t)(v + 31) / 32, NT = T * (T + 1) / 2;
+  const uint32_t total = NT * (uint32_t)npairs;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  for (uint32_t t = blockIdx.x; t < total; t += gridDim.x) {
+    const uint32_t pr = t / NT, id = t - pr * NT;
+    uint32_t tc, td;
+    tri_tile(id, tc, td);
+    const int c0 = (int)tc * 32, d0 = (int)td * 32;
+    const int2 ab = pairs[pr];
+    const int64_t ap = ab.x - a0, bp = ab.y - a0;
+    const bool minus = ab.x < ab.y;
+    __nv_bfloat16* op = Vp + (int64_t)pr * kp_p;
+    __nv_bfloat16* om = minus ? Vm + ((int64_t)pr - ap - 1) * kp_m : Vm;
+    const VT* X = V + v * ap + lda * v * bp;  // X[c,d] = X[c + lda d]
+    double xr[4], yr[4];
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      const int d = d0 + ty + 8 * jj, c = c0 + tx;
+      xr[jj] = (d < v && c <= d) ? (double)X[c + lda * d] : 0.0;
+      const int cm = c0 + ty + 8 * jj, dm = d0 + tx;  // X[dm, cm] for (c, d) = (cm, dm)
+      yr[jj] = (cm < v && dm < v) ? (double)X[dm + lda * cm] : 0.0;
+    }
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) ys[ty + 8 * jj][tx] = yr[jj];  // ys[c - c0][d - d0]
+    __syncthreads();
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      const int d = d0 + ty + 8 * jj, c = c0 + tx;
+      if (d < v && c <= d) {
+        const double x = xr[jj], y = ys[tx][ty + 8 * jj];
+        const int64_t k = (int64_t)d * (d + 1) / 2 + c;
+        put_slices3(op, sl_p, k, c == d ? x : x + y);
+        if (minus && c < d) put_slices3(om, sl_m, k - d, x - y);
+      }
+    }
+    if (id == 0) {
+      const int f = ty * 32 + tx;
+      for (int64_t k = ncdp + f; k < kp_p; k += 256) put_slices3(op, sl_p, k, 0.0);
+      if (minus)
+        for (int64_t k = ncdm + f; k < kp_m; k += 256) put_slices3(om, sl_m, k, 0.0);
+    }
+    __syncthreads();
+  }
+}
+
 }  // namespace
 
 int ladder_pack_v_split(stream_t s, int nv, int a0, int na, int npairs, const int* pairs,
@@ -807,19 +879,28 @@ int ladder_pack_v_split(stream_t s, int nv, int a0, int na, int npairs, const in
   const int64_t kp_m = v > 1 ? pad_k(v * (v - 1) / 2) : 0;
   const int64_t sl_m = npm > 0 ? pad_rows(npm) * kp_m : 0;
   if (kp_m - v * (v - 1) / 2 > kp_p) return (int)cudaErrorInvalidValue;
-  const int64_t total = kp_p * npairs;
-  const unsigned g = (unsigned)std::min<int64_t>((total + 255) / 256, 148 * 16);
   cudaStream_t st = (cudaStream_t)s;
-  const bool small = total < ((int64_t)1 << 32) - 256 * 148 * 16;
-#define ECG_PACK_SPLIT(VT, IT)                                                                \
-  ladder_pack_split_kernel<VT, IT><<<g, 256, 0, st>>>(                                        \
+  const int64_t T = (v + 31) / 32, tiles = T * (T + 1) / 2 * npairs;
+  if (tiles < ((int64_t)1 << 32) - 148 * 16) {
+    const unsigned g = (unsigned)std::min<int64_t>(tiles, 148 * 16);
+#define ECG_PACK_TILED(VT)                                                                     \
+  ladder_pack_split_tiled_kernel<VT><<<g, dim3(32, 8), 0, st>>>(                               \
+      nv, a0, na, npairs, (const int2*)pairs, (const VT*)V, kp_p, sl_p, kp_m, sl_m,            \
+      (__nv_bfloat16*)Vp, (__nv_bfloat16*)Vm)
+    if (v_f32) ECG_PACK_TILED(float);
+    else ECG_PACK_TILED(double);
+#undef ECG_PACK_TILED
+  } else {
+    const int64_t total = kp_p * npairs;
+    const unsigned g = (unsigned)std::min<int64_t>((total + 255) / 256, 148 * 16);
+#define ECG_PACK_SPLIT(VT)                                                                    \
+  ladder_pack_split_kernel<VT, uint64_t><<<g, 256, 0, st>>>(                                  \
       nv, a0, na, npairs, (const int2*)pairs, (const int2*)cdp, (const VT*)V, kp_p, sl_p, kp_m, \
       sl_m, (__nv_bfloat16*)Vp, (__nv_bfloat16*)Vm)
-  if (v_f32 && small) ECG_PACK_SPLIT(float, uint32_t);
-  else if (v_f32) ECG_PACK_SPLIT(float, uint64_t);
-  else if (small) ECG_PACK_SPLIT(double, uint32_t);
-  else ECG_PACK_SPLIT(double, uint64_t);
+    if (v_f32) ECG_PACK_SPLIT(float);
+    else ECG_PACK_SPLIT(double);
 #undef ECG_PACK_SPLIT
+  }
   note_launches(1);
   return (int)cudaGetLastError();
 }
