@@ -55,6 +55,18 @@ def algorithmic_flops(no, nv, nq, dc=False):
     return 2 * o**2 * v**4 + 2 * nq * v**4 + ring * o**3 * v**3 + 4 * o**4 * v**2
 
 
+def max_over_ranks(x, dist=None, device="cuda"):
+    """The largest of the ranks' values of x (every rank gets it); x itself
+    when there is one process.  Replicas time their own steps and the job's
+    time is the slowest rank's."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def parse_args():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -574,10 +586,7 @@ def main():
     if dist:
         dist.barrier()
     clk = clocks.stop() if clocks else None
-    if dist:
-        t = torch.tensor([total], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total = float(t.item())
+    total = max_over_ranks(total, dist)
 
     # ---- e2e: the same iterations through the C ABI with pinned host amplitudes ----
     n1, n2 = nv * no, nv * nv * no * no
@@ -590,10 +599,7 @@ def main():
     def host_step():
         ctx.cc_step_host(T1p, T2p, dc=dc)
     total_e2e = timed_steps(a.steps, host_step)
-    if dist:
-        t = torch.tensor([total_e2e], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_e2e = float(t.item())
+    total_e2e = max_over_ranks(total_e2e, dist)
 
     # ---- roofline of the FP64 DMMA GEMM: every GEMM launch of R FP64 steps ----
     R = 2
